@@ -1,0 +1,352 @@
+#!/usr/bin/env python3
+"""Benchmark: particle-updates/s of the MLS-MPM step (P2G + grid update + G2P
+with plasticity) on B200, through the solver's C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3] [--impl ours|reference]
+
+One JSON line on rank 0. A step is one P2G -> grid -> G2P pass over every
+particle of the workload (default: the 3D snowball-on-slab scene, 128^3 grid,
+8 particles per cell, 1.65M particles; its ~0.3 GB of particle and grid state
+is larger than the 126 MB L2, so no flush is needed between steps).
+
+* value     device time (CUDA events on the solver's stream) for K steps with
+            state resident in HBM; max over ranks; N ranks run independent
+            replicas (the path does not shard across GPUs here).
+* e2e       the same metric through the public C ABI with host buffers: every
+            step uploads the particle state from pinned host memory
+            (mpm_set_state), steps, and reads the state back (mpm_get_state).
+* roofline  the dominant kernel's algorithmic bytes / its CUDA-event duration,
+            against MEASURED_PEAKS.json's HBM copy bandwidth.
+* cpu_baseline  the oracle's FP32 OpenMP port of the reference MLS step on the
+            host cores, a bounded number of steps of the same scene.
+
+--impl reference times the reference's CPU implementation of this step on the
+host cores (rank 0 only): the oracle's FP32 restatement of the reference
+shaders with OpenMP, since the reference's own CPU path (src/cpu) is 2D only;
+for 2D workloads the reference's compiled src/cpu runs instead, one solver
+per core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-updates/s (P2G+grid+G2P), plain vs MLP-plasticity, 1 B200, % HBM peak"
+UNIT = "particle-updates/s"
+
+# Algorithmic bytes (minimal FP32 SoA state, uniform mass/volume).
+# Per particle-step: P2G reads x, v, B, F_E, J_p; G2P reads x, F_E, J_p and
+# writes x, v, B, F_E, J_p.   Per active node: accumulator clear + read
+# 8(d+1) each, node velocities write 8d, G2P read 8d.
+def bytes_per_particle(d):
+    p2g = 4 * (2 * d + 2 * d * d + 1)
+    g2p = 4 * (d + d * d + 1) + 4 * (2 * d + 2 * d * d + 1)
+    return p2g, g2p
+
+
+def bytes_per_node(d):
+    grid = 8 * (d + 1) * 2 + 8 * d
+    g2p = 8 * d
+    return grid, g2p
+
+
+WORKLOADS = {
+    "c3": "3D snowball (r 0.12, v -3) on a 0.1 slab, 128^3 grid, 8 ppc, dt 5e-5",
+    "c2": "2D 8 random blocks, 512^2 grid, 8 ppc, dt 2.5e-5",
+    "c2_1m": "2D 8 random blocks, 512^2 grid, 27 ppc (~1M particles), dt 2.5e-5",
+    "c1": "2D 3 blocks, 128^2 grid, 4 ppc, dt 1e-4",
+    "c5": "3D two snowballs (r 0.15, relative speed 6), 256^3 grid, 8 ppc, dt 5e-5",
+}
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_scene(name):
+    from mpm_snow_sim2d_b200 import scenes
+    return scenes.workload(name)
+
+
+def cpu_port_time(scene, target_s=12.0, max_steps=20):
+    """FP32 OpenMP port of the reference MLS step on all host cores."""
+    from oracle import oracle as O
+    threads = O.lib().orc_max_threads()
+    st = O.initial_state(scene, np.float32)
+    t0 = time.perf_counter()
+    O.run_oracle(scene, st, 1, fp32=True, threads=threads)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, target_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    O.run_oracle(scene, st, steps, fp32=True, threads=threads)
+    dt = time.perf_counter() - t0
+    return dict(value=scene.count * steps / dt, unit=UNIT, cores=threads, kind="port",
+                sample=f"{steps} full steps of the {scene.name} scene ({scene.count} particles), FP32, "
+                       f"{threads} OpenMP threads, after 1 untimed step")
+
+
+def refcpu_time(scene, steps, replicas):
+    from oracle import oracle as O
+    _, info = O.run_refcpu(scene, steps, replicas=replicas)
+    return scene.count * steps * replicas / info["loop_seconds"], info
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    scene = make_scene(args.workload)
+    from oracle import oracle as O
+    if scene.dim == 2 and O.refcpu_available():
+        cores = os.cpu_count() or 1
+        for _ in range(args.warmup and 1):
+            refcpu_time(scene, 1, 1)
+        rate, info = refcpu_time(scene, args.steps, cores)
+        kind, sample = "reference", (f"{args.steps} steps of the {scene.name} scene, reference src/cpu compiled "
+                                      f"unmodified, {cores} independent single-threaded solvers")
+        value = rate
+    else:
+        threads = O.lib().orc_max_threads()
+        st = O.initial_state(scene, np.float32)
+        O.run_oracle(scene, st, 1, fp32=True, threads=threads)  # untimed warm-up step
+        done, spent = 0, 0.0
+        while done < args.steps and spent < args.budget_s:
+            t0 = time.perf_counter()
+            O.run_oracle(scene, st, 1, fp32=True, threads=threads)
+            spent += time.perf_counter() - t0
+            done += 1
+        value = scene.count * done / spent
+        cores, kind = threads, "port"
+        sample = (f"{done} of {args.steps} full steps of the {scene.name} scene ({scene.count} particles), capped at "
+                  f"{args.budget_s:.0f} s: FP32 restatement of the reference MLS step (src/gpu/shaders/"
+                  f"{scene.dim}d) with {threads} OpenMP threads; the reference's own CPU path is 2D only")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+        "config": {"workload": f"{args.workload}: {WORKLOADS.get(args.workload, '')}", "particles": scene.count},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--budget-s", type=float, default=60.0, help="CPU time cap of the reference arm")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from mpm_snow_sim2d_b200 import Solver
+    from mpm_snow_sim2d_b200.build import build
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    if rank == 0:
+        build()
+    if world > 1:
+        dist.barrier()
+    device = torch.cuda.current_device()
+
+    scene = make_scene(args.workload)
+    d = scene.dim
+    stream = torch.cuda.Stream()
+    solver = Solver.from_scene(scene)
+    solver.set_stream(stream.cuda_stream)
+
+    # warm-up, then active-node count (untimed P2G-only pass)
+    solver.Step(args.warmup)
+    torch.cuda.synchronize()
+    m, _ = solver.rasterize()
+    active = int((m > 0).sum())
+
+    # ---- timed region: K steps, state resident in HBM ----
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clocks:
+        e0.record(stream)
+        solver.Step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    flags = solver.status()
+    value = world * scene.count * args.steps / (ms / 1e3)
+
+    # ---- per-stage device time (events between kernels), for the roofline ----
+    stages = solver.step_profiled(args.steps)
+    stage_avg = {k: v / args.steps for k, v in stages.items()}
+
+    # ---- e2e: host state in (pinned), step, host state out, through the C ABI ----
+    import ctypes as C
+    from mpm_snow_sim2d_b200._lib import MpmStateHost, check
+    n = scene.count
+    pin = lambda *shape: torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    host_in = [pin(n, d), pin(n, d), pin(n, d, d), pin(n, d, d), pin(n)]
+    host_out = [pin(n, d), pin(n, d), pin(n, d, d), pin(n, d, d), pin(n)]
+    st0 = solver.get_state()
+    for t_, a in zip(host_in, (st0.position, st0.velocity, st0.affine_b, st0.elastic_f, st0.plastic_det)):
+        t_.numpy()[...] = a
+    fp = lambda t_: C.cast(C.c_void_p(t_.data_ptr()), C.POINTER(C.c_float))
+    hin = MpmStateHost(n, *[fp(t_) for t_ in host_in])
+    hout = MpmStateHost(n, *[fp(t_) for t_ in host_out])
+    lib = solver._lib
+    bytes_state = sum(t_.numel() * 4 for t_ in host_in)
+    ke = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        check(lib.mpm_set_state(solver._h, C.byref(hin)), solver._h)
+        check(lib.mpm_step(solver._h, 1), solver._h)
+        check(lib.mpm_get_state(solver._h, C.byref(hout)), solver._h)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n * ke / e2e_s
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_src = load_peaks()
+    p2g_b, g2p_b = bytes_per_particle(d)
+    grid_b, g2p_nb = bytes_per_node(d)
+    alg = {"p2g": n * p2g_b, "grid_update": active * grid_b, "g2p": n * g2p_b + active * g2p_nb}
+    dom = max(stage_avg, key=stage_avg.get)
+    achieved = alg[dom] / (stage_avg[dom] / 1e3) / 1e9
+    step_bytes = sum(alg.values())
+    step_ms = ms / args.steps
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg[dom],
+                "step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
+                         "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_port_time(scene)
+        except Exception as e:  # the CPU baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": f"synthetic (seeded {scene.name} scene, {scene.count} particles)",
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]}", "particles": scene.count,
+                       "nodes": scene.nodes, "active_nodes": active, "plasticity": "exact",
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "roofline": roofline,
+            "stages_ms": stage_avg,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
+                    "d2h_bytes_per_step": bytes_state, "steps": ke},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks.summary(),
+            "status_flags": flags,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+/*
+ * mpm.h — C ABI of the B200 (sm_100a) MLS-MPM snow solver.
+ *
+ * This is the drop-in boundary for the reference's solver interface
+ * (michal-sitarz2/MPM_Snow_Sim2D): the compile-time alias
+ * `using Solver = GPUSolver | CPUSolver` (src/main.cpp:23-29) with
+ *     Solver()                                  src/gpu/GPUSolver.cpp:7-51, src/cpu/CPUSolver.h:12-15
+ *     void Step()                               src/gpu/GPUSolver.cpp:63-80, src/cpu/CPUSolver.h:16
+ *     const std::vector<Vec>& GetParticlePositions()
+ *                                               src/gpu/GPUSolver.cpp:276-295, src/cpu/CPUSolver.h:20-27
+ * Knobs mirror src/shared/Parameters.h:6-84; particle arrays mirror the SSBO
+ * contents built by GPUSolver::InitBuffers (src/gpu/GPUSolver.cpp:95-159).
+ *
+ * Units are the reference's grid units: cell size 1, node (i, j[, k]) at
+ * x = (i, j[, k]), positions in [0, WIDTH] x [0, HEIGHT] (x [0, DEPTH]).
+ *
+ * Conventions
+ *   - Every entry point returns an mpm_status; nothing throws across the ABI.
+ *   - A solver owns its device memory (freed by mpm_destroy); the caller owns
+ *     every host array it passes. Input arrays are copied before return.
+ *   - Vectors are interleaved per particle (x, y[, z]) like std::vector<glm::vec2|3>;
+ *     matrices are row-major dim x dim per particle.
+ *   - A solver is bound to one device (the current one at mpm_create) and one
+ *     CUDA stream; a handle must not be used from two threads at once.
+ *   - mpm_step is asynchronous; every getter synchronises the solver's stream.
+ *   - The product path has no CPU fallback: without a usable sm_100 device,
+ *     mpm_create returns MPM_ERR_NO_DEVICE.
+ */
+#ifndef MPM_B200_MPM_H
+#define MPM_B200_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(MPM_BUILDING_LIBRARY) && defined(__GNUC__)
+#define MPM_API __attribute__((visibility("default")))
+#else
+#define MPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID_ARGUMENT = 1,
+    MPM_ERR_CUDA = 2,
+    MPM_ERR_OUT_OF_MEMORY = 3,
+    MPM_ERR_NAN_STATE = 4,            /* a particle state became non-finite */
+    MPM_ERR_FIXED_POINT_OVERFLOW = 5, /* a grid contribution exceeded the int64 fixed-point range */
+    MPM_ERR_NO_DEVICE = 6,
+    MPM_ERR_IO = 7,
+    MPM_ERR_STATE_MISMATCH = 8,       /* checkpoint does not match this solver */
+    MPM_ERR_TIMEOUT = 9,              /* a bounded device-side wait gave up */
+    MPM_ERR_UNSUPPORTED = 10,
+    MPM_ERR_CAPACITY = 11             /* a buffer or fixed device capacity is too small */
+} mpm_status;
+
+/* Device status word bits (mpm_get_status). Kernels set them with atomicOr
+ * and never trap. */
+enum {
+    MPM_FLAG_NAN_STATE = 1u << 0,
+    MPM_FLAG_FIXED_POINT_OVERFLOW = 1u << 1,
+    MPM_FLAG_PARTICLE_OUT_OF_DOMAIN = 1u << 2, /* a stencil reached outside the grid */
+    MPM_FLAG_SVD_FP64_FALLBACK = 1u << 3,      /* informational: the FP64 SVD branch ran */
+    MPM_FLAG_TIMEOUT = 1u << 4
+};
+
+typedef enum mpm_formulation {
+    MPM_FORMULATION_MLS = 0,    /* the reference GPU shaders (src/gpu/shaders/{2d,3d}) */
+    MPM_FORMULATION_CLASSIC = 1 /* the reference CPU path (src/cpu), 2D only */
+} mpm_formulation;
+
+typedef enum mpm_boundary {
+    MPM_BOUNDARY_FRICTION = 0, /* wall planes with separation + Coulomb friction (grid_update.glsl) */
+    MPM_BOUNDARY_STICKY = 1    /* nodes within BORDER_MARGIN of a wall are held at rest */
+} mpm_boundary;
+
+typedef enum mpm_plasticity {
+    MPM_PLASTIC_EXACT = 0, /* SVD return map (g2p.glsl:74-93) */
+    MPM_PLASTIC_MLP = 1    /* learned surrogate with per-particle exact fallback */
+} mpm_plasticity;
+
+/* Simulation knobs: one field per src/shared/Parameters.h knob on the step
+ * path, plus the solver's own choices. Fill with mpm_params_default(). */
+typedef struct mpm_params {
+    int32_t dim;           /* 2 or 3 (SIM_3D)                                   */
+    int32_t width;         /* WIDTH: cells along x; nodes = WIDTH + 1           */
+    int32_t height;        /* HEIGHT                                            */
+    int32_t depth;         /* DEPTH (3D only)                                   */
+    int32_t border_margin; /* BORDER_MARGIN (cells)                             */
+    int32_t formulation;   /* mpm_formulation                                   */
+    int32_t boundary;      /* mpm_boundary                                      */
+    int32_t sort_period;   /* steps between particle re-binning (0 = auto)      */
+    float delta_time;      /* DELTA_TIME                                        */
+    float gravity;         /* GRAVITY (along -y when negative), grid units/s^2  */
+    float friction;        /* FRICTION (Coulomb coefficient at the walls)       */
+    float theta_c;         /* THETA_C critical compression                      */
+    float theta_s;         /* THETA_S critical stretch                          */
+    float xi;              /* XI hardening coefficient                          */
+    float nu;              /* NU Poisson ratio                                  */
+    float youngs;          /* E Young's modulus                                 */
+    float rho;             /* RHO: mass = volume * RHO / 100 when no mass given */
+    int32_t fixed_point_log2_mass;     /* grid mass scale 2^k (0 = auto)        */
+    int32_t fixed_point_log2_momentum; /* grid momentum scale 2^k (0 = auto)    */
+    int32_t reserved[5];
+} mpm_params;
+
+/* Initial particles, as InitBuffers builds them (GPUSolver.cpp:95-159). */
+typedef struct mpm_particles_init {
+    int64_t count;
+    const float* position; /* count * dim                                    */
+    const float* velocity; /* count * dim (NULL = at rest)                   */
+    const float* volume;   /* count                                          */
+    const float* mass;     /* count, or NULL: volume * rho / 100 (Particles.cpp:18) */
+} mpm_particles_init;
+
+/* Host view of the particle state. Each pointer may be NULL (skipped). The
+ * elastic gradient F_E and the plastic determinant J_p = det F_P are the
+ * plastic state; the reference stores the full F_P but reads only its
+ * determinant (p2g.glsl:46,52), so the solver stores J_p. */
+typedef struct mpm_state_host {
+    int64_t count;
+    float* position;        /* count * dim                     */
+    float* velocity;        /* count * dim                     */
+    float* affine_b;        /* count * dim * dim (B_p)         */
+    float* elastic_f;       /* count * dim * dim (F_E)         */
+    float* plastic_det;     /* count (J_p)                     */
+} mpm_state_host;
+
+struct mpm_solver;
+typedef struct mpm_solver mpm_solver;
+
+/* Parameters.h defaults (WIDTH 200, HEIGHT 100, DEPTH 100, BORDER_MARGIN 2,
+ * GRAVITY -9.81, FRICTION 0.3, DELTA_TIME 1e-3, THETA_C 2e-2, THETA_S 6e-3,
+ * XI 10, NU 0.2, E 1.4e5, RHO 400), MLS formulation, friction walls.
+ * Replaces the constants of src/shared/Parameters.h:29-84. */
+MPM_API void mpm_params_default(mpm_params* out, int32_t dim);
+
+/* Solver(): copies particles to the device and prepares the step.
+ * Replaces GPUSolver::GPUSolver + InitBuffers (src/gpu/GPUSolver.cpp:7-51,83-202). */
+MPM_API mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* particles, mpm_solver** out);
+
+/* ~Solver(): releases every device buffer (src/gpu/GPUSolver.cpp:53-60). */
+MPM_API mpm_status mpm_destroy(mpm_solver* solver);
+
+/* Step(): advances `nsteps` time steps of DELTA_TIME (P2G, grid update,
+ * G2P with plasticity); asynchronous on the solver's stream.
+ * Replaces GPUSolver::Step (src/gpu/GPUSolver.cpp:63-80) called nsteps times. */
+MPM_API mpm_status mpm_step(mpm_solver* solver, int32_t nsteps);
+
+/* GetParticlePositions(): copies `count * dim` floats into `out` (capacity
+ * `cap_floats`), in the order the particles were given to mpm_create.
+ * Replaces GPUSolver::GetParticlePositions (src/gpu/GPUSolver.cpp:276-295). */
+MPM_API mpm_status mpm_get_positions(mpm_solver* solver, float* out, size_t cap_floats);
+
+/* Number of particles and the dimension. */
+MPM_API mpm_status mpm_get_info(const mpm_solver* solver, int64_t* count, int32_t* dim);
+
+/* Full particle state, host copies in creation order (the SSBO contents of
+ * bindings 0-6, src/gpu/GPUSolver.cpp:166-172, minus mass/volume). */
+MPM_API mpm_status mpm_get_state(mpm_solver* solver, mpm_state_host* state);
+
+/* Overwrite the particle state (same layout as mpm_get_state; NULL fields keep
+ * their values). */
+MPM_API mpm_status mpm_set_state(mpm_solver* solver, const mpm_state_host* state);
+
+/* One particle-to-grid pass on the current state without advancing time
+ * (Grid::RasterizeToGrid, src/cpu/Grid.cpp:118-163; p2g.glsl): returns node
+ * mass and momentum (MLS: momentum with the stress impulse folded in; CLASSIC:
+ * momentum - DELTA_TIME * force) as doubles, `nodes` and `nodes * dim` values.
+ * Optional raw int64 fixed-point sums in `raw` ((1 + dim) * nodes, component-major). */
+MPM_API mpm_status mpm_rasterize(mpm_solver* solver, double* node_mass, double* node_momentum, int64_t* raw,
+                         size_t nodes);
+
+/* OR of every MPM_FLAG_* a kernel raised since creation (synchronises). */
+MPM_API mpm_status mpm_get_status(mpm_solver* solver, uint32_t* flags);
+
+/* Launch work on this stream (a cudaStream_t) instead of the solver's own. */
+MPM_API mpm_status mpm_set_stream(mpm_solver* solver, void* cuda_stream);
+
+/* Checkpoint / resume: flat binary SoA with a header (dim, count, grid, params
+ * hash, step). The reference has none; frames were PNGs (src/main.cpp:177-205). */
+MPM_API mpm_status mpm_save_state(mpm_solver* solver, const char* path);
+MPM_API mpm_status mpm_load_state(mpm_solver* solver, const char* path);
+
+/* Steps taken since creation (or since the loaded checkpoint's step). */
+MPM_API mpm_status mpm_get_step(const mpm_solver* solver, int64_t* step);
+
+/* Human-readable description of the last error on this handle ("" if none).
+ * Replaces CheckGLError's log line (src/gpu/GPUSolver.cpp:407-417). */
+MPM_API const char* mpm_last_error(const mpm_solver* solver);
+
+/* Text for a status code. */
+MPM_API const char* mpm_status_string(mpm_status status);
+
+/* Per-stage device timing: runs `nsteps` steps like mpm_step with a CUDA
+ * event after every stage and adds each stage's device time in milliseconds to
+ * stage_ms[s] for s < min(nstages, mpm_stage_count()). Synchronises. The
+ * reference has no timers (src/main.cpp:11 includes <chrono> unused). */
+MPM_API mpm_status mpm_step_profiled(mpm_solver* solver, int32_t nsteps, double* stage_ms, int32_t nstages);
+MPM_API int32_t mpm_stage_count(const mpm_solver* solver);
+MPM_API const char* mpm_stage_name(const mpm_solver* solver, int32_t stage);
+
+/* Fixed-point scales in use (log2), for diagnostics. */
+MPM_API mpm_status mpm_get_fixed_point(const mpm_solver* solver, int32_t* log2_mass, int32_t* log2_momentum);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* MPM_B200_MPM_H */

@@ -1,0 +1,582 @@
+// C ABI of the B200 MLS-MPM solver (include/mpm/mpm.h): device memory, the
+// step sequence, state import/export and checkpoints. The product path has no
+// CPU fallback: without a usable sm_100 device every create fails.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mpm/mpm.h"
+#include "mpm_kernels.cuh"
+
+using namespace mpm;
+
+struct mpm_solver {
+    mpm_params params{};
+    int dim = 2, form = kMLS;
+    int n = 0;
+    long long nodes = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    // particles (SoA)
+    float *x = nullptr, *v = nullptr, *B = nullptr, *Fe = nullptr, *Jp = nullptr;
+    float *mass = nullptr, *vol = nullptr;
+    float mass_u = 0.f, vol_u = 0.f;
+    int* id = nullptr;
+    // grid
+    unsigned long long* acc = nullptr;
+    float4* gv = nullptr;
+    unsigned* status = nullptr;
+    float* staging = nullptr;
+    size_t staging_floats = 0;
+    int log2_sm = 0, log2_sp = 0, log2_sf = 0;
+    long long step = 0;
+    StepConsts C{};
+    std::string err;
+};
+
+namespace {
+
+const char* kStatusText[] = {"ok",
+                             "invalid argument",
+                             "CUDA error",
+                             "out of device memory",
+                             "particle state became non-finite",
+                             "fixed-point grid overflow",
+                             "no usable sm_100 CUDA device",
+                             "I/O error",
+                             "checkpoint does not match this solver",
+                             "device-side wait timed out",
+                             "unsupported configuration",
+                             "capacity too small"};
+
+mpm_status fail(mpm_solver* s, mpm_status code, const std::string& what) {
+    if (s) s->err = what;
+    return code;
+}
+
+mpm_status cuda_fail(mpm_solver* s, cudaError_t e, const char* where) {
+    std::string msg = std::string(where) + ": " + cudaGetErrorString(e);
+    if (s) s->err = msg;
+    return e == cudaErrorMemoryAllocation ? MPM_ERR_OUT_OF_MEMORY : MPM_ERR_CUDA;
+}
+
+#define MPM_CUDA(s, call)                                      \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail((s), e_, #call); \
+    } while (0)
+
+int nacc(int dim, int form) { return form == kClassic ? 1 + 2 * dim : 1 + dim; }
+
+template <typename T> cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+void release(mpm_solver* s) {
+    float* fl[] = {s->x, s->v, s->B, s->Fe, s->Jp, s->mass, s->vol, s->staging};
+    for (float* p : fl)
+        if (p) cudaFree(p);
+    if (s->id) cudaFree(s->id);
+    if (s->acc) cudaFree(s->acc);
+    if (s->gv) cudaFree(s->gv);
+    if (s->status) cudaFree(s->status);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+}
+
+Particles particle_view(mpm_solver* s) {
+    Particles P;
+    P.x = s->x; P.v = s->v; P.B = s->B; P.Fe = s->Fe; P.Jp = s->Jp;
+    P.mass = s->mass; P.vol = s->vol; P.mass_u = s->mass_u; P.vol_u = s->vol_u;
+    P.n = s->n;
+    return P;
+}
+
+template <int D, int FORM> cudaError_t launch_p2g(mpm_solver* s) {
+    if (s->n == 0) return cudaSuccess;
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_p2g_simple<D, FORM><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->acc, s->status);
+    return cudaGetLastError();
+}
+
+template <int D, int FORM> cudaError_t launch_grid(mpm_solver* s) {
+    const int threads = 256;
+    const long long blocks = (s->nodes + threads - 1) / threads;
+    k_grid_update<D, FORM><<<(unsigned)blocks, threads, 0, s->stream>>>(s->C, s->acc, s->gv, s->status);
+    return cudaGetLastError();
+}
+
+template <int D, int FORM> cudaError_t launch_g2p(mpm_solver* s) {
+    if (s->n == 0) return cudaSuccess;
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_g2p_simple<D, FORM><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->status);
+    return cudaGetLastError();
+}
+
+template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
+    cudaError_t e = launch_p2g<D, FORM>(s);
+    if (e != cudaSuccess) return e;
+    e = launch_grid<D, FORM>(s);
+    if (e != cudaSuccess) return e;
+    return launch_g2p<D, FORM>(s);
+}
+
+cudaError_t dispatch_step(mpm_solver* s) {
+    if (s->dim == 2) return s->form == kClassic ? step_once<2, kClassic>(s) : step_once<2, kMLS>(s);
+    return step_once<3, kMLS>(s);
+}
+
+cudaError_t dispatch_p2g(mpm_solver* s) {
+    if (s->dim == 2) return s->form == kClassic ? launch_p2g<2, kClassic>(s) : launch_p2g<2, kMLS>(s);
+    return launch_p2g<3, kMLS>(s);
+}
+
+// Choose power-of-two fixed-point scales so that no node sum can exceed 2^62
+// while |node velocity| <= v_cap = 16 cells per step (a blow-up long before
+// that point is flagged by the grid pass).
+void choose_scales(mpm_solver* s, double total_mass) {
+    const mpm_params& p = s->params;
+    const double v_cap = 16.0 / p.delta_time;
+    const double mt = total_mass > 0 ? total_mass * 1.125 : 1.0;
+    int lm = (int)std::floor(62.0 - std::log2(mt));
+    int lp = (int)std::floor(62.0 - std::log2(mt * v_cap));
+    lm = lm > 100 ? 100 : (lm < -100 ? -100 : lm);
+    lp = lp > 100 ? 100 : (lp < -100 ? -100 : lp);
+    if (p.fixed_point_log2_mass != 0) lm = p.fixed_point_log2_mass;
+    if (p.fixed_point_log2_momentum != 0) lp = p.fixed_point_log2_momentum;
+    s->log2_sm = lm;
+    s->log2_sp = lp;
+    s->log2_sf = lp + (int)std::floor(std::log2((double)p.delta_time));
+    s->C.sm = std::ldexp(1.0f, lm);
+    s->C.sp = std::ldexp(1.0f, lp);
+    s->C.sf = std::ldexp(1.0f, s->log2_sf);
+    s->C.inv_sm = std::ldexp(1.0f, -lm);
+    s->C.inv_sp = std::ldexp(1.0f, -lp);
+    s->C.inv_sf = std::ldexp(1.0f, -s->log2_sf);
+    s->C.v_cap = (float)v_cap;
+}
+
+void fill_consts(mpm_solver* s) {
+    const mpm_params& p = s->params;
+    StepConsts& C = s->C;
+    C.W = p.width; C.H = p.height; C.Dp = s->dim == 3 ? p.depth : 0;
+    C.nx = p.width + 1; C.ny = p.height + 1; C.nz = s->dim == 3 ? p.depth + 1 : 1;
+    C.nodes = (long long)C.nx * C.ny * C.nz;
+    C.dt = p.delta_time; C.gravity = p.gravity; C.friction = p.friction;
+    C.theta_c = p.theta_c; C.theta_s = p.theta_s; C.xi = p.xi;
+    // Lame parameters as in src/shared/Parameters.h:82-84, evaluated in double.
+    const double E = p.youngs, nu = p.nu;
+    C.mu0 = (float)(E / (2.0 * (1.0 + nu)));
+    C.la0 = (float)((E * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+    C.margin = (float)p.border_margin;
+    C.boundary = p.boundary;
+}
+
+mpm_status validate(const mpm_params* p, std::string& why) {
+    if (!p) { why = "params is NULL"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->dim != 2 && p->dim != 3) { why = "dim must be 2 or 3"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->width < 1 || p->height < 1 || (p->dim == 3 && p->depth < 1)) { why = "grid extent must be >= 1 cell"; return MPM_ERR_INVALID_ARGUMENT; }
+    const double nodes = double(p->width + 1) * (p->height + 1) * (p->dim == 3 ? p->depth + 1 : 1);
+    if (nodes > 2.0e9) { why = "grid too large"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (!(p->delta_time > 0.f) || !std::isfinite(p->delta_time)) { why = "delta_time must be > 0"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->formulation != MPM_FORMULATION_MLS && p->formulation != MPM_FORMULATION_CLASSIC) { why = "unknown formulation"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->formulation == MPM_FORMULATION_CLASSIC && p->dim != 2) { why = "the CLASSIC (reference CPU) formulation is 2D only"; return MPM_ERR_UNSUPPORTED; }
+    if (p->boundary != MPM_BOUNDARY_FRICTION && p->boundary != MPM_BOUNDARY_STICKY) { why = "unknown boundary"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->border_margin < 0) { why = "border_margin must be >= 0"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (!(p->nu > -1.f && p->nu < 0.5f)) { why = "nu must be in (-1, 0.5)"; return MPM_ERR_INVALID_ARGUMENT; }
+    return MPM_OK;
+}
+
+mpm_status ensure_staging(mpm_solver* s, size_t floats) {
+    if (floats <= s->staging_floats) return MPM_OK;
+    if (s->staging) cudaFree(s->staging);
+    s->staging = nullptr;
+    s->staging_floats = 0;
+    MPM_CUDA(s, dalloc(&s->staging, floats));
+    s->staging_floats = floats;
+    return MPM_OK;
+}
+
+// Device SoA field -> host interleaved array in creation order.
+mpm_status export_field(mpm_solver* s, const float* soa, int comps, float* host) {
+    if (s->n == 0) return MPM_OK;
+    mpm_status st = ensure_staging(s, (size_t)s->n * comps);
+    if (st != MPM_OK) return st;
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_export_soa<<<blocks, threads, 0, s->stream>>>(soa, comps, s->n, s->id, s->staging);
+    MPM_CUDA(s, cudaGetLastError());
+    MPM_CUDA(s, cudaMemcpyAsync(host, s->staging, sizeof(float) * (size_t)s->n * comps, cudaMemcpyDeviceToHost, s->stream));
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+mpm_status import_field(mpm_solver* s, float* soa, int comps, const float* host) {
+    if (s->n == 0) return MPM_OK;
+    mpm_status st = ensure_staging(s, (size_t)s->n * comps);
+    if (st != MPM_OK) return st;
+    MPM_CUDA(s, cudaMemcpyAsync(s->staging, host, sizeof(float) * (size_t)s->n * comps, cudaMemcpyHostToDevice, s->stream));
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_import_soa<<<blocks, threads, 0, s->stream>>>(soa, comps, s->n, s->id, s->staging);
+    MPM_CUDA(s, cudaGetLastError());
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+uint64_t params_hash(const mpm_params& p) {
+    // FNV-1a over the knob bytes (the reserved tail excluded).
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&p);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < offsetof(mpm_params, reserved); ++i) { h ^= b[i]; h *= 1099511628211ull; }
+    return h;
+}
+
+}  // namespace
+
+namespace {
+const char* kStageNames[] = {"p2g", "grid_update", "g2p"};
+constexpr int kStages = 3;
+
+template <int D, int FORM> cudaError_t stage(mpm_solver* s, int k) {
+    if (k == 0) return launch_p2g<D, FORM>(s);
+    if (k == 1) return launch_grid<D, FORM>(s);
+    return launch_g2p<D, FORM>(s);
+}
+cudaError_t dispatch_stage(mpm_solver* s, int k) {
+    if (s->dim == 2) return s->form == kClassic ? stage<2, kClassic>(s, k) : stage<2, kMLS>(s, k);
+    return stage<3, kMLS>(s, k);
+}
+}  // namespace
+
+extern "C" {
+
+void mpm_params_default(mpm_params* out, int32_t dim) {
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    out->dim = dim == 3 ? 3 : 2;
+    out->width = 200;
+    out->height = 100;
+    out->depth = 100;
+    out->border_margin = 2;
+    out->formulation = MPM_FORMULATION_MLS;
+    out->boundary = MPM_BOUNDARY_FRICTION;
+    out->sort_period = 0;
+    out->delta_time = 1e-3f;
+    out->gravity = -9.81f;
+    out->friction = 0.3f;
+    out->theta_c = 2.0e-2f;
+    out->theta_s = 6.0e-3f;
+    out->xi = 10.f;
+    out->nu = 2.0e-1f;
+    out->youngs = 1.4e5f;
+    out->rho = 400.f;
+}
+
+const char* mpm_status_string(mpm_status status) {
+    const int i = (int)status;
+    if (i < 0 || i >= (int)(sizeof(kStatusText) / sizeof(kStatusText[0]))) return "unknown status";
+    return kStatusText[i];
+}
+
+mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, mpm_solver** out) {
+    if (!out) return MPM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    std::string why;
+    mpm_status st = validate(params, why);
+    if (st != MPM_OK) return st;
+    if (!init || init->count < 0 || init->count > 0x7fffffff) return MPM_ERR_INVALID_ARGUMENT;
+    if (init->count > 0 && (!init->position || !init->volume)) return MPM_ERR_INVALID_ARGUMENT;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return MPM_ERR_NO_DEVICE; }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_NO_DEVICE;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_grid_update<2, kMLS>) != cudaSuccess) { cudaGetLastError(); return MPM_ERR_NO_DEVICE; }
+
+    mpm_solver* s = new mpm_solver();
+    s->params = *params;
+    s->dim = params->dim;
+    s->form = params->formulation;
+    s->device = dev;
+    s->n = (int)init->count;
+    fill_consts(s);
+    s->nodes = s->C.nodes;
+    const int D = s->dim, n = s->n;
+
+    auto bail = [&](mpm_status code) { release(s); delete s; return code; };
+    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(MPM_ERR_CUDA);
+    s->stream = s->own_stream;
+    if (dalloc(&s->x, (size_t)n * D) || dalloc(&s->v, (size_t)n * D) || dalloc(&s->B, (size_t)n * D * D) ||
+        dalloc(&s->Fe, (size_t)n * D * D) || dalloc(&s->Jp, (size_t)n) || dalloc(&s->id, (size_t)n) ||
+        dalloc(&s->acc, (size_t)nacc(D, s->form) * s->nodes) || dalloc(&s->gv, (size_t)s->nodes * (D == 3 ? 2 : 1)) ||
+        dalloc(&s->status, 1)) {
+        cudaGetLastError();
+        return bail(MPM_ERR_OUT_OF_MEMORY);
+    }
+
+    // Host-side preparation: mass = vol * RHO / 100 when not given
+    // (src/cpu/Particles.cpp:18, src/gpu/GPUSolver.cpp:119,148).
+    std::vector<float> massv(n), volv(n);
+    double total_mass = 0.0;
+    bool uni_m = true, uni_v = true;
+    for (int i = 0; i < n; ++i) {
+        volv[i] = init->volume[i];
+        massv[i] = init->mass ? init->mass[i] : (init->volume[i] * params->rho) / 100.f;
+        if (!std::isfinite(volv[i]) || !std::isfinite(massv[i])) return bail(MPM_ERR_INVALID_ARGUMENT);
+        total_mass += massv[i];
+        if (massv[i] != massv[0]) uni_m = false;
+        if (volv[i] != volv[0]) uni_v = false;
+    }
+    for (long long i = 0; i < (long long)n * D; ++i)
+        if (!std::isfinite(init->position[i]) || (init->velocity && !std::isfinite(init->velocity[i])))
+            return bail(MPM_ERR_INVALID_ARGUMENT);
+    choose_scales(s, total_mass);
+    if (uni_m && n > 0) s->mass_u = massv[0];
+    else if (n > 0) {
+        if (dalloc(&s->mass, (size_t)n)) return bail(MPM_ERR_OUT_OF_MEMORY);
+        cudaMemcpy(s->mass, massv.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    }
+    if (uni_v && n > 0) s->vol_u = volv[0];
+    else if (n > 0) {
+        if (dalloc(&s->vol, (size_t)n)) return bail(MPM_ERR_OUT_OF_MEMORY);
+        cudaMemcpy(s->vol, volv.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    }
+
+    // SoA upload: F_E = I, B = 0, J_p = 1 (Particle ctor, src/cpu/Particles.cpp:7-19).
+    std::vector<float> soa((size_t)n * D * D);
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; ++i) ids[i] = i;
+    auto up = [&](float* dst, size_t count) {
+        return cudaMemcpy(dst, soa.data(), sizeof(float) * count, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    bool ok = true;
+    for (int k = 0; k < D; ++k)
+        for (int i = 0; i < n; ++i) soa[(size_t)k * n + i] = init->position[(size_t)i * D + k];
+    ok = ok && up(s->x, (size_t)n * D);
+    for (int k = 0; k < D; ++k)
+        for (int i = 0; i < n; ++i) soa[(size_t)k * n + i] = init->velocity ? init->velocity[(size_t)i * D + k] : 0.f;
+    ok = ok && up(s->v, (size_t)n * D);
+    std::fill(soa.begin(), soa.end(), 0.f);
+    ok = ok && up(s->B, (size_t)n * D * D);
+    for (int k = 0; k < D * D; ++k)
+        for (int i = 0; i < n; ++i) soa[(size_t)k * n + i] = (k % (D + 1) == 0) ? 1.f : 0.f;
+    ok = ok && up(s->Fe, (size_t)n * D * D);
+    for (int i = 0; i < n; ++i) soa[i] = 1.f;
+    ok = ok && up(s->Jp, (size_t)n);
+    ok = ok && cudaMemcpy(s->id, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && cudaMemset(s->acc, 0, sizeof(unsigned long long) * nacc(D, s->form) * s->nodes) == cudaSuccess;
+    ok = ok && cudaMemset(s->gv, 0, sizeof(float4) * s->nodes * (D == 3 ? 2 : 1)) == cudaSuccess;
+    ok = ok && cudaMemset(s->status, 0, sizeof(unsigned)) == cudaSuccess;
+    ok = ok && cudaDeviceSynchronize() == cudaSuccess;
+    if (!ok) { cudaGetLastError(); return bail(MPM_ERR_CUDA); }
+    *out = s;
+    return MPM_OK;
+}
+
+mpm_status mpm_destroy(mpm_solver* s) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    release(s);
+    delete s;
+    return MPM_OK;
+}
+
+mpm_status mpm_step(mpm_solver* s, int32_t nsteps) {
+    if (!s || nsteps < 0) return fail(s, MPM_ERR_INVALID_ARGUMENT, "nsteps must be >= 0");
+    for (int32_t k = 0; k < nsteps; ++k) {
+        cudaError_t e = dispatch_step(s);
+        if (e != cudaSuccess) return cuda_fail(s, e, "step launch");
+        ++s->step;
+    }
+    return MPM_OK;
+}
+
+
+int32_t mpm_stage_count(const mpm_solver*) { return kStages; }
+
+const char* mpm_stage_name(const mpm_solver*, int32_t k) {
+    return (k >= 0 && k < kStages) ? kStageNames[k] : "";
+}
+
+mpm_status mpm_step_profiled(mpm_solver* s, int32_t nsteps, double* stage_ms, int32_t nstages) {
+    if (!s || nsteps < 0 || (nstages > 0 && !stage_ms)) return MPM_ERR_INVALID_ARGUMENT;
+    cudaEvent_t ev[kStages + 1];
+    for (auto& e : ev) MPM_CUDA(s, cudaEventCreate(&e));
+    mpm_status st = MPM_OK;
+    for (int32_t it = 0; it < nsteps && st == MPM_OK; ++it) {
+        cudaError_t e = cudaEventRecord(ev[0], s->stream);
+        for (int k = 0; k < kStages && e == cudaSuccess; ++k) {
+            e = dispatch_stage(s, k);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[k + 1], s->stream);
+        }
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[kStages]);
+        if (e != cudaSuccess) { st = cuda_fail(s, e, "profiled step"); break; }
+        ++s->step;
+        for (int k = 0; k < kStages && k < nstages; ++k) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            stage_ms[k] += ms;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return st;
+}
+
+mpm_status mpm_get_info(const mpm_solver* s, int64_t* count, int32_t* dim) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    if (count) *count = s->n;
+    if (dim) *dim = s->dim;
+    return MPM_OK;
+}
+
+mpm_status mpm_get_positions(mpm_solver* s, float* out, size_t cap_floats) {
+    if (!s || (!out && s->n > 0)) return fail(s, MPM_ERR_INVALID_ARGUMENT, "out is NULL");
+    if (cap_floats < (size_t)s->n * s->dim) return fail(s, MPM_ERR_CAPACITY, "output capacity below count * dim");
+    return export_field(s, s->x, s->dim, out);
+}
+
+mpm_status mpm_get_state(mpm_solver* s, mpm_state_host* st) {
+    if (!s || !st) return MPM_ERR_INVALID_ARGUMENT;
+    if (st->count != s->n) return fail(s, MPM_ERR_CAPACITY, "state.count must equal the particle count");
+    const int D = s->dim;
+    mpm_status r = MPM_OK;
+    if (st->position && (r = export_field(s, s->x, D, st->position)) != MPM_OK) return r;
+    if (st->velocity && (r = export_field(s, s->v, D, st->velocity)) != MPM_OK) return r;
+    if (st->affine_b && (r = export_field(s, s->B, D * D, st->affine_b)) != MPM_OK) return r;
+    if (st->elastic_f && (r = export_field(s, s->Fe, D * D, st->elastic_f)) != MPM_OK) return r;
+    if (st->plastic_det && (r = export_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
+    return MPM_OK;
+}
+
+mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
+    if (!s || !st) return MPM_ERR_INVALID_ARGUMENT;
+    if (st->count != s->n) return fail(s, MPM_ERR_CAPACITY, "state.count must equal the particle count");
+    const int D = s->dim;
+    mpm_status r = MPM_OK;
+    if (st->position && (r = import_field(s, s->x, D, st->position)) != MPM_OK) return r;
+    if (st->velocity && (r = import_field(s, s->v, D, st->velocity)) != MPM_OK) return r;
+    if (st->affine_b && (r = import_field(s, s->B, D * D, st->affine_b)) != MPM_OK) return r;
+    if (st->elastic_f && (r = import_field(s, s->Fe, D * D, st->elastic_f)) != MPM_OK) return r;
+    if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
+    return MPM_OK;
+}
+
+mpm_status mpm_rasterize(mpm_solver* s, double* node_mass, double* node_momentum, int64_t* raw, size_t nodes) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    if (nodes != (size_t)s->nodes) return fail(s, MPM_ERR_CAPACITY, "nodes must equal the grid node count");
+    const int D = s->dim, NA = nacc(D, s->form);
+    cudaError_t e = dispatch_p2g(s);
+    if (e != cudaSuccess) return cuda_fail(s, e, "p2g launch");
+    std::vector<long long> h((size_t)NA * s->nodes);
+    MPM_CUDA(s, cudaMemcpyAsync(h.data(), s->acc, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost, s->stream));
+    MPM_CUDA(s, cudaMemsetAsync(s->acc, 0, sizeof(long long) * h.size(), s->stream));
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    const double ism = std::ldexp(1.0, -s->log2_sm), isp = std::ldexp(1.0, -s->log2_sp),
+                 isf = std::ldexp(1.0, -s->log2_sf);
+    const long long N = s->nodes;
+    for (long long i = 0; i < N; ++i) {
+        if (node_mass) node_mass[i] = (double)h[i] * ism;
+        for (int k = 0; k < D && node_momentum; ++k) {
+            double p = (double)h[(1 + k) * N + i] * isp;
+            if (s->form == kClassic) p -= (double)s->params.delta_time * ((double)h[(1 + D + k) * N + i] * isf);
+            node_momentum[i * D + k] = p;
+        }
+    }
+    if (raw) std::memcpy(raw, h.data(), sizeof(long long) * (size_t)(1 + D) * N);
+    return MPM_OK;
+}
+
+mpm_status mpm_get_status(mpm_solver* s, uint32_t* flags) {
+    if (!s || !flags) return MPM_ERR_INVALID_ARGUMENT;
+    unsigned h = 0;
+    MPM_CUDA(s, cudaMemcpyAsync(&h, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    *flags = h;
+    return MPM_OK;
+}
+
+mpm_status mpm_set_stream(mpm_solver* s, void* stream) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    s->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : s->own_stream;
+    return MPM_OK;
+}
+
+mpm_status mpm_get_step(const mpm_solver* s, int64_t* step) {
+    if (!s || !step) return MPM_ERR_INVALID_ARGUMENT;
+    *step = s->step;
+    return MPM_OK;
+}
+
+const char* mpm_last_error(const mpm_solver* s) { return s ? s->err.c_str() : "null solver"; }
+
+mpm_status mpm_get_fixed_point(const mpm_solver* s, int32_t* lm, int32_t* lp) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    if (lm) *lm = s->log2_sm;
+    if (lp) *lp = s->log2_sp;
+    return MPM_OK;
+}
+
+// Checkpoint: "MPMS" | u32 version=1 | i32 dim | i64 count | i32 W, H, D |
+// u64 params hash | i64 step | f32 x[n*d] v[n*d] B[n*d*d] Fe[n*d*d] Jp[n]
+mpm_status mpm_save_state(mpm_solver* s, const char* path) {
+    if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
+    const int D = s->dim;
+    const size_t n = (size_t)s->n;
+    std::vector<float> x(n * D), v(n * D), B(n * D * D), Fe(n * D * D), Jp(n);
+    mpm_state_host st{(int64_t)n, x.data(), v.data(), B.data(), Fe.data(), Jp.data()};
+    mpm_status r = mpm_get_state(s, &st);
+    if (r != MPM_OK) return r;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
+    const uint32_t ver = 1;
+    const int32_t dim = D, ext[3] = {s->params.width, s->params.height, D == 3 ? s->params.depth : 0};
+    const int64_t count = (int64_t)n, step = s->step;
+    const uint64_t h = params_hash(s->params);
+    bool ok = std::fwrite("MPMS", 1, 4, f) == 4 && std::fwrite(&ver, 4, 1, f) == 1 && std::fwrite(&dim, 4, 1, f) == 1 &&
+              std::fwrite(&count, 8, 1, f) == 1 && std::fwrite(ext, 4, 3, f) == 3 && std::fwrite(&h, 8, 1, f) == 1 &&
+              std::fwrite(&step, 8, 1, f) == 1;
+    for (auto* vec : {&x, &v, &B, &Fe, &Jp})
+        ok = ok && std::fwrite(vec->data(), sizeof(float), vec->size(), f) == vec->size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? MPM_OK : fail(s, MPM_ERR_IO, "short write");
+}
+
+mpm_status mpm_load_state(mpm_solver* s, const char* path) {
+    if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
+    char magic[4];
+    uint32_t ver = 0;
+    int32_t dim = 0, ext[3];
+    int64_t count = 0, step = 0;
+    uint64_t h = 0;
+    bool ok = std::fread(magic, 1, 4, f) == 4 && std::fread(&ver, 4, 1, f) == 1 && std::fread(&dim, 4, 1, f) == 1 &&
+              std::fread(&count, 8, 1, f) == 1 && std::fread(ext, 4, 3, f) == 3 && std::fread(&h, 8, 1, f) == 1 &&
+              std::fread(&step, 8, 1, f) == 1;
+    if (!ok || std::memcmp(magic, "MPMS", 4) != 0 || ver != 1) { std::fclose(f); return fail(s, MPM_ERR_IO, "not a checkpoint"); }
+    if (dim != s->dim || count != s->n || ext[0] != s->params.width || ext[1] != s->params.height ||
+        (dim == 3 && ext[2] != s->params.depth) || h != params_hash(s->params)) {
+        std::fclose(f);
+        return fail(s, MPM_ERR_STATE_MISMATCH, "checkpoint was written by a different configuration");
+    }
+    const int D = s->dim;
+    const size_t n = (size_t)count;
+    std::vector<float> x(n * D), v(n * D), B(n * D * D), Fe(n * D * D), Jp(n);
+    for (auto* vec : {&x, &v, &B, &Fe, &Jp}) ok = ok && std::fread(vec->data(), sizeof(float), vec->size(), f) == vec->size();
+    std::fclose(f);
+    if (!ok) return fail(s, MPM_ERR_IO, "truncated checkpoint");
+    mpm_state_host st{(int64_t)n, x.data(), v.data(), B.data(), Fe.data(), Jp.data()};
+    mpm_status r = mpm_set_state(s, &st);
+    if (r != MPM_OK) return r;
+    s->step = step;
+    return MPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,477 @@
+// Step kernels of the B200 MLS-MPM solver: P2G scatter, grid update, G2P with
+// plasticity, plus state import/export. Templated on the dimension D and the
+// formulation FORM (kMLS: the reference GPU shaders; kClassic: the reference
+// CPU path, 2D).
+//
+// HBM layout (structure of arrays, FP32, component-major with stride n):
+//   x[D][n], v[D][n], B[D*D][n], Fe[D*D][n], Jp[n]
+//   mass/vol: per particle or a uniform scalar (pointer == nullptr)
+// Grid (nodes = (W+1)(H+1)(D+1), x fastest):
+//   acc[NACC][nodes]  int64 fixed-point sums: mass, momentum[D] (+ force[D] CLASSIC)
+//   gv                node velocities for G2P: 2D float4 (vf.x, vf.y, vc.x, vc.y);
+//                     3D two float4 per node (vf.xyz, 0), (vc.xyz, 0)
+#pragma once
+
+#include "mpm_math.cuh"
+
+namespace mpm {
+
+struct StepConsts {
+    int W, H, Dp;             // cells per axis (WIDTH, HEIGHT, DEPTH)
+    int nx, ny, nz;           // nodes per axis
+    long long nodes;
+    float dt, gravity, friction, theta_c, theta_s, xi, mu0, la0, margin;
+    float sm, sp, sf;         // fixed-point scales: mass, momentum, force (powers of two)
+    float inv_sm, inv_sp, inv_sf;
+    float v_cap;              // |node velocity| above this means the momentum scale may have wrapped
+    int boundary;
+};
+
+struct Particles {
+    float* x;
+    float* v;
+    float* B;
+    float* Fe;
+    float* Jp;
+    const float* mass;  // nullptr: uniform mass_u
+    const float* vol;   // nullptr: uniform vol_u
+    float mass_u, vol_u;
+    int n;
+};
+
+template <int D, int FORM> struct Layout {
+    static constexpr int NACC = (FORM == kClassic) ? 1 + 2 * D : 1 + D;
+};
+
+__device__ __forceinline__ void raise_flag(unsigned* status, unsigned bit) {
+    atomicOr(status, bit);
+}
+
+// Largest magnitude one fixed-point contribution may take (2^62): leaves room
+// for partial sums; a node velocity above v_cap flags a possible wrap instead.
+constexpr float kFixedLimit = 4.611686e18f;
+
+__device__ __forceinline__ long long to_fixed(float val, float scale, unsigned* status) {
+    float t = val * scale;
+    if (!(fabsf(t) < kFixedLimit)) {
+        raise_flag(status, (t != t) ? 1u /*NAN*/ : 2u /*OVERFLOW*/);
+        t = (t != t) ? 0.f : copysignf(kFixedLimit, t);
+    }
+    return __float2ll_rn(t);
+}
+
+__device__ __forceinline__ void red_add(unsigned long long* p, long long v) {
+    if (v != 0) atomicAdd(p, (unsigned long long)v);
+}
+
+// First stencil node int(x) - 1 (C truncation, as int() in p2g.glsl:61 and
+// static_cast<int> in src/cpu/Grid.cpp:122). x is first clamped to
+// [-8, extent + 8] so that non-finite or far-away positions cannot overflow the
+// index arithmetic; their stencils then lie wholly outside the grid, as they
+// would in the reference.
+__device__ __forceinline__ int stencil_base(float x, int extent) {
+    return int(fminf(fmaxf(x, -8.f), float(extent) + 8.f)) - 1;
+}
+
+// ---------------------------------------------------------------------------
+// P2G, one thread per particle.
+// MLS (src/gpu/shaders/2d/p2g.glsl:29-92, 3d/p2g.glsl:31-96): per node
+//   m_i += w m_p
+//   p_i += w (m_p v_p + A_p (x_i - x_p)),  A_p = 3 m_p B_p - 3 dt V_p sigma_p
+// which is the shader's  m (v + 3 B (-dist)) + w V sigma dist 3 dt  regrouped.
+// CLASSIC (src/cpu/Grid.cpp:118-163): p_i += w m_p (v_p + 3 B_p (x_i - x_p)),
+//   f_i += A_p^T grad w (A_p = V_p sigma_p, glm row-vector product).
+// Sums are int64 fixed point (exact, order independent).
+template <int D, int FORM>
+__global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, unsigned long long* __restrict__ acc,
+                                                    unsigned* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    float x[D], v[D], B[D * D], Fe[D * D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
+    const float Jp = P.Jp[i];
+    const float mass = P.mass ? P.mass[i] : P.mass_u;
+    const float vol = P.vol ? P.vol[i] : P.vol_u;
+    if (FORM == kMLS && vol == 0.f) return;
+
+    float sig[D * D];
+    if (vol != 0.f) hardened_stress<D, FORM>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+    else {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) sig[k] = 0.f;
+    }
+    float A[D * D], mv[D];
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+        mv[r] = mass * v[r];
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            if (FORM == kMLS) A[r * D + c] = 3.f * mass * B[r * D + c] - 3.f * C.dt * vol * sig[r * D + c];
+            else A[r * D + c] = vol * sig[r * D + c];
+        }
+    }
+
+    const int ext[3] = {C.W, C.H, C.Dp};
+    int base[3] = {0, 0, 0};
+    float wk[3][4], dwk[3][4], off[3][4];  // off = x_i - x_p per axis
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        base[k] = stencil_base(x[k], ext[k]);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const float dist = x[k] - float(base[k] + o);
+            wk[k][o] = bspline_n(dist);
+            dwk[k][o] = (FORM == kClassic) ? bspline_dn(dist) : 0.f;
+            off[k][o] = -dist;
+        }
+    }
+    const int lim[3] = {C.W, C.H, C.Dp};
+    bool outside = false;
+    constexpr int NACC = Layout<D, FORM>::NACC;
+    const int nzs = (D == 3) ? 4 : 1;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int ix = base[0] + a;
+        if (ix < 0 || ix > lim[0]) { outside = true; continue; }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int iy = base[1] + b;
+            if (iy < 0 || iy > lim[1]) { outside = true; continue; }
+#pragma unroll
+            for (int c = 0; c < nzs; ++c) {
+                const int iz = (D == 3) ? base[2] + c : 0;
+                if (D == 3 && (iz < 0 || iz > lim[2])) { outside = true; continue; }
+                const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
+                const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
+                const float d[3] = {off[0][a], off[1][b], D == 3 ? off[2][c] : 0.f};
+                red_add(&acc[cid], to_fixed(w * mass, C.sm, status));
+                if (FORM == kMLS) {
+#pragma unroll
+                    for (int r = 0; r < D; ++r) {
+                        float s = mv[r];
+#pragma unroll
+                        for (int k = 0; k < D; ++k) s += A[r * D + k] * d[k];
+                        red_add(&acc[(1 + r) * C.nodes + cid], to_fixed(w * s, C.sp, status));
+                    }
+                } else {
+                    float dw[3];
+                    dw[0] = dwk[0][a] * wk[1][b];
+                    dw[1] = wk[0][a] * dwk[1][b];
+                    if (D == 3) { dw[0] *= wk[2][c]; dw[1] *= wk[2][c]; dw[2] = wk[0][a] * wk[1][b] * dwk[2][c]; }
+#pragma unroll
+                    for (int r = 0; r < D; ++r) {
+                        float bd = 0.f, f = 0.f;
+#pragma unroll
+                        for (int k = 0; k < D; ++k) { bd += B[r * D + k] * d[k]; f += dw[k] * A[k * D + r]; }
+                        red_add(&acc[(1 + r) * C.nodes + cid], to_fixed((w * mass) * (v[r] + 3.f * bd), C.sp, status));
+                        red_add(&acc[(1 + D + r) * C.nodes + cid], to_fixed(f, C.sf, status));
+                    }
+                }
+            }
+        }
+    }
+    (void)NACC;
+    if (outside) raise_flag(status, 4u);
+}
+
+// ---------------------------------------------------------------------------
+// Wall response on one node. MLS: src/gpu/shaders/2d/grid_update.glsl:17-80
+// (3D :19-86); CLASSIC: src/cpu/Grid.cpp:15-59 (same planes and order).
+template <int D, int FORM>
+__device__ __forceinline__ void collide(const StepConsts& C, const float* loc, const float* vel, float* vc, float* vf) {
+    const float w = float(C.W), h = float(C.H), dd = float(C.Dp), m = C.margin;
+    // plane point component along the normal's axis, normal sign, axis
+    float pp[6];
+    float ns[6];
+    int ax[6];
+    int nb;
+    if (D == 2) {
+        // right, bottom, left, top
+        pp[0] = w - m; ns[0] = -1.f; ax[0] = 0;
+        pp[1] = m;     ns[1] = 1.f;  ax[1] = 1;
+        pp[2] = m;     ns[2] = 1.f;  ax[2] = 0;
+        pp[3] = h - m; ns[3] = -1.f; ax[3] = 1;
+        nb = 4;
+    } else {
+        // +x, -x, +y, -y, +z, -z
+        pp[0] = w - m;  ns[0] = -1.f; ax[0] = 0;
+        pp[1] = m;      ns[1] = 1.f;  ax[1] = 0;
+        pp[2] = h - m;  ns[2] = -1.f; ax[2] = 1;
+        pp[3] = m;      ns[3] = 1.f;  ax[3] = 1;
+        pp[4] = dd - m; ns[4] = -1.f; ax[4] = 2;
+        pp[5] = m;      ns[5] = 1.f;  ax[5] = 2;
+        nb = 6;
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) vc[k] = vel[k];
+    int hit[6];
+    int nh = 0;
+#pragma unroll
+    for (int b = 0; b < nb; ++b) {
+        const int a = ax[b];
+        // n . (loc - P): only the normal's axis contributes (the other terms are 0 * x)
+        const float dist = ns[b] * (loc[a] - pp[b]);
+        const float test = ns[b] * ((loc[a] + C.dt * vc[a]) - pp[b]);
+        const float delta = test - fminf(dist, 0.f);
+        if (delta < 0.f) {
+            if (FORM == kClassic) vc[a] -= (delta * ns[b]) / C.dt;
+            else vc[a] -= (delta / C.dt) * ns[b];
+            hit[nh++] = b;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) vf[k] = vc[k];
+    for (int c = 0; c < nh; ++c) {
+        const int b = hit[c], a = ax[b];
+        // vt = vc - n (n . vf)
+        float vt[3];
+#pragma unroll
+        for (int k = 0; k < D; ++k) vt[k] = vc[k];
+        vt[a] = vc[a] - ns[b] * (ns[b] * vf[a]);
+        float vt2 = 0.f, dc2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < D; ++k) { vt2 += vt[k] * vt[k]; const float e = vc[k] - vel[k]; dc2 += e * e; }
+        const float vtn = sqrtf(vt2);
+        if (vtn <= 1e-7f) continue;
+        const float mag = fminf(vtn, C.friction * sqrtf(dc2));
+#pragma unroll
+        for (int k = 0; k < D; ++k) vf[k] -= mag * (vt[k] / vtn);
+    }
+}
+
+// Grid update, one thread per node (MLS: src/gpu/shaders/2d/grid_update.glsl:
+// 82-108, 3D :88-117; CLASSIC: src/cpu/Grid.cpp:165-184). Reads and clears the
+// fixed-point accumulators (the reference's separate reset pass,
+// reset.glsl:13-23, is fused here) and writes the velocities G2P gathers.
+template <int D, int FORM>
+__global__ void __launch_bounds__(256) k_grid_update(StepConsts C, unsigned long long* __restrict__ acc,
+                                                     float4* __restrict__ gv, unsigned* __restrict__ status) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= C.nodes) return;
+    constexpr int NACC = Layout<D, FORM>::NACC;
+    long long q[NACC];
+#pragma unroll
+    for (int c = 0; c < NACC; ++c) {
+        q[c] = (long long)acc[c * C.nodes + id];
+        if (q[c] != 0) acc[c * C.nodes + id] = 0ull;
+    }
+    float vc[3] = {0.f, 0.f, 0.f}, vf[3] = {0.f, 0.f, 0.f};
+    const float mass = __ll2float_rn(q[0]) * C.inv_sm;
+    if (mass >= 1e-6f) {
+        float vel[3] = {0.f, 0.f, 0.f};
+        if (FORM == kMLS) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) vel[k] = (__ll2float_rn(q[1 + k]) * C.inv_sp) / mass;
+            vel[1] += C.gravity * C.dt;
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const float vk = (__ll2float_rn(q[1 + k]) * C.inv_sp) / mass;
+                const float fk = (k == 1 ? C.gravity : 0.f) + (-(__ll2float_rn(q[1 + D + k]) * C.inv_sf) / mass);
+                vel[k] = vk + fk * C.dt;
+            }
+        }
+        float sp2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < D; ++k) sp2 += vel[k] * vel[k];
+        if (!(sp2 <= C.v_cap * C.v_cap)) raise_flag(status, (sp2 != sp2) ? 1u : 2u);
+        const long long ix = id % C.nx, iy = (id / C.nx) % C.ny, iz = id / ((long long)C.nx * C.ny);
+        const float loc[3] = {float(ix), float(iy), float(iz)};
+        if (C.boundary == kBoundarySticky) {
+            const int mm = int(C.margin);
+            const bool wall = ix < mm || ix > C.W - mm || iy < mm || iy > C.H - mm ||
+                              (D == 3 && (iz < mm || iz > C.Dp - mm));
+#pragma unroll
+            for (int k = 0; k < D; ++k) { vc[k] = wall ? 0.f : vel[k]; vf[k] = vc[k]; }
+        } else {
+            collide<D, FORM>(C, loc, vel, vc, vf);
+        }
+    }
+    if (D == 2) {
+        gv[id] = make_float4(vf[0], vf[1], vc[0], vc[1]);
+    } else {
+        gv[2 * id] = make_float4(vf[0], vf[1], vf[2], 0.f);
+        gv[2 * id + 1] = make_float4(vc[0], vc[1], vc[2], 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plasticity return map shared by every G2P variant (src/gpu/shaders/2d/
+// g2p.glsl:73-93, 3d/g2p.glsl:73-104, src/cpu/Particles.cpp:64-106):
+//   F_hat = (I + dt L) F_E;  U S V^T = svd(F_hat);  S' = max(clamp(S, 1-tc, 1+ts), 1e-6)
+//   F_E' = U S' V^T;  J_p' = J_p prod(S / S')  (= det of V diag(S/S') V^T F_P)
+// The FP32 SVD is recomputed in FP64 when F_hat is near-degenerate
+// (sigma_min^2 < 1e-2 sigma_max^2), where squaring in M^T M loses FP32 digits.
+template <int D, int FORM>
+__device__ __forceinline__ void plasticity(const StepConsts& C, const float* Fh, float* Fe_out, float& Jp,
+                                           unsigned* status) {
+    float U[D * D], S[D], V[D * D];
+    svd<D, FORM>(Fh, U, S, V);
+    float smin = fabsf(S[0]), smax = fabsf(S[0]);
+#pragma unroll
+    for (int k = 1; k < D; ++k) { smin = fminf(smin, fabsf(S[k])); smax = fmaxf(smax, fabsf(S[k])); }
+    if (!(smin * smin >= 1e-2f * smax * smax)) {
+        double Md[D * D], Ud[D * D], Sd[D], Vd[D * D];
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) Md[k] = double(Fh[k]);
+        svd<D, FORM, double>(Md, Ud, Sd, Vd);
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) { U[k] = float(Ud[k]); V[k] = float(Vd[k]); }
+#pragma unroll
+        for (int k = 0; k < D; ++k) S[k] = float(Sd[k]);
+        raise_flag(status, 8u);
+    }
+    const float t0 = 1.f - C.theta_c, t1 = 1.f + C.theta_s;
+    float ratio = 1.f, Sc[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        Sc[k] = fmaxf(fminf(fmaxf(S[k], t0), t1), 1e-6f);
+        ratio *= S[k] / Sc[k];
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += (U[r * D + k] * Sc[k]) * V[c * D + k];
+            Fe_out[r * D + c] = s;
+        }
+    Jp *= ratio;
+}
+
+// G2P + APIC + plasticity, one thread per particle (MLS: src/gpu/shaders/2d/
+// g2p.glsl:21-93, 3d/g2p.glsl:22-104; CLASSIC: src/cpu/Particles.cpp:133-216).
+// The new position  sum w (x_i + dt v_col)  is evaluated as
+// x_p * sum(w) + sum w ((x_i - x_p) + dt v_col), with sum(w) taken as exactly 1
+// when the whole stencil lies inside the grid (partition of unity): the same
+// value in exact arithmetic, without rounding node coordinates of O(W) into
+// every term. Where the reference skipped out-of-grid nodes the partial weight
+// sum is kept, as there.
+template <int D, int FORM>
+__global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, const float4* __restrict__ gv,
+                                                    unsigned* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
+    const int ext[3] = {C.W, C.H, C.Dp};
+    int base[3] = {0, 0, 0};
+    float wk[3][4], dwk[3][4], off[3][4];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        base[k] = stencil_base(x[k], ext[k]);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const float dist = x[k] - float(base[k] + o);
+            wk[k][o] = bspline_n(dist);
+            dwk[k][o] = (FORM == kClassic) ? bspline_dn(dist) : 0.f;
+            off[k][o] = -dist;
+        }
+    }
+    float nv[D], nx[D], nB[D * D], gvel[D * D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) { nv[k] = 0.f; nx[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) { nB[k] = 0.f; gvel[k] = 0.f; }
+    const int lim[3] = {C.W, C.H, C.Dp};
+    const int nzs = (D == 3) ? 4 : 1;
+    float wsum = 0.f;
+    bool clipped = false;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int ix = base[0] + a;
+        if (ix < 0 || ix > lim[0]) { clipped = true; continue; }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int iy = base[1] + b;
+            if (iy < 0 || iy > lim[1]) { clipped = true; continue; }
+#pragma unroll
+            for (int c = 0; c < nzs; ++c) {
+                const int iz = (D == 3) ? base[2] + c : 0;
+                if (D == 3 && (iz < 0 || iz > lim[2])) { clipped = true; continue; }
+                const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
+                const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
+                const float d[3] = {off[0][a], off[1][b], D == 3 ? off[2][c] : 0.f};
+                wsum += w;
+                float vf[3], vc[3];
+                if (D == 2) {
+                    const float4 g = gv[cid];
+                    vf[0] = g.x; vf[1] = g.y; vc[0] = g.z; vc[1] = g.w;
+                } else {
+                    const float4 g0 = gv[2 * cid], g1 = gv[2 * cid + 1];
+                    vf[0] = g0.x; vf[1] = g0.y; vf[2] = g0.z; vc[0] = g1.x; vc[1] = g1.y; vc[2] = g1.z;
+                }
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    nv[r] += vf[r] * w;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) nB[r * D + k] += w * (vf[r] * d[k]);
+                    nx[r] += (d[r] + C.dt * vc[r]) * w;
+                }
+                if (FORM == kClassic) {
+                    float dw[3];
+                    dw[0] = dwk[0][a] * wk[1][b];
+                    dw[1] = wk[0][a] * dwk[1][b];
+                    if (D == 3) { dw[0] *= wk[2][c]; dw[1] *= wk[2][c]; dw[2] = wk[0][a] * wk[1][b] * dwk[2][c]; }
+#pragma unroll
+                    for (int r = 0; r < D; ++r)
+#pragma unroll
+                        for (int k = 0; k < D; ++k) gvel[r * D + k] += vc[r] * dw[k];
+                }
+            }
+        }
+    }
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const float xn = (clipped ? x[k] * wsum : x[k]) + nx[k];
+        P.v[k * n + i] = nv[k];
+        P.x[k * n + i] = xn;
+        finite = finite && isfinite(xn);
+    }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.B[k * n + i] = nB[k];
+
+    float Fe[D * D], A[D * D], Fh[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) {
+        Fe[k] = P.Fe[k * n + i];
+        const float L = (FORM == kMLS) ? 3.f * nB[k] : gvel[k];
+        A[k] = ((k % (D + 1)) == 0 ? 1.f : 0.f) + C.dt * L;
+    }
+    matmul<D>(A, Fe, Fh);
+    float Jp = P.Jp[i];
+    plasticity<D, FORM>(C, Fh, Fe, Jp, status);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
+    P.Jp[i] = Jp;
+    if (!finite || !isfinite(Jp)) raise_flag(status, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Import / export between the caller's interleaved per-particle arrays (in
+// creation order) and the device SoA (in slot order; slot s holds particle id[s]).
+__global__ void k_export_soa(const float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
+                             float* __restrict__ aos) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int p = id ? id[s] : s;
+    for (int c = 0; c < comps; ++c) aos[(long long)p * comps + c] = soa[(long long)c * n + s];
+}
+
+__global__ void k_import_soa(float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
+                             const float* __restrict__ aos) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int p = id ? id[s] : s;
+    for (int c = 0; c < comps; ++c) soa[(long long)c * n + s] = aos[(long long)p * comps + c];
+}
+
+}  // namespace mpm

@@ -1,0 +1,252 @@
+// Device math of the MLS-MPM step: cubic B-spline weights, the reference's
+// SVD variants, polar rotation and the hardened stress. FP32 in the hot path;
+// the same templates instantiate in FP64 for the near-degenerate SVD branch.
+//
+// Matrices are row-major dim x dim register arrays (M[r*D+c]).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpm {
+
+enum : int { kMLS = 0, kClassic = 1 };
+enum : int { kBoundaryFriction = 0, kBoundarySticky = 1 };
+
+// Cubic B-spline N(x) and dN/dx with support |x| < 2:
+// src/gpu/shaders/2d/common.glsl:43-69 (src/cpu/Grid.h:86-116). pow(a, 3.0)
+// is evaluated as a product.
+template <typename R> __device__ __forceinline__ R bspline_n(R x) {
+    R a = fabs(x);
+    if (a < R(1)) return R(0.5) * a * a * a - a * a + R(2) / R(3);
+    if (a < R(2)) { R t = R(2) - a; return t * t * t / R(6); }
+    return R(0);
+}
+template <typename R> __device__ __forceinline__ R bspline_dn(R x) {
+    R a = fabs(x);
+    if (a < R(1)) return R(1.5) * a * x - R(2) * x;
+    if (a < R(2)) return R(-0.5) * a * x + R(2) * x - (R(2) * x) / a;
+    return R(0);
+}
+
+template <int D, typename R> __device__ __forceinline__ R det(const R* A) {
+    if (D == 2) return A[0] * A[3] - A[1] * A[2];
+    return A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+           A[2] * (A[3] * A[7] - A[4] * A[6]);
+}
+
+template <int D, typename R> __device__ __forceinline__ void matmul(const R* A, const R* B, R* C) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            R s = R(0);
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += A[i * D + k] * B[k * D + j];
+            C[i * D + j] = s;
+        }
+}
+
+// 2x2 SVD by one analytic Jacobi rotation of M^T M (src/gpu/shaders/2d/
+// common.glsl:2-37). A reflection is folded into the sign of S[1].
+template <typename R> __device__ __forceinline__ void svd2_glsl(const R* M, R* U, R* S, R* V) {
+    const R a = M[0] * M[0] + M[2] * M[2];
+    const R b = M[0] * M[1] + M[2] * M[3];
+    const R d = M[1] * M[1] + M[3] * M[3];
+    const R theta = (fabs(b) < R(1e-10) && fabs(a - d) < R(1e-10)) ? R(0) : R(0.5) * atan2(R(2) * b, a - d);
+    R st, ct;
+    st = sin(theta);
+    ct = cos(theta);
+    V[0] = ct; V[1] = -st; V[2] = st; V[3] = ct;
+    // diag(V^T (M^T M) V)
+    const R d0 = ct * (a * ct + b * st) + st * (b * ct + d * st);
+    const R d1 = -st * (-a * st + b * ct) + ct * (-b * st + d * ct);
+    S[0] = sqrt(fmax(d0, R(1e-12)));
+    S[1] = sqrt(fmax(d1, R(1e-12)));
+    const R i0 = R(1) / S[0], i1 = R(1) / S[1];
+    U[0] = (M[0] * V[0] + M[1] * V[2]) * i0;
+    U[1] = (M[0] * V[1] + M[1] * V[3]) * i1;
+    U[2] = (M[2] * V[0] + M[3] * V[2]) * i0;
+    U[3] = (M[2] * V[1] + M[3] * V[3]) * i1;
+    if (U[0] * U[3] - U[1] * U[2] < R(0)) { U[1] = -U[1]; U[3] = -U[3]; S[1] = -S[1]; }
+}
+
+// 2x2 SVD with the conventions of Eigen 3.4 JacobiSVD (singular values >= 0,
+// descending), the decomposition the reference CPU path uses
+// (src/cpu/Particles.cpp:31-32,73-78). Two-sided Jacobi as published in
+// Eigen/src/SVD/JacobiSVD.h:666-780 and Eigen/src/misc/RealSvd2x2.h:18-49.
+template <typename R> __device__ __forceinline__ void svd2_eigen(const R* A, R* U, R* S, R* V) {
+    const R eps = sizeof(R) == 4 ? R(1.1920928955078125e-07) : R(2.220446049250313e-16);
+    const R tiny = sizeof(R) == 4 ? R(1.1754943508222875e-38) : R(2.2250738585072014e-308);
+    R scale = fmax(fmax(fabs(A[0]), fabs(A[1])), fmax(fabs(A[2]), fabs(A[3])));
+    U[0] = R(1); U[1] = R(0); U[2] = R(0); U[3] = R(1);
+    V[0] = R(1); V[1] = R(0); V[2] = R(0); V[3] = R(1);
+    if (!isfinite(scale)) { S[0] = S[1] = scale - scale; return; }
+    if (scale == R(0)) scale = R(1);
+    R w[4] = {A[0] / scale, A[1] / scale, A[2] / scale, A[3] / scale};
+    R maxd = fmax(fabs(w[0]), fabs(w[3]));
+    for (int it = 0; it < 8; ++it) {
+        const R thr = fmax(tiny, R(2) * eps * maxd);
+        if (!(fabs(w[2]) > thr || fabs(w[1]) > thr)) break;
+        // (p, q) = (1, 0): sub-block m = [[w11, w10], [w01, w00]]
+        R m0 = w[3], m1 = w[2], m2 = w[1], m3 = w[0];
+        const R t = m0 + m3, dd = m2 - m1;
+        R c1 = R(1), s1 = R(0);
+        if (!(fabs(dd) < tiny)) { const R u = t / dd, tmp = sqrt(R(1) + u * u); c1 = u / tmp; s1 = R(1) / tmp; }
+        {   // rows 0,1 of m by rot1
+            R x0 = m0, x1 = m1, y0 = m2, y1 = m3;
+            m0 = c1 * x0 + s1 * y0; m1 = c1 * x1 + s1 * y1;
+            m2 = -s1 * x0 + c1 * y0; m3 = -s1 * x1 + c1 * y1;
+        }
+        R cr = R(1), sr = R(0);
+        const R deno = R(2) * fabs(m1);
+        if (!(deno < tiny)) {
+            const R tau = (m0 - m3) / deno, ww = sqrt(tau * tau + R(1));
+            const R tt = tau > R(0) ? R(1) / (tau + ww) : R(1) / (tau - ww);
+            const R sg = tt > R(0) ? R(1) : R(-1), n = R(1) / sqrt(tt * tt + R(1));
+            cr = n;
+            sr = -sg * (m1 / fabs(m1)) * fabs(tt) * n;
+        }
+        // j_left = rot1 * j_right^T
+        const R cl = c1 * cr - s1 * (-sr), sl = c1 * (-sr) + s1 * cr;
+        {   // w rows (1, 0) by j_left: x = row1, y = row0
+            R x0 = w[2], x1 = w[3], y0 = w[0], y1 = w[1];
+            w[2] = cl * x0 + sl * y0; w[3] = cl * x1 + sl * y1;
+            w[0] = -sl * x0 + cl * y0; w[1] = -sl * x1 + cl * y1;
+        }
+        {   // U columns (1, 0) by j_left (applyOnTheRight with j_left^T)
+            R x0 = U[1], x1 = U[3], y0 = U[0], y1 = U[2];
+            U[1] = cl * x0 + sl * y0; U[3] = cl * x1 + sl * y1;
+            U[0] = -sl * x0 + cl * y0; U[2] = -sl * x1 + cl * y1;
+        }
+        {   // w and V columns (1, 0) by j_right^T
+            R x0 = w[1], x1 = w[3], y0 = w[0], y1 = w[2];
+            w[1] = cr * x0 - sr * y0; w[3] = cr * x1 - sr * y1;
+            w[0] = sr * x0 + cr * y0; w[2] = sr * x1 + cr * y1;
+            x0 = V[1]; x1 = V[3]; y0 = V[0]; y1 = V[2];
+            V[1] = cr * x0 - sr * y0; V[3] = cr * x1 - sr * y1;
+            V[0] = sr * x0 + cr * y0; V[2] = sr * x1 + cr * y1;
+        }
+        maxd = fmax(maxd, fmax(fabs(w[3]), fabs(w[0])));
+    }
+    S[0] = fabs(w[0]);
+    S[1] = fabs(w[3]);
+    if (w[0] < R(0)) { U[0] = -U[0]; U[2] = -U[2]; }
+    if (w[3] < R(0)) { U[1] = -U[1]; U[3] = -U[3]; }
+    S[0] *= scale;
+    S[1] *= scale;
+    if (S[1] > S[0]) {
+        R t = S[0]; S[0] = S[1]; S[1] = t;
+        t = U[0]; U[0] = U[1]; U[1] = t; t = U[2]; U[2] = U[3]; U[3] = t;
+        t = V[0]; V[0] = V[1]; V[1] = t; t = V[2]; V[2] = V[3]; V[3] = t;
+    }
+}
+
+// 3x3 SVD of src/gpu/shaders/3d/common.glsl:8-105: cyclic Jacobi on
+// S = M^T M over the pairs (0,1), (0,2), (1,2); U = M V Sigma^-1, reflection
+// folded into Sigma[2]. The reference runs 6 fixed sweeps; here the iteration
+// stops after the first sweep that leaves the off-diagonal of S below 2 eps of
+// its diagonal (further rotations then only move rounding noise around), with
+// 6 sweeps as the bound.
+template <typename R> __device__ __forceinline__ void schur2(R app, R apq, R aqq, R& c, R& s) {
+    if (fabs(apq) < R(1e-10)) { c = R(1); s = R(0); return; }
+    const R tau = (aqq - app) / (R(2) * apq);
+    const R stt = sqrt(R(1) + tau * tau);
+    R tn = R(1) / (fabs(tau) + stt);
+    if (tau < R(0)) tn = -tn;
+    c = R(1) / sqrt(R(1) + tn * tn);
+    s = tn * c;
+}
+
+template <int P, int Q, typename R> __device__ __forceinline__ void jacobi_step(R* S, R* V) {
+    constexpr int O = 3 - P - Q;  // the third index
+    R c, s;
+    schur2(S[P * 3 + P], S[P * 3 + Q], S[Q * 3 + Q], c, s);
+    const R Spp = S[P * 3 + P], Sqq = S[Q * 3 + Q], Spq = S[P * 3 + Q];
+    S[P * 3 + P] = c * c * Spp - R(2) * s * c * Spq + s * s * Sqq;
+    S[Q * 3 + Q] = s * s * Spp + R(2) * s * c * Spq + c * c * Sqq;
+    S[P * 3 + Q] = R(0);
+    S[Q * 3 + P] = R(0);
+    const R Sop = S[O * 3 + P], Soq = S[O * 3 + Q];
+    S[O * 3 + P] = c * Sop - s * Soq;
+    S[P * 3 + O] = S[O * 3 + P];
+    S[O * 3 + Q] = s * Sop + c * Soq;
+    S[Q * 3 + O] = S[O * 3 + Q];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const R vp = V[r * 3 + P], vq = V[r * 3 + Q];
+        V[r * 3 + P] = c * vp - s * vq;
+        V[r * 3 + Q] = s * vp + c * vq;
+    }
+}
+
+template <typename R> __device__ __forceinline__ void svd3_glsl(const R* M, R* U, R* Sig, R* V) {
+    R S[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) S[i * 3 + j] = M[0 * 3 + i] * M[0 * 3 + j] + M[1 * 3 + i] * M[1 * 3 + j] + M[2 * 3 + i] * M[2 * 3 + j];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? R(1) : R(0);
+    const R tol = sizeof(R) == 4 ? R(2.4e-7) : R(4.5e-16);  // 2 eps
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        jacobi_step<0, 1>(S, V);
+        jacobi_step<0, 2>(S, V);
+        jacobi_step<1, 2>(S, V);
+        const R off = S[1] * S[1] + S[2] * S[2] + S[5] * S[5];
+        const R dia = S[0] * S[0] + S[4] * S[4] + S[8] * S[8];
+        if (off <= tol * tol * dia) break;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Sig[i] = sqrt(fmax(S[i * 4], R(1e-12)));
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            U[r * 3 + c] = (M[r * 3 + 0] * V[0 * 3 + c] + M[r * 3 + 1] * V[1 * 3 + c] + M[r * 3 + 2] * V[2 * 3 + c]) * (R(1) / Sig[c]);
+    if (det<3>(U) < R(0)) { U[2] = -U[2]; U[5] = -U[5]; U[8] = -U[8]; Sig[2] = -Sig[2]; }
+}
+
+template <int D, int FORM, typename R> __device__ __forceinline__ void svd(const R* M, R* U, R* S, R* V) {
+    if constexpr (D == 2) {
+        if constexpr (FORM == kClassic) svd2_eigen(M, U, S, V);
+        else svd2_glsl(M, U, S, V);
+    } else {
+        svd3_glsl(M, U, S, V);
+    }
+}
+
+// Polar rotation R = U V^T of F_E and the hardened stress
+// sigma = 2 mu (F_E - R) F_E^T + lambda (J_e - 1) J_e I,
+// mu = MU exp(XI (1 - J_p)), lambda = LAMBDA exp(XI (1 - J_p))
+// (src/gpu/shaders/2d/p2g.glsl:44-59, 3d/p2g.glsl:46-61, src/cpu/Particles.cpp:21-48).
+template <int D, int FORM> __device__ __forceinline__ void hardened_stress(const float* Fe, float Jp, float mu0,
+                                                                          float la0, float xi, float* sig) {
+    float U[D * D], S[D], V[D * D];
+    svd<D, FORM>(Fe, U, S, V);
+    float Rm[D * D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += U[i * D + k] * V[j * D + k];
+            Rm[i * D + j] = s;
+        }
+    const float Je = det<D>(Fe);
+    const float h = expf(xi * (1.f - Jp));
+    const float mu = mu0 * h, la = la0 * h;
+    const float diag = la * (Je - 1.f) * Je;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += (Fe[i * D + k] - Rm[i * D + k]) * Fe[j * D + k];
+            sig[i * D + j] = 2.f * mu * s + (i == j ? diag : 0.f);
+        }
+}
+
+}  // namespace mpm

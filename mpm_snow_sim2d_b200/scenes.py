@@ -1,0 +1,210 @@
+"""Seeded snow scenes in the reference's grid units.
+
+The workloads are stated on the unit square / cube with cell size dx = 1/W.
+The reference integrates in grid units (node i at x = i, src/cpu/Grid.cpp:
+10-14; p2g.glsl:73), so a physical scene maps as
+    x~ = x / dx,  v~ = v / dx,  GRAVITY = g / dx,
+    volume~ = 1 / ppc (cell fractions),  RHO~ = rho * dx^2 * 100,
+which makes mass~ = volume~ * RHO~ / 100 = rho dx^2 / ppc. With these the
+reference's grid-unit force term  V~ sigma (x_p - x_i) 3 dt  and momentum
+m~ v~ keep the physical ratio 1 / (rho dx^2) in 2D and 3D alike, so the
+scaled step is the physical step divided by dx. E, nu, theta_c, theta_s, xi
+and dt are unchanged.
+
+The reference samples with std::random_device (src/shared/Shapes.h:23,150),
+which is not reproducible; here every scene draws from numpy's PCG64 with a
+fixed seed, and the CUDA solver and the oracles consume the same arrays.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+
+from ._lib import BOUNDARY_FRICTION, FORMULATION_MLS
+
+
+@dataclass
+class Scene:
+    name: str
+    dim: int
+    width: int
+    height: int
+    depth: int
+    border_margin: int
+    delta_time: float
+    gravity: float
+    friction: float
+    theta_c: float
+    theta_s: float
+    xi: float
+    nu: float
+    youngs: float
+    rho: float
+    steps: int
+    position: np.ndarray          # (n, dim) float32, grid units
+    velocity: np.ndarray          # (n, dim) float32, grid units / s
+    volume: np.ndarray            # (n,) float32
+    mass: np.ndarray              # (n,) float32
+    formulation: int = FORMULATION_MLS
+    boundary: int = BOUNDARY_FRICTION
+    info: dict = field(default_factory=dict)
+
+    @property
+    def count(self) -> int:
+        return int(self.position.shape[0])
+
+    @property
+    def nodes(self) -> int:
+        n = (self.width + 1) * (self.height + 1)
+        return n * (self.depth + 1) if self.dim == 3 else n
+
+    def with_(self, **kw) -> "Scene":
+        return replace(self, **kw)
+
+
+# Snow material of the workloads (E, nu, rho, xi, theta_c, theta_s).
+MATERIAL = dict(youngs=1.4e5, nu=0.2, rho_phys=400.0, xi=10.0, theta_c=2.5e-2, theta_s=7.5e-3)
+FRICTION = 0.3  # Parameters.h:60
+MARGIN = 3
+
+
+def _scene(name, dim, W, dt, steps, pos_phys, vel_phys, ppc, rng_info, *, depth=None, g=-9.8,
+           youngs=MATERIAL["youngs"], nu=MATERIAL["nu"]) -> Scene:
+    dx = 1.0 / W
+    n = pos_phys.shape[0]
+    vol = np.full(n, 1.0 / ppc, dtype=np.float32)
+    rho_ref = MATERIAL["rho_phys"] * dx * dx * 100.0
+    mass = (vol * np.float32(rho_ref)) / np.float32(100.0)  # Particle ctor: vol * RHO / 100
+    return Scene(
+        name=name, dim=dim, width=W, height=W, depth=(depth or W) if dim == 3 else 0,
+        border_margin=MARGIN, delta_time=dt, gravity=g / dx, friction=FRICTION,
+        theta_c=MATERIAL["theta_c"], theta_s=MATERIAL["theta_s"], xi=MATERIAL["xi"],
+        nu=nu, youngs=youngs, rho=rho_ref, steps=steps,
+        position=np.ascontiguousarray((pos_phys / dx).astype(np.float32)),
+        velocity=np.ascontiguousarray((vel_phys / dx).astype(np.float32)),
+        volume=vol, mass=mass.astype(np.float32), info=dict(rng_info, dx=dx, ppc=ppc),
+    )
+
+
+def _box(rng, lo, hi, ppc, dx):
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    count = int(round(np.prod(hi - lo) / dx ** len(lo) * ppc))
+    return lo + rng.random((count, len(lo))) * (hi - lo)
+
+
+def _ball(rng, center, radius, ppc, dx):
+    center = np.asarray(center, np.float64)
+    d = len(center)
+    vol = (np.pi * radius ** 2) if d == 2 else (4.0 / 3.0 * np.pi * radius ** 3)
+    count = int(round(vol / dx ** d * ppc))
+    out = np.empty((0, d))
+    while out.shape[0] < count:
+        cand = rng.random((2 * count, d)) * 2.0 - 1.0
+        cand = cand[(cand ** 2).sum(1) <= 1.0]
+        out = np.concatenate([out, center + radius * cand])
+    return out[:count]
+
+
+def snow_blocks_2d(ppc: int = 4, seed: int = 1001, steps: int = 1000) -> Scene:
+    """Three axis-aligned snow blocks of side 0.15 on a 128^2 grid, dt 1e-4."""
+    W, dx = 128, 1.0 / 128
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = [_box(rng, np.array(c) - 0.075, np.array(c) + 0.075, ppc, dx) for c in ((0.3, 0.6), (0.5, 0.8), (0.7, 0.6))]
+    pos = np.concatenate(pts)
+    vel = np.array([0.0, -1.0]) + rng.uniform(-0.1, 0.1, pos.shape)
+    return _scene(f"blocks2d_128_ppc{ppc}", 2, W, 1e-4, steps, pos, vel, ppc, dict(seed=seed))
+
+
+def impact_2d(W: int = 128, ppc: int = 2, seed: int = 1011, steps: int = 400, dt: float = 1e-4) -> Scene:
+    """One block (side 0.2) thrown at the floor with v = (0.5, -4): wall
+    separation, Coulomb friction and plastic flow within a few hundred steps."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pos = _box(rng, (0.4, 0.06), (0.6, 0.26), ppc, dx)
+    vel = np.array([0.5, -4.0]) + rng.uniform(-0.05, 0.05, pos.shape)
+    return _scene(f"impact2d_{W}_ppc{ppc}", 2, W, dt, steps, pos, vel, ppc, dict(seed=seed))
+
+
+def impact_3d(W: int = 32, ppc: int = 2, seed: int = 1013, steps: int = 300, dt: float = 1e-4) -> Scene:
+    """A snowball dropped onto a slab at 4 m/s on a small grid (contact within ~50 steps)."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ball = _ball(rng, (0.5, 0.45, 0.5), 0.15, ppc, dx)
+    m = MARGIN * dx
+    slab = _box(rng, (m, m, m), (1.0 - m, m + 0.2, 1.0 - m), ppc, dx)
+    pos = np.concatenate([ball, slab])
+    vel = np.zeros_like(pos)
+    vel[: ball.shape[0], 1] = -4.0
+    vel[: ball.shape[0], 0] = 0.5
+    return _scene(f"impact3d_{W}_ppc{ppc}", 3, W, dt, steps, pos, vel, ppc, dict(seed=seed))
+
+
+def random_blocks_2d(W: int = 512, nblocks: int = 8, ppc: int = 8, seed: int = 1002, steps: int = 2000,
+                     dt: float = 2.5e-5, side=(0.05, 0.2)) -> Scene:
+    """Non-overlapping square blocks of random side placed by rejection."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lo_wall, hi_wall = (MARGIN + 2) * dx, 1.0 - (MARGIN + 2) * dx
+    boxes = []
+    tries = 0
+    while len(boxes) < nblocks:
+        tries += 1
+        if tries > 100000:
+            raise RuntimeError("could not place the blocks without overlap")
+        s = rng.uniform(*side)
+        c = rng.uniform(lo_wall + s / 2, hi_wall - s / 2, 2)
+        lo, hi = c - s / 2, c + s / 2
+        if all(np.any(hi <= b_lo) or np.any(lo >= b_hi) for b_lo, b_hi in boxes):
+            boxes.append((lo, hi))
+    pos = np.concatenate([_box(rng, lo, hi, ppc, dx) for lo, hi in boxes])
+    vel = np.array([0.0, -1.0]) + rng.uniform(-0.1, 0.1, pos.shape)
+    return _scene(f"randblocks2d_{W}_ppc{ppc}", 2, W, dt, steps, pos, vel, ppc,
+                  dict(seed=seed, blocks=[(lo.tolist(), hi.tolist()) for lo, hi in boxes]))
+
+
+def snowball_on_slab_3d(W: int = 128, ppc: int = 8, seed: int = 1003, steps: int = 1000, dt: float = 5e-5,
+                        radius: float = 0.12, slab: float = 0.1) -> Scene:
+    """A snowball (r 0.12, centre (0.5, 0.7, 0.5), v (0, -3, 0)) above a 0.1-thick slab on the floor."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ball = _ball(rng, (0.5, 0.7, 0.5), radius, ppc, dx)
+    m = MARGIN * dx
+    slab_pts = _box(rng, (m, m, m), (1.0 - m, m + slab, 1.0 - m), ppc, dx)
+    pos = np.concatenate([ball, slab_pts])
+    vel = np.zeros_like(pos)
+    vel[: ball.shape[0], 1] = -3.0
+    return _scene(f"snowball_slab3d_{W}_ppc{ppc}", 3, W, dt, steps, pos, vel, ppc,
+                  dict(seed=seed, ball_particles=int(ball.shape[0])))
+
+
+def two_snowballs_3d(W: int = 256, ppc: int = 8, seed: int = 1005, steps: int = 1000, dt: float = 5e-5,
+                     radius: float = 0.15, speed: float = 6.0) -> Scene:
+    """Two snowballs (r 0.15) colliding head-on along x at relative speed 6."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = _ball(rng, (0.32, 0.5, 0.5), radius, ppc, dx)
+    b = _ball(rng, (0.68, 0.5, 0.5), radius, ppc, dx)
+    pos = np.concatenate([a, b])
+    vel = np.zeros_like(pos)
+    vel[: a.shape[0], 0] = speed / 2
+    vel[a.shape[0]:, 0] = -speed / 2
+    return _scene(f"two_snowballs3d_{W}_ppc{ppc}", 3, W, dt, steps, pos, vel, ppc, dict(seed=seed))
+
+
+def workload(name: str) -> Scene:
+    """The named workloads: c1..c5 with the sizes stated for them."""
+    if name == "c1":
+        return snow_blocks_2d()
+    if name == "c1_22k":
+        return snow_blocks_2d(ppc=20)
+    if name == "c2":
+        return random_blocks_2d()
+    if name == "c2_1m":
+        return random_blocks_2d(ppc=27)
+    if name == "c3":
+        return snowball_on_slab_3d()
+    if name == "c5":
+        return two_snowballs_3d()
+    raise KeyError(name)

@@ -1,0 +1,252 @@
+"""GPU parity: the CUDA solver, called through the C ABI, against the FP64
+oracle (MLS, 2D and 3D) and against the reference's own CPU code (CLASSIC,
+golden fixtures), plus determinism, conservation and the API contract.
+
+Tolerances are relative L2 norms over all particles (B normalised by the
+velocity norm, see conftest.state_errors). The workload target is 1e-4 after
+1000 steps; short horizons are held much tighter."""
+import numpy as np
+import pytest
+
+from conftest import state_errors
+from golden_io import load_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_ref(O, scene, steps, formulation=None):
+    st = O.initial_state(scene)
+    out, prev = {}, 0
+    for s in steps:
+        O.run_oracle(scene, st, s - prev, formulation=formulation)
+        prev = s
+        out[s] = dict(position=st.position.copy(), velocity=st.velocity.copy(), affine_b=st.affine_b.copy(),
+                      elastic_f=st.elastic_f.copy(), plastic_det=st.plastic_det.copy())
+    return out
+
+
+def _gpu_run(scene, steps, **kw):
+    from mpm_snow_sim2d_b200 import Solver
+    out, prev = {}, 0
+    with Solver.from_scene(scene, **kw) as s:
+        for st in steps:
+            s.Step(st - prev)
+            prev = st
+            out[st] = s.get_state()
+        flags = s.status()
+    return out, flags
+
+
+def _check(errs, tol, label):
+    for k, v in errs.items():
+        assert v <= tol[k], f"{label}: {k} rel-L2 {v:.3e} > {tol[k]:.1e} (all: { {a: f'{b:.2e}' for a, b in errs.items()} })"
+
+
+TIGHT = dict(x=1e-6, v=1e-5, B=1e-5, F=1e-6, Jp=1e-6)
+TARGET = dict(x=1e-4, v=1e-4, B=1e-4, F=1e-4, Jp=1e-4)
+
+
+def test_mls_2d_blocks_1000_steps(gpu_lib, oracle_mod):
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.snow_blocks_2d()          # the 128^2 three-block workload, 4425 particles
+    steps = [1, 10, 100, 1000]
+    ref = _oracle_ref(oracle_mod, sc, steps)
+    got, flags = _gpu_run(sc, steps)
+    assert flags & 1 == 0
+    _check(state_errors(got[1], ref[1], 2), TIGHT, "step 1")
+    for s in (100, 1000):
+        _check(state_errors(got[s], ref[s], 2), TARGET, f"step {s}")
+
+
+def test_mls_2d_impact(gpu_lib, oracle_mod):
+    """Contact, friction and plastic flow (J_p leaves 1)."""
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.impact_2d()
+    steps = [1, 100, 400]
+    ref = _oracle_ref(oracle_mod, sc, steps)
+    assert ref[400]["plastic_det"].min() < 0.99
+    got, flags = _gpu_run(sc, steps)
+    _check(state_errors(got[1], ref[1], 2), TIGHT, "step 1")
+    _check(state_errors(got[100], ref[100], 2), TARGET, "step 100")
+    _check(state_errors(got[400], ref[400], 2), dict(x=1e-4, v=2e-3, B=1e-3, F=1e-3, Jp=1e-3), "step 400")
+
+
+def test_mls_3d_impact(gpu_lib, oracle_mod):
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.impact_3d()
+    steps = [1, 100, 300]
+    ref = _oracle_ref(oracle_mod, sc, steps)
+    got, flags = _gpu_run(sc, steps)
+    assert flags & 1 == 0
+    _check(state_errors(got[1], ref[1], 3), TIGHT, "step 1")
+    _check(state_errors(got[100], ref[100], 3), TARGET, "step 100")
+    _check(state_errors(got[300], ref[300], 3), dict(x=1e-4, v=2e-3, B=1e-3, F=1e-3, Jp=1e-3), "step 300")
+
+
+def test_mls_3d_snowball_slab_1000_steps(gpu_lib, oracle_mod):
+    """The snowball-on-slab workload at reduced resolution (48^3, 2 ppc)."""
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.snowball_on_slab_3d(W=48, ppc=2)
+    steps = [1, 1000]
+    ref = _oracle_ref(oracle_mod, sc, steps)
+    got, _ = _gpu_run(sc, steps)
+    _check(state_errors(got[1], ref[1], 3), TIGHT, "step 1")
+    _check(state_errors(got[1000], ref[1000], 3), TARGET, "step 1000")
+
+
+@pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d"])
+def test_classic_matches_reference_cpu(gpu_lib, oracle_mod, case):
+    """CLASSIC formulation vs the reference's compiled src/cpu (golden fixtures).
+    Both are FP32 with different operation order; each is held to the FP64
+    oracle, and to the reference within the sum of their FP64 distances."""
+    from mpm_snow_sim2d_b200._lib import FORMULATION_CLASSIC
+    scene, dumps = load_case(case)
+    steps = sorted(dumps)
+    got, _ = _gpu_run(scene, steps, formulation=FORMULATION_CLASSIC)
+    f64 = _oracle_ref(oracle_mod, scene, steps, formulation=oracle_mod.CLASSIC)
+    for s in steps:
+        ref = dict(dumps[s])
+        e_gpu = state_errors(got[s], f64[s], 2)
+
+        class R:  # reference dump as a state
+            position, velocity, affine_b, elastic_f = ref["position"], ref["velocity"], ref["affine_b"], ref["elastic_f"]
+            plastic_det = np.linalg.det(ref["plastic_f"].astype(np.float64))
+        e_ref = state_errors(R, f64[s], 2)
+        e_pair = state_errors(got[s], dict(ref, plastic_det=R.plastic_det), 2)
+        for k in e_gpu:
+            assert e_gpu[k] <= max(2.0 * e_ref[k], 2e-6), f"step {s} {k}: gpu {e_gpu[k]:.2e} vs reference {e_ref[k]:.2e}"
+            assert e_pair[k] <= 2.0 * (e_gpu[k] + e_ref[k]) + 1e-6, f"step {s} {k}: {e_pair[k]:.2e}"
+        if s == 1:
+            _check(e_pair, dict(x=1e-6, v=1e-5, B=1e-5, F=1e-6, Jp=1e-6), "step 1 vs reference")
+
+
+def test_run_to_run_bitwise_determinism(gpu_lib):
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    sc = scenes.impact_3d()
+    outs = []
+    for _ in range(2):
+        with Solver.from_scene(sc) as s:
+            s.Step(150)
+            m, p, raw = s.rasterize(raw=True)
+            st = s.get_state()
+            outs.append((raw, st))
+    (r0, s0), (r1, s1) = outs
+    assert np.array_equal(r0, r1)
+    for f in ("position", "velocity", "affine_b", "elastic_f", "plastic_det"):
+        assert np.array_equal(getattr(s0, f), getattr(s1, f)), f
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_p2g_conservation(gpu_lib, dim):
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    sc = scenes.impact_2d() if dim == 2 else scenes.impact_3d()
+    with Solver.from_scene(sc) as s:
+        s.Step(60)
+        st = s.get_state()
+        m, p = s.rasterize()
+    total = float(sc.mass.astype(np.float64).sum())
+    assert abs(m.sum() - total) <= 1e-9 * total
+    mom = (sc.mass.astype(np.float64)[:, None] * st.velocity.astype(np.float64)).sum(0)
+    scale = (sc.mass.astype(np.float64)[:, None] * np.abs(st.velocity)).sum()
+    assert np.all(np.abs(p.sum(0) - mom) <= 1e-5 * scale)
+
+
+def test_rest_state_stays_at_rest(gpu_lib):
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    sc = scenes.snow_blocks_2d().with_(gravity=0.0)
+    sc = sc.with_(velocity=np.zeros_like(sc.velocity))
+    with Solver.from_scene(sc) as s:
+        s.Step(50)
+        st = s.get_state()
+    assert np.array_equal(st.position, sc.position)
+    assert not np.any(st.velocity)
+    assert np.array_equal(st.elastic_f, np.broadcast_to(np.eye(2, dtype=np.float32), st.elastic_f.shape))
+
+
+def test_free_fall_is_exact(gpu_lib):
+    """Uniform fall, no wall in reach: v = v0 + g t, x quadratic in t."""
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    sc = scenes.snow_blocks_2d(steps=100)
+    sc = sc.with_(velocity=np.tile(np.float32([0.0, -50.0]), (sc.count, 1)))
+    with Solver.from_scene(sc) as s:
+        s.Step(100)
+        st = s.get_state()
+    t = 100 * sc.delta_time
+    v_exp = -50.0 + sc.gravity * t
+    inner = np.median(st.velocity[:, 1])
+    assert abs(inner - v_exp) < 1e-4 * abs(v_exp)
+    dy = np.median(st.position[:, 1] - sc.position[:, 1])
+    y_exp = sum((-50.0 + sc.gravity * sc.delta_time * (k + 1)) * sc.delta_time for k in range(100))
+    assert abs(dy - y_exp) < 1e-3 * abs(y_exp)
+
+
+def test_positions_state_checkpoint_roundtrip(gpu_lib, tmp_path):
+    from mpm_snow_sim2d_b200 import MpmError, Solver, scenes
+    sc = scenes.impact_2d()
+    with Solver.from_scene(sc) as a:
+        a.Step(30)
+        a.save(tmp_path / "ck.bin")
+        pos = a.GetParticlePositions()
+        a.Step(20)
+        end = a.get_state()
+    assert pos.shape == (sc.count, 2)
+    with Solver.from_scene(sc) as b:
+        b.load(tmp_path / "ck.bin")
+        assert b.step_count == 30
+        assert np.array_equal(b.GetParticlePositions(), pos)
+        b.Step(20)
+        again = b.get_state()
+    for f in ("position", "velocity", "affine_b", "elastic_f", "plastic_det"):
+        assert np.array_equal(getattr(end, f), getattr(again, f)), f
+    # a checkpoint from another configuration is refused
+    other = scenes.impact_2d(W=64)
+    with Solver.from_scene(other) as c:
+        with pytest.raises(MpmError) as ei:
+            c.load(tmp_path / "ck.bin")
+        assert ei.value.status == 8
+    # a truncated file is refused without touching the state
+    raw = (tmp_path / "ck.bin").read_bytes()
+    (tmp_path / "bad.bin").write_bytes(raw[: len(raw) // 2])
+    with Solver.from_scene(sc) as d:
+        with pytest.raises(MpmError) as ei:
+            d.load(tmp_path / "bad.bin")
+        assert ei.value.status == 7
+
+
+def test_api_errors_and_flags(gpu_lib):
+    import ctypes as C
+    from mpm_snow_sim2d_b200 import MpmError, Solver, scenes
+    lib = gpu_lib
+    sc = scenes.impact_2d()
+    with Solver.from_scene(sc) as s:
+        small = np.empty(3, np.float32)
+        rc = lib.mpm_get_positions(s._h, small.ctypes.data_as(C.POINTER(C.c_float)), 3)
+        assert rc == 11 and b"capacity" in lib.mpm_last_error(s._h)
+        with pytest.raises(MpmError):
+            s.Step(-1)
+        assert s.status() & 1 == 0
+        # a NaN injected into the state is reported through the status word, no trap
+        st = s.get_state()
+        st.position[5] = np.nan
+        s.set_state(position=st.position)
+        s.Step(1)
+        assert s.status() & 1
+    with pytest.raises(MpmError) as ei:
+        Solver.from_scene(sc.with_(position=np.full_like(sc.position, np.nan)))
+    assert ei.value.status == 1
+
+
+def test_set_stream_and_external_events(gpu_lib):
+    import torch
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    sc = scenes.impact_2d()
+    stream = torch.cuda.Stream()
+    with Solver.from_scene(sc) as s:
+        s.set_stream(stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.Step(10)
+        e1.record(stream)
+        e1.synchronize()
+        assert e0.elapsed_time(e1) > 0
+        assert s.step_count == 10
