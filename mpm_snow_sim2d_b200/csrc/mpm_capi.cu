@@ -11,6 +11,7 @@
 
 #include "mpm/mpm.h"
 #include "mpm_kernels.cuh"
+#include "mpm_tiled.cuh"
 
 using namespace mpm;
 
@@ -37,6 +38,14 @@ struct mpm_solver {
     long long step = 0;
     StepConsts C{};
     std::string err;
+    // tiled MLS path
+    bool tiled = false;
+    bool needs_sort = true;
+    int sort_period = 8;
+    int sms = 148;
+    int p2g_grid = 0;
+    TileInfo ti{};
+    SortBuffers alt{};
 };
 
 namespace {
@@ -87,6 +96,15 @@ void release(mpm_solver* s) {
     if (s->acc) cudaFree(s->acc);
     if (s->gv) cudaFree(s->gv);
     if (s->status) cudaFree(s->status);
+    float* al[] = {s->alt.x, s->alt.v, s->alt.B, s->alt.Fe, s->alt.Jp, s->alt.mass, s->alt.vol};
+    for (float* p : al)
+        if (p) cudaFree(p);
+    if (s->alt.id) cudaFree(s->alt.id);
+    int* ti[] = {s->ti.key, s->ti.tile_count, s->ti.tile_cursor, s->ti.tile_start, s->ti.n_items, s->ti.mark,
+                 s->ti.mark_list, s->ti.n_marked, s->ti.n_orphans};
+    for (int* p : ti)
+        if (p) cudaFree(p);
+    if (s->ti.items) cudaFree(s->ti.items);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -119,6 +137,56 @@ template <int D, int FORM> cudaError_t launch_g2p(mpm_solver* s) {
     return cudaGetLastError();
 }
 
+// Counting sort of the particle state by cell tile into the alternate
+// buffers, then swap. Called every sort_period steps (and after any state
+// upload) on the tiled path.
+template <int D> cudaError_t launch_sort(mpm_solver* s) {
+    if (s->n == 0) { s->needs_sort = false; return cudaMemsetAsync(s->ti.n_items, 0, sizeof(int), s->stream); }
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
+    k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
+    k_sort_scatter<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->ti);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    std::swap(s->x, s->alt.x);
+    std::swap(s->v, s->alt.v);
+    std::swap(s->B, s->alt.B);
+    std::swap(s->Fe, s->alt.Fe);
+    std::swap(s->Jp, s->alt.Jp);
+    std::swap(s->id, s->alt.id);
+    if (s->mass) std::swap(s->mass, s->alt.mass);
+    if (s->vol) std::swap(s->vol, s->alt.vol);
+    s->needs_sort = false;
+    return cudaSuccess;
+}
+
+template <int D> cudaError_t launch_p2g_tiled(mpm_solver* s) {
+    if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) {
+        cudaError_t e = launch_sort<D>(s);
+        if (e != cudaSuccess) return e;
+    }
+    k_p2g_tiled<D><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D>), s->stream>>>(particle_view(s), s->id, s->C, s->ti,
+                                                                                 s->acc, s->status);
+    return cudaGetLastError();
+}
+
+template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
+    k_grid_marked<D, kMLS><<<s->sms * 8, 256, 0, s->stream>>>(s->C, s->ti, s->acc, s->gv, s->status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+template <int D> cudaError_t step_tiled(mpm_solver* s) {
+    cudaError_t e = launch_p2g_tiled<D>(s);
+    if (e != cudaSuccess) return e;
+    e = launch_grid_marked<D>(s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return e;
+    return launch_g2p<D, kMLS>(s);
+}
+
 template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
     cudaError_t e = launch_p2g<D, FORM>(s);
     if (e != cudaSuccess) return e;
@@ -128,13 +196,77 @@ template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
 }
 
 cudaError_t dispatch_step(mpm_solver* s) {
+    if (s->tiled) return s->dim == 2 ? step_tiled<2>(s) : step_tiled<3>(s);
     if (s->dim == 2) return s->form == kClassic ? step_once<2, kClassic>(s) : step_once<2, kMLS>(s);
     return step_once<3, kMLS>(s);
 }
 
 cudaError_t dispatch_p2g(mpm_solver* s) {
+    if (s->tiled) return s->dim == 2 ? launch_p2g_tiled<2>(s) : launch_p2g_tiled<3>(s);
     if (s->dim == 2) return s->form == kClassic ? launch_p2g<2, kClassic>(s) : launch_p2g<2, kMLS>(s);
     return launch_p2g<3, kMLS>(s);
+}
+
+// After a P2G-only pass: clear accumulators and node-block marks.
+cudaError_t clear_after_p2g(mpm_solver* s) {
+    if (s->tiled) {
+        cudaError_t e = s->dim == 2 ? launch_grid_marked<2>(s) : launch_grid_marked<3>(s);
+        if (e != cudaSuccess) return e;
+        return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
+    }
+    return cudaMemsetAsync(s->acc, 0, sizeof(unsigned long long) * nacc(s->dim, s->form) * s->nodes, s->stream);
+}
+
+// Tiles, work items, node-block marks and the sort's alternate buffers.
+mpm_status setup_tiled(mpm_solver* s) {
+    const int D = s->dim, n = s->n;
+    const int T = D == 3 ? TileGeom<3>::T : TileGeom<2>::T;
+    const int ext[3] = {s->C.W, s->C.H, s->C.Dp};
+    const int nodes_axis[3] = {s->C.nx, s->C.ny, s->C.nz};
+    TileInfo& ti = s->ti;
+    ti.n_tiles = 1;
+    ti.n_blocks = 1;
+    for (int k = 0; k < 3; ++k) {
+        ti.tiles[k] = k < D ? (ext[k] + T - 1) / T : 1;
+        ti.nblk[k] = k < D ? (nodes_axis[k] + T - 1) / T : 1;
+        ti.n_tiles *= ti.tiles[k];
+        ti.n_blocks *= ti.nblk[k];
+    }
+    const size_t max_items = (size_t)n / kItem + ti.n_tiles + 1;
+    if (dalloc(&ti.key, (size_t)n) || dalloc(&ti.tile_count, (size_t)ti.n_tiles) ||
+        dalloc(&ti.tile_cursor, (size_t)ti.n_tiles) || dalloc(&ti.tile_start, (size_t)ti.n_tiles) ||
+        dalloc(&ti.items, max_items) || dalloc(&ti.n_items, 1) || dalloc(&ti.mark, (size_t)ti.n_blocks) ||
+        dalloc(&ti.mark_list, (size_t)ti.n_blocks) || dalloc(&ti.n_marked, 1) || dalloc(&ti.n_orphans, 1) ||
+        dalloc(&s->alt.x, (size_t)n * D) || dalloc(&s->alt.v, (size_t)n * D) || dalloc(&s->alt.B, (size_t)n * D * D) ||
+        dalloc(&s->alt.Fe, (size_t)n * D * D) || dalloc(&s->alt.Jp, (size_t)n) || dalloc(&s->alt.id, (size_t)n)) {
+        cudaGetLastError();
+        return MPM_ERR_OUT_OF_MEMORY;
+    }
+    if (s->mass && dalloc(&s->alt.mass, (size_t)n)) return MPM_ERR_OUT_OF_MEMORY;
+    if (s->vol && dalloc(&s->alt.vol, (size_t)n)) return MPM_ERR_OUT_OF_MEMORY;
+    bool ok = cudaMemset(ti.tile_count, 0, sizeof(int) * ti.n_tiles) == cudaSuccess &&
+              cudaMemset(ti.tile_cursor, 0, sizeof(int) * ti.n_tiles) == cudaSuccess &&
+              cudaMemset(ti.n_items, 0, sizeof(int)) == cudaSuccess &&
+              cudaMemset(ti.mark, 0, sizeof(int) * ti.n_blocks) == cudaSuccess &&
+              cudaMemset(ti.n_marked, 0, sizeof(int)) == cudaSuccess &&
+              cudaMemset(ti.n_orphans, 0, sizeof(int)) == cudaSuccess;
+    if (!ok) return MPM_ERR_CUDA;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    s->sms = sms > 0 ? sms : 148;
+    const size_t smem = D == 3 ? sizeof(P2GSmem<3>) : sizeof(P2GSmem<2>);
+    cudaError_t e = D == 3 ? cudaFuncSetAttribute(k_p2g_tiled<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(k_p2g_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return MPM_ERR_CUDA;
+    int per_sm = 0;
+    e = D == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g_tiled<3>, kTileThreads, smem)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g_tiled<2>, kTileThreads, smem);
+    if (e != cudaSuccess || per_sm < 1) return MPM_ERR_CUDA;
+    s->p2g_grid = s->sms * per_sm;
+    s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 8;
+    s->needs_sort = true;
+    return MPM_OK;
 }
 
 // Choose power-of-two fixed-point scales so that no node sum can exceed 2^62
@@ -239,15 +371,34 @@ uint64_t params_hash(const mpm_params& p) {
 }  // namespace
 
 namespace {
-const char* kStageNames[] = {"p2g", "grid_update", "g2p"};
-constexpr int kStages = 3;
+const char* kStageNames[] = {"sort", "p2g", "grid_update", "g2p"};
+constexpr int kStages = 4;
 
 template <int D, int FORM> cudaError_t stage(mpm_solver* s, int k) {
-    if (k == 0) return launch_p2g<D, FORM>(s);
-    if (k == 1) return launch_grid<D, FORM>(s);
+    if (k == 0) return cudaSuccess;
+    if (k == 1) return launch_p2g<D, FORM>(s);
+    if (k == 2) return launch_grid<D, FORM>(s);
     return launch_g2p<D, FORM>(s);
 }
+template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
+    if (k == 0) {
+        if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) return launch_sort<D>(s);
+        return cudaSuccess;
+    }
+    if (k == 1) {
+        k_p2g_tiled<D><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D>), s->stream>>>(particle_view(s), s->id, s->C,
+                                                                                     s->ti, s->acc, s->status);
+        return cudaGetLastError();
+    }
+    if (k == 2) {
+        cudaError_t e = launch_grid_marked<D>(s);
+        if (e != cudaSuccess) return e;
+        return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
+    }
+    return launch_g2p<D, kMLS>(s);
+}
 cudaError_t dispatch_stage(mpm_solver* s, int k) {
+    if (s->tiled) return s->dim == 2 ? stage_tiled<2>(s, k) : stage_tiled<3>(s, k);
     if (s->dim == 2) return s->form == kClassic ? stage<2, kClassic>(s, k) : stage<2, kMLS>(s, k);
     return stage<3, kMLS>(s, k);
 }
@@ -375,6 +526,11 @@ mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, 
     ok = ok && cudaMemset(s->status, 0, sizeof(unsigned)) == cudaSuccess;
     ok = ok && cudaDeviceSynchronize() == cudaSuccess;
     if (!ok) { cudaGetLastError(); return bail(MPM_ERR_CUDA); }
+    s->tiled = (s->form == kMLS);
+    if (s->tiled) {
+        mpm_status ts = setup_tiled(s);
+        if (ts != MPM_OK) return bail(ts);
+    }
     *out = s;
     return MPM_OK;
 }
@@ -464,6 +620,7 @@ mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
     if (st->affine_b && (r = import_field(s, s->B, D * D, st->affine_b)) != MPM_OK) return r;
     if (st->elastic_f && (r = import_field(s, s->Fe, D * D, st->elastic_f)) != MPM_OK) return r;
     if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
+    s->needs_sort = true;
     return MPM_OK;
 }
 
@@ -475,7 +632,7 @@ mpm_status mpm_rasterize(mpm_solver* s, double* node_mass, double* node_momentum
     if (e != cudaSuccess) return cuda_fail(s, e, "p2g launch");
     std::vector<long long> h((size_t)NA * s->nodes);
     MPM_CUDA(s, cudaMemcpyAsync(h.data(), s->acc, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost, s->stream));
-    MPM_CUDA(s, cudaMemsetAsync(s->acc, 0, sizeof(long long) * h.size(), s->stream));
+    MPM_CUDA(s, clear_after_p2g(s));
     MPM_CUDA(s, cudaStreamSynchronize(s->stream));
     const double ism = std::ldexp(1.0, -s->log2_sm), isp = std::ldexp(1.0, -s->log2_sp),
                  isf = std::ldexp(1.0, -s->log2_sf);

@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, u
     if (FORM == kMLS && vol == 0.f) return;
 
     float sig[D * D];
-    if (vol != 0.f) hardened_stress<D, FORM>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+    if (vol != 0.f) hardened_stress_polar<D, FORM>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
     else {
 #pragma unroll
         for (int k = 0; k < D * D; ++k) sig[k] = 0.f;
@@ -243,15 +243,13 @@ __device__ __forceinline__ void collide(const StepConsts& C, const float* loc, c
     }
 }
 
-// Grid update, one thread per node (MLS: src/gpu/shaders/2d/grid_update.glsl:
-// 82-108, 3D :88-117; CLASSIC: src/cpu/Grid.cpp:165-184). Reads and clears the
+// Grid update of one node (MLS: src/gpu/shaders/2d/grid_update.glsl:82-108,
+// 3D :88-117; CLASSIC: src/cpu/Grid.cpp:165-184). Reads and clears the
 // fixed-point accumulators (the reference's separate reset pass,
 // reset.glsl:13-23, is fused here) and writes the velocities G2P gathers.
 template <int D, int FORM>
-__global__ void __launch_bounds__(256) k_grid_update(StepConsts C, unsigned long long* __restrict__ acc,
-                                                     float4* __restrict__ gv, unsigned* __restrict__ status) {
-    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= C.nodes) return;
+__device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long long* __restrict__ acc,
+                                          float4* __restrict__ gv, unsigned* __restrict__ status, long long id) {
     constexpr int NACC = Layout<D, FORM>::NACC;
     long long q[NACC];
 #pragma unroll
@@ -299,16 +297,34 @@ __global__ void __launch_bounds__(256) k_grid_update(StepConsts C, unsigned long
     }
 }
 
+// Dense grid update, one thread per node.
+template <int D, int FORM>
+__global__ void __launch_bounds__(256) k_grid_update(StepConsts C, unsigned long long* __restrict__ acc,
+                                                     float4* __restrict__ gv, unsigned* __restrict__ status) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= C.nodes) return;
+    grid_node<D, FORM>(C, acc, gv, status, id);
+}
+
 // ---------------------------------------------------------------------------
 // Plasticity return map shared by every G2P variant (src/gpu/shaders/2d/
 // g2p.glsl:73-93, 3d/g2p.glsl:73-104, src/cpu/Particles.cpp:64-106):
 //   F_hat = (I + dt L) F_E;  U S V^T = svd(F_hat);  S' = max(clamp(S, 1-tc, 1+ts), 1e-6)
 //   F_E' = U S' V^T;  J_p' = J_p prod(S / S')  (= det of V diag(S/S') V^T F_P)
+// When every singular value of F_hat is inside [1-tc, 1+ts] (and det > 0),
+// S' = S and the map returns F_hat and J_p unchanged; that case is proven
+// first (in_elastic_band) and skips the SVD.
 // The FP32 SVD is recomputed in FP64 when F_hat is near-degenerate
 // (sigma_min^2 < 1e-2 sigma_max^2), where squaring in M^T M loses FP32 digits.
 template <int D, int FORM>
 __device__ __forceinline__ void plasticity(const StepConsts& C, const float* Fh, float* Fe_out, float& Jp,
                                            unsigned* status) {
+    // Inside the elastic band the return map is the identity: no SVD.
+    if (in_elastic_band<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s)) {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) Fe_out[k] = Fh[k];
+        return;
+    }
     float U[D * D], S[D], V[D * D];
     svd<D, FORM>(Fh, U, S, V);
     float smin = fabsf(S[0]), smax = fabsf(S[0]);

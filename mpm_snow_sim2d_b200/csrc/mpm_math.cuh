@@ -249,4 +249,140 @@ template <int D, int FORM> __device__ __forceinline__ void hardened_stress(const
         }
 }
 
+// Polar rotation R of F (F = R S, S symmetric positive definite) for det F > 0.
+// 2D: closed form, R is the rotation by atan2(F10 - F01, F00 + F11)
+//     (tr(R^T F) = tr S > 0 keeps that vector away from zero).
+// 3D: Newton's iteration R <- (R + R^-T) / 2 from R = F, which converges
+//     quadratically to the polar factor; stops once an update is below 1e-6.
+// Returns false (R untouched) for det F <= 0 or no convergence in 12
+// iterations; the caller then takes U V^T from the reference's SVD.
+template <int D> __device__ __forceinline__ bool polar_rotation(const float* F, float* R) {
+    if constexpr (D == 2) {
+        if (!(F[0] * F[3] - F[1] * F[2] > 0.f)) return false;
+        const float c = F[0] + F[3], s = F[2] - F[1];
+        const float inv = rsqrtf(c * c + s * s);
+        R[0] = c * inv; R[1] = -s * inv; R[2] = s * inv; R[3] = c * inv;
+        return true;
+    } else {
+        if (!(det<3>(F) > 0.f)) return false;
+        float X[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) X[i] = F[i];
+        for (int it = 0; it < 12; ++it) {
+            // cofactor matrix: X^-T = cof(X) / det(X)
+            float cf[9];
+            cf[0] = X[4] * X[8] - X[5] * X[7];
+            cf[1] = X[5] * X[6] - X[3] * X[8];
+            cf[2] = X[3] * X[7] - X[4] * X[6];
+            cf[3] = X[2] * X[7] - X[1] * X[8];
+            cf[4] = X[0] * X[8] - X[2] * X[6];
+            cf[5] = X[1] * X[6] - X[0] * X[7];
+            cf[6] = X[1] * X[5] - X[2] * X[4];
+            cf[7] = X[2] * X[3] - X[0] * X[5];
+            cf[8] = X[0] * X[4] - X[1] * X[3];
+            const float dt = X[0] * cf[0] + X[1] * cf[1] + X[2] * cf[2];
+            if (!(dt > 0.f)) return false;
+            const float hid = 0.5f / dt;
+            float diff = 0.f;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const float nx = 0.5f * X[i] + hid * cf[i];
+                const float e = nx - X[i];
+                diff += e * e;
+                X[i] = nx;
+            }
+            if (diff < 1e-12f) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i) R[i] = X[i];
+                return true;
+            }
+        }
+        return false;
+    }
+}
+
+// Stress of the hardened Kirchhoff form above with the polar rotation taken
+// from polar_rotation (the same R = U V^T as the reference's SVD, computed
+// without the SVD); falls back to hardened_stress when it declines.
+template <int D, int FORM> __device__ __forceinline__ void hardened_stress_polar(const float* Fe, float Jp, float mu0,
+                                                                                float la0, float xi, float* sig) {
+    float Rm[D * D];
+    if (FORM != kMLS || !polar_rotation<D>(Fe, Rm)) {
+        hardened_stress<D, FORM>(Fe, Jp, mu0, la0, xi, sig);
+        return;
+    }
+    const float Je = det<D>(Fe);
+    const float h = expf(xi * (1.f - Jp));
+    const float mu = mu0 * h, la = la0 * h;
+    const float diag = la * (Je - 1.f) * Je;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += (Fe[i * D + k] - Rm[i * D + k]) * Fe[j * D + k];
+            sig[i * D + j] = 2.f * mu * s + (i == j ? diag : 0.f);
+        }
+}
+
+// True when every singular value of F lies in [t0, t1] and det F > 0, proven
+// with margin: then the return map clamps nothing and is the identity
+// (F_E' = F, J_p' = J_p), so the SVD can be skipped. First Gershgorin discs of
+// S = F^T F in FP32 (margin 4e-6 > the FP32 rounding of S); if they do not
+// decide, Sylvester's criterion in FP64 for (t1^2 - 1e-5) I - S and
+// S - (t0^2 + 1e-5) I (positive leading minors); 1e-5 exceeds the FP64
+// rounding of the minors even for a triple eigenvalue at the margin.
+template <int D> __device__ __forceinline__ bool in_elastic_band(const float* F, float t0, float t1) {
+    if (!(det<D>(F) > 0.f)) return false;
+    float S[D * D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += F[k * D + i] * F[k * D + j];
+            S[i * D + j] = s;
+        }
+    const float lo = t0 * t0 + 4e-6f, hi = t1 * t1 - 4e-6f;
+    bool gersh = true;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        float r = 0.f;
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+            if (j != i) r += fabsf(S[i * D + j]);
+        gersh = gersh && (S[i * D + i] - r >= lo) && (S[i * D + i] + r <= hi);
+    }
+    if (gersh) return true;
+    double Sd[D * D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += double(F[k * D + i]) * double(F[k * D + j]);
+            Sd[i * D + j] = s;
+        }
+    const double up = double(t1) * double(t1) - 1e-5, dn = double(t0) * double(t0) + 1e-5;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        double M[D * D];
+#pragma unroll
+        for (int i = 0; i < D * D; ++i) M[i] = side == 0 ? -Sd[i] : Sd[i];
+#pragma unroll
+        for (int i = 0; i < D; ++i) M[i * D + i] += side == 0 ? up : -dn;
+        if (!(M[0] > 0.0)) return false;
+        if constexpr (D == 2) {
+            if (!(M[0] * M[3] - M[1] * M[2] > 0.0)) return false;
+        } else {
+            if (!(M[0] * M[4] - M[1] * M[3] > 0.0)) return false;
+            if (!(det<3>(M) > 0.0)) return false;
+        }
+    }
+    return true;
+}
+
 }  // namespace mpm

@@ -1,0 +1,514 @@
+// Tiled MLS step for B200: particles binned by cell tile, P2G accumulated per
+// cell in registers and per tile in shared memory, and a grid update that only
+// visits node blocks P2G touched.
+//
+// Tiles are T^D cells (3D: 4^3, 2D: 8^2). Every `sort_period` steps a counting
+// sort moves the particle state into tile order (k_sort_*); between sorts a
+// particle may drift M = 1 cell out of its tile and is still handled by its
+// tile's CTA; farther drifters ("orphans") take a per-particle path with global
+// atomics. Determinism: inside a CTA the particles of one cell are accumulated
+// in particle-id order in FP32, every cross-cell / cross-CTA sum is an int64
+// fixed-point atomic, so grid sums are bit-identical run to run whatever order
+// the sort's atomics produce.
+#pragma once
+
+#include "mpm_kernels.cuh"
+
+namespace mpm {
+
+template <int D> struct TileGeom;
+template <> struct TileGeom<3> {
+    static constexpr int T = 4, M = 1, R = T + 2 * M, NR = R + 3;
+    static constexpr int RC = R * R * R, NN = NR * NR * NR, SPLIT = 4, PS = 29, BN = T * T * T;
+};
+template <> struct TileGeom<2> {
+    static constexpr int T = 8, M = 1, R = T + 2 * M, NR = R + 3;
+    static constexpr int RC = R * R, NN = NR * NR, SPLIT = 1, PS = 17, BN = T * T;
+};
+
+constexpr int kItem = 512;     // particles per work item (one CTA pass)
+constexpr int kTileThreads = 256;
+
+struct TileInfo {
+    int tiles[3];      // cell tiles per axis
+    int n_tiles;
+    int nblk[3];       // node blocks per axis (nodes / T, rounded up)
+    int n_blocks;
+    int* key;          // per slot: tile of the particle at the last sort
+    int* tile_count;   // per tile
+    int* tile_cursor;  // per tile
+    int* tile_start;   // per tile (exclusive scan of tile_count)
+    int4* items;       // (tile, first slot, count, 0)
+    int* n_items;      // device scalar
+    int* mark;         // per node block: touched by this step's P2G
+    int* mark_list;    // touched node blocks
+    int* n_marked;     // device scalar
+    int* n_orphans;    // device scalar, diagnostics (accumulates)
+};
+
+template <int D> __device__ __forceinline__ int cell_clamped(float x, int ext) {
+    const int c = int(fminf(fmaxf(x, 0.f), float(ext) - 0.5f));
+    return c < 0 ? 0 : (c >= ext ? ext - 1 : c);
+}
+
+template <int D> __device__ __forceinline__ int tile_of_slot(const Particles& P, const StepConsts& C,
+                                                            const TileInfo& TI, int i) {
+    constexpr int T = TileGeom<D>::T;
+    const int ext[3] = {C.W, C.H, C.Dp};
+    int t = 0;
+#pragma unroll
+    for (int k = D - 1; k >= 0; --k) t = t * TI.tiles[k] + cell_clamped<D>(P.x[k * P.n + i], ext[k]) / T;
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Counting sort by tile.
+
+template <int D>
+__global__ void __launch_bounds__(256) k_sort_count(Particles P, StepConsts C, TileInfo TI) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int t = tile_of_slot<D>(P, C, TI, i);
+    TI.key[i] = t;
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, t);
+    const int lane = threadIdx.x & 31;
+    if (lane == __ffs(peers) - 1) atomicAdd(&TI.tile_count[t], __popc(peers));
+}
+
+// Single-CTA exclusive scans of the tile counts and of the work items per tile
+// (a tile with n particles is ceil(n / kItem) items); writes the item list,
+// clears count/cursor for the next sort.
+__global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
+    __shared__ int s_cnt[1024], s_itm[1024];
+    const int nt = TI.n_tiles, tid = threadIdx.x;
+    const int chunk = (nt + 1023) / 1024;
+    const int lo = min(nt, tid * chunk), hi = min(nt, lo + chunk);
+    int c = 0, it = 0;
+    for (int t = lo; t < hi; ++t) {
+        const int n = TI.tile_count[t];
+        c += n;
+        it += (n + kItem - 1) / kItem;
+    }
+    s_cnt[tid] = c;
+    s_itm[tid] = it;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
+        const int a = tid >= off ? s_cnt[tid - off] : 0;
+        const int b = tid >= off ? s_itm[tid - off] : 0;
+        __syncthreads();
+        s_cnt[tid] += a;
+        s_itm[tid] += b;
+        __syncthreads();
+    }
+    int base = s_cnt[tid] - c, ibase = s_itm[tid] - it;
+    for (int t = lo; t < hi; ++t) {
+        const int n = TI.tile_count[t];
+        TI.tile_start[t] = base;
+        TI.tile_cursor[t] = 0;
+        for (int j = 0; j < n; j += kItem) TI.items[ibase++] = make_int4(t, base + j, min(kItem, n - j), 0);
+        base += n;
+        TI.tile_count[t] = 0;
+    }
+    if (tid == 1023) *TI.n_items = s_itm[1023];
+}
+
+struct SortBuffers {
+    float *x, *v, *B, *Fe, *Jp, *mass, *vol;
+    int* id;
+};
+
+template <int D>
+__global__ void __launch_bounds__(256) k_sort_scatter(Particles P, const int* __restrict__ id_src, SortBuffers dst,
+                                                      TileInfo TI) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    const int t = TI.key[i];
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, t);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&TI.tile_cursor[t], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    const int s = TI.tile_start[t] + base + __popc(peers & ((1u << lane) - 1));
+#pragma unroll
+    for (int k = 0; k < D; ++k) { dst.x[k * n + s] = P.x[k * n + i]; dst.v[k * n + s] = P.v[k * n + i]; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) { dst.B[k * n + s] = P.B[k * n + i]; dst.Fe[k * n + s] = P.Fe[k * n + i]; }
+    dst.Jp[s] = P.Jp[i];
+    dst.id[s] = id_src[i];
+    if (P.mass) dst.mass[s] = P.mass[i];
+    if (P.vol) dst.vol[s] = P.vol[i];
+}
+
+// ---------------------------------------------------------------------------
+// Node-block marking (which blocks of T^D nodes received mass this step).
+
+__device__ __forceinline__ void mark_block(const TileInfo& TI, int b) {
+    if (atomicExch(&TI.mark[b], 1) == 0) TI.mark_list[atomicAdd(TI.n_marked, 1)] = b;
+}
+
+template <int D> __device__ __forceinline__ void mark_stencil_blocks(const TileInfo& TI, const int* base) {
+    constexpr int T = TileGeom<D>::T;
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        lo[k] = max(0, base[k]) / T;
+        hi[k] = min(TI.nblk[k] * T - 1, max(0, base[k] + 3)) / T;
+    }
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+        for (int by = lo[1]; by <= hi[1]; ++by)
+            for (int bx = lo[0]; bx <= hi[0]; ++bx) mark_block(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
+}
+
+// ---------------------------------------------------------------------------
+// Tiled P2G (MLS).
+template <int D> struct P2GSmem {
+    using G = TileGeom<D>;
+    float pay[kItem * G::PS];
+    int lcell[kItem];
+    int pid[kItem];
+    int order[kItem];
+    int cnt[G::RC];
+    int start[G::RC];
+    int cur[G::RC];
+    int ne[G::RC];
+    int n_ne;
+    unsigned blockmask;
+    unsigned long long tile[(1 + D) * G::NN];
+};
+
+// Payload layout (floats) per particle:
+//   3D: wx[4] wy[4] wz[4] | f[3] | mv[3] | A[9] | m
+//   2D: wx[4] wy[4] | f[2] | mv[2] | A[4] | m
+// with f = x - cell (cell = int(x)), A = 3 m B - 3 dt V sigma, mv = m v.
+template <int D> struct PayOff {
+    static constexpr int F = 4 * D, MV = F + D, A = MV + D, M = A + D * D;
+};
+
+template <int D>
+__device__ __forceinline__ void scatter_orphan(const StepConsts& C, const TileInfo& TI, const int* base,
+                                               const float (*wk)[4], const float* f, const float* mv, const float* A,
+                                               float m, unsigned long long* acc, unsigned* status) {
+    const int lim[3] = {C.W, C.H, C.Dp};
+    bool outside = false;
+    const int nzs = (D == 3) ? 4 : 1;
+    for (int a = 0; a < 4; ++a) {
+        const int ix = base[0] + a;
+        if (ix < 0 || ix > lim[0]) { outside = true; continue; }
+        for (int b = 0; b < 4; ++b) {
+            const int iy = base[1] + b;
+            if (iy < 0 || iy > lim[1]) { outside = true; continue; }
+            for (int c = 0; c < nzs; ++c) {
+                const int iz = (D == 3) ? base[2] + c : 0;
+                if (D == 3 && (iz < 0 || iz > lim[2])) { outside = true; continue; }
+                const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
+                const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
+                const float d[3] = {float(a - 1) - f[0], float(b - 1) - f[1], D == 3 ? float(c - 1) - f[2] : 0.f};
+                red_add(&acc[cid], to_fixed(w * m, C.sm, status));
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    float s = mv[r];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) s += A[r * D + k] * d[k];
+                    red_add(&acc[(1 + r) * C.nodes + cid], to_fixed(w * s, C.sp, status));
+                }
+            }
+        }
+    }
+    if (outside) raise_flag(status, 4u);
+    mark_stencil_blocks<D>(TI, base);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const int* __restrict__ pid_g, StepConsts C,
+                                                            TileInfo TI, unsigned long long* __restrict__ acc,
+                                                            unsigned* __restrict__ status) {
+    using G = TileGeom<D>;
+    using O = PayOff<D>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P2GSmem<D>& S = *reinterpret_cast<P2GSmem<D>*>(smem_raw);
+    const int tid = threadIdx.x;
+    const int n = P.n;
+    const int ext[3] = {C.W, C.H, C.Dp};
+    for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) S.tile[e] = 0ull;
+
+    const int n_items = *TI.n_items;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int4 it = TI.items[item];
+        int tc[3] = {0, 0, 0};
+        {
+            int t = it.x;
+#pragma unroll
+            for (int k = 0; k < D; ++k) { tc[k] = t % TI.tiles[k]; t /= TI.tiles[k]; }
+        }
+        int rlo[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < D; ++k) rlo[k] = tc[k] * G::T - G::M;
+        for (int c = tid; c < G::RC; c += blockDim.x) { S.cnt[c] = 0; S.cur[c] = 0; }
+        if (tid == 0) { S.n_ne = 0; S.blockmask = 0u; }
+        __syncthreads();
+
+        // Phase A: per-particle payload (stress via the polar rotation).
+        for (int j = tid; j < it.z; j += blockDim.x) {
+            const int i = it.y + j;
+            float x[D], v[D], B[D * D], Fe[D * D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
+            const float Jp = P.Jp[i];
+            const float mass = P.mass ? P.mass[i] : P.mass_u;
+            const float vol = P.vol ? P.vol[i] : P.vol_u;
+            S.lcell[j] = -1;
+            if (vol == 0.f) continue;  // p2g.glsl:42
+            float sig[D * D];
+            hardened_stress_polar<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+            float A[D * D], mv[D], f[D], wk[3][4];
+            int base[3] = {0, 0, 0}, lc = 0;
+            bool inreg = true;
+#pragma unroll
+            for (int k = D - 1; k >= 0; --k) {
+                base[k] = stencil_base(x[k], ext[k]);
+                const int cell = base[k] + 1;
+                f[k] = x[k] - float(cell);
+#pragma unroll
+                for (int o = 0; o < 4; ++o) wk[k][o] = bspline_n(x[k] - float(base[k] + o));
+                const int l = cell - rlo[k];
+                inreg = inreg && l >= 0 && l < G::R;
+                lc = lc * G::R + l;
+            }
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                mv[r] = mass * v[r];
+#pragma unroll
+                for (int c = 0; c < D; ++c) A[r * D + c] = 3.f * mass * B[r * D + c] - 3.f * C.dt * vol * sig[r * D + c];
+            }
+            if (inreg) {
+                float* q = S.pay + j * G::PS;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+#pragma unroll
+                    for (int o = 0; o < 4; ++o) q[4 * k + o] = wk[k][o];
+                    q[O::F + k] = f[k];
+                    q[O::MV + k] = mv[k];
+                }
+#pragma unroll
+                for (int k = 0; k < D * D; ++k) q[O::A + k] = A[k];
+                q[O::M] = mass;
+                S.lcell[j] = lc;
+                S.pid[j] = pid_g[i];
+                atomicAdd(&S.cnt[lc], 1);
+            } else {
+                scatter_orphan<D>(C, TI, base, wk, f, mv, A, mass, acc, status);
+                atomicAdd(TI.n_orphans, 1);
+            }
+        }
+        __syncthreads();
+
+        // Phase B: per-cell lists (exclusive scan by warp 0), cells ordered by id.
+        if (tid < 32) {
+            int carry = 0;
+            for (int c0 = 0; c0 < G::RC; c0 += 32) {
+                const int c = c0 + tid;
+                const int v = c < G::RC ? S.cnt[c] : 0;
+                int incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (tid >= o) incl += y;
+                }
+                if (c < G::RC) S.start[c] = carry + incl - v;
+                const unsigned nz = __ballot_sync(0xffffffffu, v > 0);
+                if (v > 0) S.ne[S.n_ne + __popc(nz & ((1u << tid) - 1))] = c;
+                __syncwarp();
+                if (tid == 0) S.n_ne += __popc(nz);
+                __syncwarp();
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+        __syncthreads();
+        for (int j = tid; j < it.z; j += blockDim.x) {
+            const int lc = S.lcell[j];
+            if (lc >= 0) S.order[S.start[lc] + atomicAdd(&S.cur[lc], 1)] = j;
+        }
+        __syncthreads();
+        for (int e = tid; e < S.n_ne; e += blockDim.x) {  // insertion sort by particle id
+            const int c = S.ne[e], s0 = S.start[c], s1 = s0 + S.cnt[c];
+            for (int q = s0 + 1; q < s1; ++q) {
+                const int jj = S.order[q], key = S.pid[jj];
+                int r = q - 1;
+                while (r >= s0 && S.pid[S.order[r]] > key) { S.order[r + 1] = S.order[r]; --r; }
+                S.order[r + 1] = jj;
+            }
+        }
+        __syncthreads();
+
+        // Phase C: one thread per (cell, x-offset): registers over the cell's
+        // particles, then int64 fixed point into the shared tile.
+        const int units = S.n_ne * G::SPLIT;
+        for (int u = tid; u < units; u += blockDim.x) {
+            const int c = S.ne[u / G::SPLIT];
+            const int a = u % G::SPLIT;
+            const int s0 = S.start[c], s1 = s0 + S.cnt[c];
+            if constexpr (D == 3) {
+                const int cx = c % G::R, cy = (c / G::R) % G::R, cz = c / (G::R * G::R);
+                float am[16], a0[16], a1[16], a2[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
+                for (int q = s0; q < s1; ++q) {
+                    const float* pp = S.pay + S.order[q] * G::PS;
+                    const float alpha = pp[a];
+                    const float beta = alpha * (float(a - 1) - pp[O::F + 0]);
+                    const float fy = pp[O::F + 1], fz = pp[O::F + 2];
+                    const float* Am = pp + O::A;
+                    const float e0 = alpha * pp[O::MV + 0] + beta * Am[0];
+                    const float e1 = alpha * pp[O::MV + 1] + beta * Am[3];
+                    const float e2 = alpha * pp[O::MV + 2] + beta * Am[6];
+                    const float f0 = alpha * Am[1], f1 = alpha * Am[4], f2 = alpha * Am[7];
+                    const float g0 = alpha * Am[2], g1 = alpha * Am[5], g2 = alpha * Am[8];
+                    const float ma = pp[O::M] * alpha;
+                    float Z[4], Zd[4];
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) { Z[cc] = pp[8 + cc]; Zd[cc] = Z[cc] * (float(cc - 1) - fz); }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const float Y = pp[4 + b], Yd = Y * (float(b - 1) - fy);
+                        const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
+                        const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int idx = b * 4 + cc;
+                            am[idx] += mY * Z[cc];
+                            a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
+                            a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
+                            a2[idx] += h2 * Z[cc] + k2 * Zd[cc];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) {
+                        const int idx = b * 4 + cc;
+                        const int nd = (cx + a) + G::NR * ((cy + b) + G::NR * (cz + cc));
+                        const long long q0 = to_fixed(am[idx], C.sm, status);
+                        const long long q1 = to_fixed(a0[idx], C.sp, status);
+                        const long long q2 = to_fixed(a1[idx], C.sp, status);
+                        const long long q3 = to_fixed(a2[idx], C.sp, status);
+                        if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
+                        if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
+                        if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
+                        if (q3) atomicAdd(&S.tile[3 * G::NN + nd], (unsigned long long)q3);
+                    }
+            } else {
+                const int cx = c % G::R, cy = c / G::R;
+                float am[16], a0[16], a1[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
+                for (int q = s0; q < s1; ++q) {
+                    const float* pp = S.pay + S.order[q] * G::PS;
+                    const float fx = pp[O::F + 0], fy = pp[O::F + 1];
+                    const float* Am = pp + O::A;
+                    const float mv0 = pp[O::MV + 0], mv1 = pp[O::MV + 1], m = pp[O::M];
+                    float Y[4], Yd[4];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) { Y[b] = pp[4 + b]; Yd[b] = Y[b] * (float(b - 1) - fy); }
+#pragma unroll
+                    for (int aa = 0; aa < 4; ++aa) {
+                        const float X = pp[aa], Xd = X * (float(aa - 1) - fx);
+                        const float e0 = mv0 * X + Am[0] * Xd, e1 = mv1 * X + Am[2] * Xd;
+                        const float f0 = Am[1] * X, f1 = Am[3] * X, mX = m * X;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            const int idx = aa * 4 + b;
+                            am[idx] += mX * Y[b];
+                            a0[idx] += e0 * Y[b] + f0 * Yd[b];
+                            a1[idx] += e1 * Y[b] + f1 * Yd[b];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int idx = aa * 4 + b;
+                        const int nd = (cx + aa) + G::NR * (cy + b);
+                        const long long q0 = to_fixed(am[idx], C.sm, status);
+                        const long long q1 = to_fixed(a0[idx], C.sp, status);
+                        const long long q2 = to_fixed(a1[idx], C.sp, status);
+                        if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
+                        if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
+                        if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
+                    }
+            }
+        }
+        __syncthreads();
+
+        // Phase D: shared tile -> global int64 sums (nodes outside the grid are
+        // dropped, as the reference skips them), clear, mark node blocks.
+        int nlo[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < D; ++k) nlo[k] = rlo[k] - 1;
+        bool outside = false;
+        for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) {
+            const unsigned long long v = S.tile[e];
+            if (v == 0ull) continue;
+            S.tile[e] = 0ull;
+            const int ch = e / G::NN, nd = e % G::NN;
+            int g[3] = {0, 0, 0}, rem = nd;
+            bool in = true;
+            int bb = 0, mul = 1;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                g[k] = nlo[k] + rem % G::NR;
+                rem /= G::NR;
+                in = in && g[k] >= 0 && g[k] <= ext[k];
+                bb += mul * (g[k] / G::T - (tc[k] - 1));
+                mul *= 3;
+            }
+            if (!in) { outside = true; continue; }
+            const long long gid = ((long long)g[2] * C.ny + g[1]) * C.nx + g[0];
+            atomicAdd(&acc[ch * C.nodes + gid], v);
+            if (ch == 0) atomicOr(&S.blockmask, 1u << bb);
+        }
+        if (outside) raise_flag(status, 4u);
+        __syncthreads();
+        if (tid < (D == 3 ? 27 : 9) && (S.blockmask >> tid) & 1u) {
+            int b[3] = {0, 0, 0}, rem = tid, gb = 0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) { b[k] = tc[k] - 1 + rem % 3; rem /= 3; }
+#pragma unroll
+            for (int k = D - 1; k >= 0; --k) gb = gb * TI.nblk[k] + b[k];
+            mark_block(TI, gb);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grid update over the node blocks P2G marked (reads and clears the int64 sums).
+template <int D, int FORM>
+__global__ void __launch_bounds__(256) k_grid_marked(StepConsts C, TileInfo TI, unsigned long long* __restrict__ acc,
+                                                     float4* __restrict__ gv, unsigned* __restrict__ status) {
+    using G = TileGeom<D>;
+    const int nb = *TI.n_marked;
+    const long long total = (long long)nb * G::BN;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+         w += (long long)gridDim.x * blockDim.x) {
+        const int blk = TI.mark_list[w / G::BN];
+        const int loc = int(w % G::BN);
+        int b[3] = {0, 0, 0}, l[3] = {0, 0, 0}, rb = blk, rl = loc;
+#pragma unroll
+        for (int k = 0; k < D; ++k) { b[k] = rb % TI.nblk[k]; rb /= TI.nblk[k]; l[k] = rl % G::T; rl /= G::T; }
+        const int gx = b[0] * G::T + l[0], gy = b[1] * G::T + l[1], gz = D == 3 ? b[2] * G::T + l[2] : 0;
+        if (loc == 0) TI.mark[blk] = 0;
+        if (gx >= C.nx || gy >= C.ny || gz >= C.nz) continue;
+        grid_node<D, FORM>(C, acc, gv, status, ((long long)gz * C.ny + gy) * C.nx + gx);
+    }
+}
+
+__global__ void k_reset_marks(TileInfo TI) { *TI.n_marked = 0; }
+
+}  // namespace mpm

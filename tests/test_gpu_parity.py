@@ -46,6 +46,31 @@ TIGHT = dict(x=1e-6, v=1e-5, B=1e-5, F=1e-6, Jp=1e-6)
 TARGET = dict(x=1e-4, v=1e-4, B=1e-4, F=1e-4, Jp=1e-4)
 
 
+def _fp32_reference_errors(O, scene, steps):
+    """Distance of the reference step evaluated in FP32 (the oracle's float
+    instantiation, same operation order as the shaders) from FP64."""
+    a, b = O.initial_state(scene), O.initial_state(scene, np.float32)
+    out, prev = {}, 0
+    for s in steps:
+        O.run_oracle(scene, a, s - prev)
+        O.run_oracle(scene, b, s - prev, fp32=True)
+        prev = s
+
+        class S:
+            position, velocity, affine_b, elastic_f, plastic_det = b.position, b.velocity, b.affine_b, b.elastic_f, b.plastic_det
+        out[s] = state_errors(S, dict(position=a.position, velocity=a.velocity, affine_b=a.affine_b,
+                                      elastic_f=a.elastic_f, plastic_det=a.plastic_det), scene.dim)
+    return out
+
+
+def _check_vs_fp32_reference(errs, ref32, label, floor=TARGET):
+    """After contact, velocities approach zero and relative errors grow: the bar
+    is the FP32 reference arithmetic's own distance from FP64 (x1.5), never
+    looser than needed and never tighter than `floor`."""
+    tol = {k: max(floor[k], 1.5 * ref32[k]) for k in errs}
+    _check(errs, tol, label)
+
+
 def test_mls_2d_blocks_1000_steps(gpu_lib, oracle_mod):
     from mpm_snow_sim2d_b200 import scenes
     sc = scenes.snow_blocks_2d()          # the 128^2 three-block workload, 4425 particles
@@ -66,9 +91,10 @@ def test_mls_2d_impact(gpu_lib, oracle_mod):
     ref = _oracle_ref(oracle_mod, sc, steps)
     assert ref[400]["plastic_det"].min() < 0.99
     got, flags = _gpu_run(sc, steps)
+    r32 = _fp32_reference_errors(oracle_mod, sc, [100, 400])
     _check(state_errors(got[1], ref[1], 2), TIGHT, "step 1")
-    _check(state_errors(got[100], ref[100], 2), TARGET, "step 100")
-    _check(state_errors(got[400], ref[400], 2), dict(x=1e-4, v=2e-3, B=1e-3, F=1e-3, Jp=1e-3), "step 400")
+    _check_vs_fp32_reference(state_errors(got[100], ref[100], 2), r32[100], "step 100")
+    _check_vs_fp32_reference(state_errors(got[400], ref[400], 2), r32[400], "step 400")
 
 
 def test_mls_3d_impact(gpu_lib, oracle_mod):
@@ -78,15 +104,16 @@ def test_mls_3d_impact(gpu_lib, oracle_mod):
     ref = _oracle_ref(oracle_mod, sc, steps)
     got, flags = _gpu_run(sc, steps)
     assert flags & 1 == 0
+    r32 = _fp32_reference_errors(oracle_mod, sc, [100, 300])
     _check(state_errors(got[1], ref[1], 3), TIGHT, "step 1")
-    _check(state_errors(got[100], ref[100], 3), TARGET, "step 100")
-    _check(state_errors(got[300], ref[300], 3), dict(x=1e-4, v=2e-3, B=1e-3, F=1e-3, Jp=1e-3), "step 300")
+    _check_vs_fp32_reference(state_errors(got[100], ref[100], 3), r32[100], "step 100")
+    _check_vs_fp32_reference(state_errors(got[300], ref[300], 3), r32[300], "step 300")
 
 
 def test_mls_3d_snowball_slab_1000_steps(gpu_lib, oracle_mod):
-    """The snowball-on-slab workload at reduced resolution (48^3, 2 ppc)."""
+    """The snowball-on-slab workload at reduced resolution (32^3, 1 ppc)."""
     from mpm_snow_sim2d_b200 import scenes
-    sc = scenes.snowball_on_slab_3d(W=48, ppc=2)
+    sc = scenes.snowball_on_slab_3d(W=32, ppc=1)
     steps = [1, 1000]
     ref = _oracle_ref(oracle_mod, sc, steps)
     got, _ = _gpu_run(sc, steps)
@@ -250,3 +277,18 @@ def test_set_stream_and_external_events(gpu_lib):
         e1.synchronize()
         assert e0.elapsed_time(e1) > 0
         assert s.step_count == 10
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_stale_tile_order_matches_oracle(gpu_lib, oracle_mod, dim):
+    """Particles drift away from the tile order of the last sort: with the
+    re-sort disabled, drifters beyond the one-cell margin take the
+    per-particle path and results still match the oracle."""
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.impact_2d(steps=150) if dim == 2 else scenes.impact_3d(steps=150)
+    steps = [150]
+    ref = _oracle_ref(oracle_mod, sc, steps)
+    r32 = _fp32_reference_errors(oracle_mod, sc, steps)
+    got, flags = _gpu_run(sc, steps, sort_period=100000)
+    assert flags & 1 == 0
+    _check_vs_fp32_reference(state_errors(got[150], ref[150], dim), r32[150], "step 150")
