@@ -2,6 +2,7 @@
 // step sequence, state import/export and checkpoints. The product path has no
 // CPU fallback: without a usable sm_100 device every create fails.
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -46,6 +47,8 @@ struct mpm_solver {
     int p2g_grid = 0;
     TileInfo ti{};
     SortBuffers alt{};
+    bool p2g_direct = false;  // P2G flush per unit to global (else via a shared tile)
+    SlowQueue q{};
 };
 
 namespace {
@@ -101,10 +104,15 @@ void release(mpm_solver* s) {
         if (p) cudaFree(p);
     if (s->alt.id) cudaFree(s->alt.id);
     int* ti[] = {s->ti.key, s->ti.tile_count, s->ti.tile_cursor, s->ti.tile_start, s->ti.n_items, s->ti.mark,
-                 s->ti.mark_list, s->ti.n_marked, s->ti.n_orphans};
+                 s->ti.mark_list, s->ti.n_marked, s->ti.n_orphans, s->ti.perm, s->ti.tile_list, s->ti.n_tile_list,
+                 s->ti.sval};
+    if (s->ti.skey) cudaFree(s->ti.skey);
     for (int* p : ti)
         if (p) cudaFree(p);
     if (s->ti.items) cudaFree(s->ti.items);
+    if (s->q.list) cudaFree(s->q.list);
+    if (s->q.count) cudaFree(s->q.count);
+    if (s->q.fh) cudaFree(s->q.fh);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -145,7 +153,8 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
     k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
     k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
-    k_sort_scatter<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->ti);
+    k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
+    k_tile_sort<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     std::swap(s->x, s->alt.x);
@@ -160,14 +169,34 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
     return cudaSuccess;
 }
 
+template <int D> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
+    if (s->p2g_direct)
+        k_p2g_tiled<D, true><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D, true>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->acc, s->status);
+    else
+        k_p2g_tiled<D, false><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D, false>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->acc, s->status);
+    return cudaGetLastError();
+}
+
+// G2P of the tiled MLS path: gather + in-band return map, then the queued
+// particles' full return map.
+template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
+    if (s->n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return e;
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_g2p_gather<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
+    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->q, s->status);
+    return cudaGetLastError();
+}
+
 template <int D> cudaError_t launch_p2g_tiled(mpm_solver* s) {
     if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) {
         cudaError_t e = launch_sort<D>(s);
         if (e != cudaSuccess) return e;
     }
-    k_p2g_tiled<D><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D>), s->stream>>>(particle_view(s), s->id, s->C, s->ti,
-                                                                                 s->acc, s->status);
-    return cudaGetLastError();
+    return launch_p2g_tiled_kernel<D>(s);
 }
 
 template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
@@ -184,7 +213,7 @@ template <int D> cudaError_t step_tiled(mpm_solver* s) {
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
-    return launch_g2p<D, kMLS>(s);
+    return launch_g2p_split<D>(s);
 }
 
 template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
@@ -217,6 +246,20 @@ cudaError_t clear_after_p2g(mpm_solver* s) {
     return cudaMemsetAsync(s->acc, 0, sizeof(unsigned long long) * nacc(s->dim, s->form) * s->nodes, s->stream);
 }
 
+template <int D> cudaError_t p2g_occupancy(bool direct, int* per_sm) {
+    cudaError_t e;
+    if (direct) {
+        const size_t smem = sizeof(P2GSmem<D, true>);
+        e = cudaFuncSetAttribute(k_p2g_tiled<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_p2g_tiled<D, true>, kTileThreads, smem);
+    } else {
+        const size_t smem = sizeof(P2GSmem<D, false>);
+        e = cudaFuncSetAttribute(k_p2g_tiled<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_p2g_tiled<D, false>, kTileThreads, smem);
+    }
+    return e;
+}
+
 // Tiles, work items, node-block marks and the sort's alternate buffers.
 mpm_status setup_tiled(mpm_solver* s) {
     const int D = s->dim, n = s->n;
@@ -237,6 +280,8 @@ mpm_status setup_tiled(mpm_solver* s) {
         dalloc(&ti.tile_cursor, (size_t)ti.n_tiles) || dalloc(&ti.tile_start, (size_t)ti.n_tiles) ||
         dalloc(&ti.items, max_items) || dalloc(&ti.n_items, 1) || dalloc(&ti.mark, (size_t)ti.n_blocks) ||
         dalloc(&ti.mark_list, (size_t)ti.n_blocks) || dalloc(&ti.n_marked, 1) || dalloc(&ti.n_orphans, 1) ||
+        dalloc(&ti.perm, (size_t)n) || dalloc(&ti.tile_list, (size_t)ti.n_tiles) || dalloc(&ti.n_tile_list, 1) ||
+        dalloc(&ti.skey, (size_t)n) || dalloc(&ti.sval, (size_t)n) ||
         dalloc(&s->alt.x, (size_t)n * D) || dalloc(&s->alt.v, (size_t)n * D) || dalloc(&s->alt.B, (size_t)n * D * D) ||
         dalloc(&s->alt.Fe, (size_t)n * D * D) || dalloc(&s->alt.Jp, (size_t)n) || dalloc(&s->alt.id, (size_t)n)) {
         cudaGetLastError();
@@ -255,15 +300,20 @@ mpm_status setup_tiled(mpm_solver* s) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     s->sms = sms > 0 ? sms : 148;
-    const size_t smem = D == 3 ? sizeof(P2GSmem<3>) : sizeof(P2GSmem<2>);
-    cudaError_t e = D == 3 ? cudaFuncSetAttribute(k_p2g_tiled<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                           : cudaFuncSetAttribute(k_p2g_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return MPM_ERR_CUDA;
+    const char* env = std::getenv("MPM_P2G_DIRECT");
+    s->p2g_direct = env && env[0] == '1';
     int per_sm = 0;
-    e = D == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g_tiled<3>, kTileThreads, smem)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p2g_tiled<2>, kTileThreads, smem);
+    cudaError_t e = cudaSuccess;
+    if (D == 3) e = p2g_occupancy<3>(s->p2g_direct, &per_sm);
+    else e = p2g_occupancy<2>(s->p2g_direct, &per_sm);
     if (e != cudaSuccess || per_sm < 1) return MPM_ERR_CUDA;
     s->p2g_grid = s->sms * per_sm;
+    s->q.capacity = n > 0 ? n : 1;
+    if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 1) ||
+        dalloc(&s->q.fh, (size_t)s->q.capacity * D * D)) {
+        cudaGetLastError();
+        return MPM_ERR_OUT_OF_MEMORY;
+    }
     s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 8;
     s->needs_sort = true;
     return MPM_OK;
@@ -385,17 +435,13 @@ template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
         if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) return launch_sort<D>(s);
         return cudaSuccess;
     }
-    if (k == 1) {
-        k_p2g_tiled<D><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D>), s->stream>>>(particle_view(s), s->id, s->C,
-                                                                                     s->ti, s->acc, s->status);
-        return cudaGetLastError();
-    }
+    if (k == 1) return launch_p2g_tiled_kernel<D>(s);
     if (k == 2) {
         cudaError_t e = launch_grid_marked<D>(s);
         if (e != cudaSuccess) return e;
         return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
     }
-    return launch_g2p<D, kMLS>(s);
+    return launch_g2p_split<D>(s);
 }
 cudaError_t dispatch_stage(mpm_solver* s, int k) {
     if (s->tiled) return s->dim == 2 ? stage_tiled<2>(s, k) : stage_tiled<3>(s, k);
@@ -680,8 +726,12 @@ mpm_status mpm_get_fixed_point(const mpm_solver* s, int32_t* lm, int32_t* lp) {
     return MPM_OK;
 }
 
-// Checkpoint: "MPMS" | u32 version=1 | i32 dim | i64 count | i32 W, H, D |
+// Checkpoint: "MPMS" | u32 version=2 | i32 dim | i64 count | i32 W, H, D |
 // u64 params hash | i64 step | f32 x[n*d] v[n*d] B[n*d*d] Fe[n*d*d] Jp[n]
+// (creation order) | u32 has_order | [i32 slot_id[n] | i32 n_items |
+// i32x4 items[n_items]]. The slot order and work items of the tiled path are
+// saved so that a resumed run groups particles exactly as the original did and
+// continues bit-identically.
 mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
     const int D = s->dim;
@@ -690,9 +740,22 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     mpm_state_host st{(int64_t)n, x.data(), v.data(), B.data(), Fe.data(), Jp.data()};
     mpm_status r = mpm_get_state(s, &st);
     if (r != MPM_OK) return r;
+    const uint32_t has_order = (s->tiled && !s->needs_sort) ? 1u : 0u;
+    std::vector<int> ids;
+    std::vector<int4> items;
+    int n_items = 0;
+    if (has_order) {
+        ids.resize(n);
+        MPM_CUDA(s, cudaMemcpyAsync(ids.data(), s->id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+        MPM_CUDA(s, cudaMemcpyAsync(&n_items, s->ti.n_items, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+        items.resize(n_items);
+        if (n_items > 0)
+            MPM_CUDA(s, cudaMemcpy(items.data(), s->ti.items, sizeof(int4) * n_items, cudaMemcpyDeviceToHost));
+    }
     FILE* f = std::fopen(path, "wb");
     if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
-    const uint32_t ver = 1;
+    const uint32_t ver = 2;
     const int32_t dim = D, ext[3] = {s->params.width, s->params.height, D == 3 ? s->params.depth : 0};
     const int64_t count = (int64_t)n, step = s->step;
     const uint64_t h = params_hash(s->params);
@@ -701,6 +764,11 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
               std::fwrite(&step, 8, 1, f) == 1;
     for (auto* vec : {&x, &v, &B, &Fe, &Jp})
         ok = ok && std::fwrite(vec->data(), sizeof(float), vec->size(), f) == vec->size();
+    ok = ok && std::fwrite(&has_order, 4, 1, f) == 1;
+    if (has_order) {
+        ok = ok && std::fwrite(ids.data(), sizeof(int), n, f) == n && std::fwrite(&n_items, 4, 1, f) == 1 &&
+             std::fwrite(items.data(), sizeof(int4), items.size(), f) == items.size();
+    }
     ok = (std::fclose(f) == 0) && ok;
     return ok ? MPM_OK : fail(s, MPM_ERR_IO, "short write");
 }
@@ -717,7 +785,7 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     bool ok = std::fread(magic, 1, 4, f) == 4 && std::fread(&ver, 4, 1, f) == 1 && std::fread(&dim, 4, 1, f) == 1 &&
               std::fread(&count, 8, 1, f) == 1 && std::fread(ext, 4, 3, f) == 3 && std::fread(&h, 8, 1, f) == 1 &&
               std::fread(&step, 8, 1, f) == 1;
-    if (!ok || std::memcmp(magic, "MPMS", 4) != 0 || ver != 1) { std::fclose(f); return fail(s, MPM_ERR_IO, "not a checkpoint"); }
+    if (!ok || std::memcmp(magic, "MPMS", 4) != 0 || (ver != 1 && ver != 2)) { std::fclose(f); return fail(s, MPM_ERR_IO, "not a checkpoint"); }
     if (dim != s->dim || count != s->n || ext[0] != s->params.width || ext[1] != s->params.height ||
         (dim == 3 && ext[2] != s->params.depth) || h != params_hash(s->params)) {
         std::fclose(f);
@@ -727,11 +795,44 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     const size_t n = (size_t)count;
     std::vector<float> x(n * D), v(n * D), B(n * D * D), Fe(n * D * D), Jp(n);
     for (auto* vec : {&x, &v, &B, &Fe, &Jp}) ok = ok && std::fread(vec->data(), sizeof(float), vec->size(), f) == vec->size();
+    uint32_t has_order = 0;
+    std::vector<int> ids;
+    std::vector<int4> items;
+    int n_items = 0;
+    if (ok && ver == 2) {
+        ok = std::fread(&has_order, 4, 1, f) == 1;
+        if (ok && has_order) {
+            ids.resize(n);
+            ok = std::fread(ids.data(), sizeof(int), n, f) == n && std::fread(&n_items, 4, 1, f) == 1 && n_items >= 0 &&
+                 (size_t)n_items <= n / kItem + (size_t)s->ti.n_tiles + 1;
+            if (ok) {
+                items.resize(n_items);
+                ok = std::fread(items.data(), sizeof(int4), items.size(), f) == items.size();
+            }
+            // every slot must name a distinct particle and every item a slot range
+            std::vector<char> seen(ok ? n : 0, 0);
+            for (size_t i = 0; ok && i < n; ++i) {
+                ok = ids[i] >= 0 && (size_t)ids[i] < n && !seen[ids[i]];
+                if (ok) seen[ids[i]] = 1;
+            }
+            for (int i = 0; ok && i < n_items; ++i)
+                ok = items[i].x >= 0 && items[i].x < s->ti.n_tiles && items[i].y >= 0 && items[i].z > 0 &&
+                     items[i].z <= kItem && (size_t)items[i].y + items[i].z <= n;
+        }
+    }
     std::fclose(f);
-    if (!ok) return fail(s, MPM_ERR_IO, "truncated checkpoint");
+    if (!ok) return fail(s, MPM_ERR_IO, "truncated or corrupt checkpoint");
+    const bool restore_order = has_order && s->tiled;
+    if (restore_order && n > 0)
+        MPM_CUDA(s, cudaMemcpy(s->id, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     mpm_state_host st{(int64_t)n, x.data(), v.data(), B.data(), Fe.data(), Jp.data()};
     mpm_status r = mpm_set_state(s, &st);
     if (r != MPM_OK) return r;
+    if (restore_order) {
+        if (n_items > 0) MPM_CUDA(s, cudaMemcpy(s->ti.items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice));
+        MPM_CUDA(s, cudaMemcpy(s->ti.n_items, &n_items, sizeof(int), cudaMemcpyHostToDevice));
+        s->needs_sort = false;
+    }
     s->step = step;
     return MPM_OK;
 }

@@ -472,6 +472,143 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 }
 
 // ---------------------------------------------------------------------------
+// G2P split in two for the MLS path. k_g2p_gather does the gather, APIC
+// update and the return map of every particle whose trial F is proven inside
+// the elastic band by the FP32 Gershgorin test (the map is then the identity);
+// the others are queued with their trial F for k_g2p_plastic, which runs the
+// full return map (FP64 band test, else the SVD). The split keeps the SVD's
+// registers out of the gather kernel so that it runs at higher occupancy.
+struct SlowQueue {
+    int* list;    // slots needing the full return map
+    int* count;   // device scalar
+    float* fh;    // trial F per queue entry, [D*D][capacity]
+    int capacity;
+};
+
+template <int D>
+__global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+                                                       SlowQueue Q, unsigned* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
+    const int ext[3] = {C.W, C.H, C.Dp};
+    int base[3] = {0, 0, 0};
+    float wk[3][4], off[3][4];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        base[k] = stencil_base(x[k], ext[k]);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const float dist = x[k] - float(base[k] + o);
+            wk[k][o] = bspline_n(dist);
+            off[k][o] = -dist;
+        }
+    }
+    float nv[D], nx[D], nB[D * D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) { nv[k] = 0.f; nx[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
+    const int nzs = (D == 3) ? 4 : 1;
+    float wsum = 0.f;
+    bool clipped = false;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int ix = base[0] + a;
+        if (ix < 0 || ix > ext[0]) { clipped = true; continue; }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int iy = base[1] + b;
+            if (iy < 0 || iy > ext[1]) { clipped = true; continue; }
+            const float wab = wk[0][a] * wk[1][b];
+#pragma unroll
+            for (int c = 0; c < nzs; ++c) {
+                const int iz = (D == 3) ? base[2] + c : 0;
+                if (D == 3 && (iz < 0 || iz > ext[2])) { clipped = true; continue; }
+                const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
+                const float w = (D == 3) ? wab * wk[2][c] : wab;
+                const float d[3] = {off[0][a], off[1][b], D == 3 ? off[2][c] : 0.f};
+                wsum += w;
+                float vf[3], vc[3];
+                if (D == 2) {
+                    const float4 g = __ldg(&gv[cid]);
+                    vf[0] = g.x; vf[1] = g.y; vc[0] = g.z; vc[1] = g.w;
+                } else {
+                    const float4 g0 = __ldg(&gv[2 * cid]), g1 = __ldg(&gv[2 * cid + 1]);
+                    vf[0] = g0.x; vf[1] = g0.y; vf[2] = g0.z; vc[0] = g1.x; vc[1] = g1.y; vc[2] = g1.z;
+                }
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    const float wv = w * vf[r];
+                    nv[r] += wv;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) nB[r * D + k] += wv * d[k];
+                    nx[r] += (d[r] + C.dt * vc[r]) * w;
+                }
+            }
+        }
+    }
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const float xn = (clipped ? x[k] * wsum : x[k]) + nx[k];
+        P.v[k * n + i] = nv[k];
+        P.x[k * n + i] = xn;
+        finite = finite && isfinite(xn);
+    }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.B[k * n + i] = nB[k];
+    float Fe[D * D], Fh[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) Fe[k] = P.Fe[k * n + i];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            float s = Fe[r * D + c];
+#pragma unroll
+            for (int k = 0; k < D; ++k) s += (C.dt * 3.f * nB[r * D + k]) * Fe[k * D + c];
+            Fh[r * D + c] = s;
+        }
+    if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s)) {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fh[k];
+    } else {
+        const unsigned act = __activemask();
+        const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+        int slot = 0;
+        if (lane == leader) slot = atomicAdd(Q.count, __popc(act));
+        slot = __shfl_sync(act, slot, leader) + __popc(act & ((1u << lane) - 1));
+        Q.list[slot] = i;
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
+    }
+    if (!finite) raise_flag(status, 1u);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, SlowQueue Q,
+                                                     unsigned* __restrict__ status) {
+    const int m = *Q.count;
+    const int n = P.n;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const int i = Q.list[e];
+        float Fh[D * D], Fe[D * D];
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) Fh[k] = Q.fh[k * Q.capacity + e];
+        float Jp = P.Jp[i];
+        plasticity<D, kMLS>(C, Fh, Fe, Jp, status);
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
+        P.Jp[i] = Jp;
+        if (!isfinite(Jp)) raise_flag(status, 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Import / export between the caller's interleaved per-particle arrays (in
 // creation order) and the device SoA (in slot order; slot s holds particle id[s]).
 __global__ void k_export_soa(const float* __restrict__ soa, int comps, int n, const int* __restrict__ id,

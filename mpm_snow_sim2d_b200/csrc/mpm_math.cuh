@@ -333,8 +333,7 @@ template <int D, int FORM> __device__ __forceinline__ void hardened_stress_polar
 // decide, Sylvester's criterion in FP64 for (t1^2 - 1e-5) I - S and
 // S - (t0^2 + 1e-5) I (positive leading minors); 1e-5 exceeds the FP64
 // rounding of the minors even for a triple eigenvalue at the margin.
-template <int D> __device__ __forceinline__ bool in_elastic_band(const float* F, float t0, float t1) {
-    if (!(det<D>(F) > 0.f)) return false;
+template <int D> __device__ __forceinline__ bool band_gershgorin(const float* F, float t0, float t1) {
     float S[D * D];
 #pragma unroll
     for (int i = 0; i < D; ++i)
@@ -355,7 +354,12 @@ template <int D> __device__ __forceinline__ bool in_elastic_band(const float* F,
             if (j != i) r += fabsf(S[i * D + j]);
         gersh = gersh && (S[i * D + i] - r >= lo) && (S[i * D + i] + r <= hi);
     }
-    if (gersh) return true;
+    return gersh;
+}
+
+template <int D> __device__ __forceinline__ bool in_elastic_band(const float* F, float t0, float t1) {
+    if (!(det<D>(F) > 0.f)) return false;
+    if (band_gershgorin<D>(F, t0, t1)) return true;
     double Sd[D * D];
 #pragma unroll
     for (int i = 0; i < D; ++i)

@@ -2,14 +2,17 @@
 // cell in registers and per tile in shared memory, and a grid update that only
 // visits node blocks P2G touched.
 //
-// Tiles are T^D cells (3D: 4^3, 2D: 8^2). Every `sort_period` steps a counting
-// sort moves the particle state into tile order (k_sort_*); between sorts a
+// Tiles are T^D cells (3D: 4^3, 2D: 8^2). Every `sort_period` steps (counted
+// in absolute steps) a sort moves the particle state into the order
+// (tile, cell in tile, particle id), which depends on the state alone
+// (k_sort_count, k_sort_scan, k_sort_bucket, k_tile_sort). Between sorts a
 // particle may drift M = 1 cell out of its tile and is still handled by its
 // tile's CTA; farther drifters ("orphans") take a per-particle path with global
-// atomics. Determinism: inside a CTA the particles of one cell are accumulated
-// in particle-id order in FP32, every cross-cell / cross-CTA sum is an int64
-// fixed-point atomic, so grid sums are bit-identical run to run whatever order
-// the sort's atomics produce.
+// atomics. Determinism: work items are fixed slices of that order; inside a
+// CTA the particles of one cell are accumulated in particle-id order in FP32;
+// every cross-cell / cross-CTA sum is an int64 fixed-point atomic. Grid sums
+// are therefore bit-identical run to run, and a checkpoint that carries the
+// slot order resumes bit-identically.
 #pragma once
 
 #include "mpm_kernels.cuh"
@@ -44,6 +47,11 @@ struct TileInfo {
     int* mark_list;    // touched node blocks
     int* n_marked;     // device scalar
     int* n_orphans;    // device scalar, diagnostics (accumulates)
+    int* perm;         // sort scratch: slot order by tile (source slots)
+    int* tile_list;    // non-empty tiles of the last sort
+    int* n_tile_list;  // device scalar
+    unsigned long long* skey;  // global sort scratch (tiles above kSortSmem particles)
+    int* sval;
 };
 
 template <int D> __device__ __forceinline__ int cell_clamped(float x, int ext) {
@@ -108,9 +116,14 @@ __global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
         TI.tile_cursor[t] = 0;
         for (int j = 0; j < n; j += kItem) TI.items[ibase++] = make_int4(t, base + j, min(kItem, n - j), 0);
         base += n;
-        TI.tile_count[t] = 0;
     }
     if (tid == 1023) *TI.n_items = s_itm[1023];
+    // list of the non-empty tiles (any order; each tile is sorted independently)
+    __syncthreads();
+    if (tid == 0) *TI.n_tile_list = 0;
+    __syncthreads();
+    for (int t = lo; t < hi; ++t)
+        if (TI.tile_count[t] > 0) TI.tile_list[atomicAdd(TI.n_tile_list, 1)] = t;
 }
 
 struct SortBuffers {
@@ -118,12 +131,10 @@ struct SortBuffers {
     int* id;
 };
 
-template <int D>
-__global__ void __launch_bounds__(256) k_sort_scatter(Particles P, const int* __restrict__ id_src, SortBuffers dst,
-                                                      TileInfo TI) {
+// Bucket the source slots by tile (order inside a tile is fixed by k_tile_sort).
+__global__ void __launch_bounds__(256) k_sort_bucket(int n, TileInfo TI) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const int n = P.n;
+    if (i >= n) return;
     const int t = TI.key[i];
     const unsigned act = __activemask();
     const unsigned peers = __match_any_sync(act, t);
@@ -131,15 +142,77 @@ __global__ void __launch_bounds__(256) k_sort_scatter(Particles P, const int* __
     int base = 0;
     if (lane == leader) base = atomicAdd(&TI.tile_cursor[t], __popc(peers));
     base = __shfl_sync(peers, base, leader);
-    const int s = TI.tile_start[t] + base + __popc(peers & ((1u << lane) - 1));
+    TI.perm[TI.tile_start[t] + base + __popc(peers & ((1u << lane) - 1))] = i;
+}
+
+// Ascending bitonic sort of m (key, value) pairs, any m: the network of the
+// next power of two with every index >= m standing for +infinity (all merges
+// ascend, so such indices are never compared with a smaller key).
+template <typename K, typename V>
+__device__ void bitonic_sort_padded(K* key, V* val, int m) {
+    int np = 1;
+    while (np < m) np <<= 1;
+    for (int k = 2; k <= np; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < np; i += blockDim.x) {
+                const int l = (j == (k >> 1)) ? (i ^ (k - 1)) : (i ^ j);
+                if (l > i && l < m) {
+                    if (key[l] < key[i]) {
+                        const K tk = key[i]; key[i] = key[l]; key[l] = tk;
+                        const V tv = val[i]; val[i] = val[l]; val[l] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+constexpr int kSortSmem = 4096;  // particles per tile sorted in shared memory
+
+// One CTA per non-empty tile: order the tile's particles by (cell in tile,
+// particle id) -- a function of the state alone -- and gather their state into
+// the destination buffers in that order.
+template <int D>
+__global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __restrict__ id_src, SortBuffers dst,
+                                                   StepConsts C, TileInfo TI) {
+    constexpr int T = TileGeom<D>::T;
+    __shared__ unsigned long long s_key[kSortSmem];
+    __shared__ int s_val[kSortSmem];
+    const int n = P.n, ext[3] = {C.W, C.H, C.Dp};
+    const int ntl = *TI.n_tile_list;
+    for (int e = blockIdx.x; e < ntl; e += gridDim.x) {
+        const int t = TI.tile_list[e];
+        const int start = TI.tile_start[t];
+        const int m = TI.tile_count[t];
+        const bool in_smem = m <= kSortSmem;
+        unsigned long long* key = in_smem ? s_key : TI.skey + start;
+        int* val = in_smem ? s_val : TI.sval + start;
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const int src = TI.perm[start + j];
+            int cl = 0;
 #pragma unroll
-    for (int k = 0; k < D; ++k) { dst.x[k * n + s] = P.x[k * n + i]; dst.v[k * n + s] = P.v[k * n + i]; }
+            for (int k = D - 1; k >= 0; --k) cl = cl * T + cell_clamped<D>(P.x[k * n + src], ext[k]) % T;
+            key[j] = ((unsigned long long)cl << 32) | (unsigned)id_src[src];
+            val[j] = src;
+        }
+        __syncthreads();
+        bitonic_sort_padded(key, val, m);
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const int src = val[j], s = start + j;
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) { dst.B[k * n + s] = P.B[k * n + i]; dst.Fe[k * n + s] = P.Fe[k * n + i]; }
-    dst.Jp[s] = P.Jp[i];
-    dst.id[s] = id_src[i];
-    if (P.mass) dst.mass[s] = P.mass[i];
-    if (P.vol) dst.vol[s] = P.vol[i];
+            for (int k = 0; k < D; ++k) { dst.x[k * n + s] = P.x[k * n + src]; dst.v[k * n + s] = P.v[k * n + src]; }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) { dst.B[k * n + s] = P.B[k * n + src]; dst.Fe[k * n + s] = P.Fe[k * n + src]; }
+            dst.Jp[s] = P.Jp[src];
+            dst.id[s] = id_src[src];
+            if (P.mass) dst.mass[s] = P.mass[src];
+            if (P.vol) dst.vol[s] = P.vol[src];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) TI.tile_count[t] = 0;
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -164,11 +237,10 @@ template <int D> __device__ __forceinline__ void mark_stencil_blocks(const TileI
 
 // ---------------------------------------------------------------------------
 // Tiled P2G (MLS).
-template <int D> struct P2GSmem {
+template <int D, bool DIRECT> struct P2GSmem {
     using G = TileGeom<D>;
     float pay[kItem * G::PS];
     int lcell[kItem];
-    int pid[kItem];
     int order[kItem];
     int cnt[G::RC];
     int start[G::RC];
@@ -176,7 +248,7 @@ template <int D> struct P2GSmem {
     int ne[G::RC];
     int n_ne;
     unsigned blockmask;
-    unsigned long long tile[(1 + D) * G::NN];
+    unsigned long long tile[DIRECT ? 1 : (1 + D) * G::NN];
 };
 
 // Payload layout (floats) per particle:
@@ -221,18 +293,45 @@ __device__ __forceinline__ void scatter_orphan(const StepConsts& C, const TileIn
     mark_stencil_blocks<D>(TI, base);
 }
 
+// Node blocks (of T^D nodes, numbered relative to tile tc - 1 per axis) that
+// hold the in-grid nodes of a unit: x in [lx, lx + wx), y and z 4 nodes from
+// ly, lz (region-local node coordinates; region node 0 is cell rlo - 1).
 template <int D>
-__global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const int* __restrict__ pid_g, StepConsts C,
-                                                            TileInfo TI, unsigned long long* __restrict__ acc,
+__device__ __forceinline__ void unit_blocks(const int* rlo, int lx, int ly, int lz, int wx, const int* ext,
+                                            const int* tc, unsigned* mask) {
+    constexpr int T = TileGeom<D>::T;
+    const int l[3] = {lx, ly, lz}, wd[3] = {wx, 4, 4};
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int g0 = max(0, rlo[k] - 1 + l[k]), g1 = min(ext[k], rlo[k] - 1 + l[k] + wd[k] - 1);
+        if (g0 > g1) return;
+        lo[k] = g0 / T - (tc[k] - 1);
+        hi[k] = g1 / T - (tc[k] - 1);
+    }
+    unsigned bits = 0u;
+    for (int z = lo[2]; z <= (D == 3 ? hi[2] : 0); ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x) bits |= 1u << (x + 3 * y + 9 * z);
+    atomicOr(mask, bits);
+}
+
+// DIRECT: each (cell, x-offset) unit adds its 16 (2D: 16) node partial sums
+// straight to the global int64 sums; otherwise they are gathered in a shared
+// int64 tile first and flushed once per work item.
+template <int D, bool DIRECT>
+__global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, StepConsts C, TileInfo TI,
+                                                            unsigned long long* __restrict__ acc,
                                                             unsigned* __restrict__ status) {
     using G = TileGeom<D>;
     using O = PayOff<D>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    P2GSmem<D>& S = *reinterpret_cast<P2GSmem<D>*>(smem_raw);
+    P2GSmem<D, DIRECT>& S = *reinterpret_cast<P2GSmem<D, DIRECT>*>(smem_raw);
     const int tid = threadIdx.x;
     const int n = P.n;
     const int ext[3] = {C.W, C.H, C.Dp};
-    for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) S.tile[e] = 0ull;
+    if (!DIRECT)
+        for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) S.tile[e] = 0ull;
 
     const int n_items = *TI.n_items;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -298,7 +397,6 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
                 for (int k = 0; k < D * D; ++k) q[O::A + k] = A[k];
                 q[O::M] = mass;
                 S.lcell[j] = lc;
-                S.pid[j] = pid_g[i];
                 atomicAdd(&S.cnt[lc], 1);
             } else {
                 scatter_orphan<D>(C, TI, base, wk, f, mv, A, mass, acc, status);
@@ -307,7 +405,9 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
         }
         __syncthreads();
 
-        // Phase B: per-cell lists (exclusive scan by warp 0), cells ordered by id.
+        // Phase B (warp 0): exclusive scan of the cell counts, list of non-empty
+        // cells, and a stable placement of the particles into per-cell lists in
+        // slot order (deterministic: the slot order is the last sort's order).
         if (tid < 32) {
             int carry = 0;
             for (int c0 = 0; c0 < G::RC; c0 += 32) {
@@ -327,20 +427,15 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
                 __syncwarp();
                 carry += __shfl_sync(0xffffffffu, incl, 31);
             }
-        }
-        __syncthreads();
-        for (int j = tid; j < it.z; j += blockDim.x) {
-            const int lc = S.lcell[j];
-            if (lc >= 0) S.order[S.start[lc] + atomicAdd(&S.cur[lc], 1)] = j;
-        }
-        __syncthreads();
-        for (int e = tid; e < S.n_ne; e += blockDim.x) {  // insertion sort by particle id
-            const int c = S.ne[e], s0 = S.start[c], s1 = s0 + S.cnt[c];
-            for (int q = s0 + 1; q < s1; ++q) {
-                const int jj = S.order[q], key = S.pid[jj];
-                int r = q - 1;
-                while (r >= s0 && S.pid[S.order[r]] > key) { S.order[r + 1] = S.order[r]; --r; }
-                S.order[r + 1] = jj;
+            for (int j0 = 0; j0 < it.z; j0 += 32) {
+                const int j = j0 + tid;
+                const int lc = j < it.z ? S.lcell[j] : -1;
+                const unsigned peers = __match_any_sync(0xffffffffu, lc);
+                const int rank = __popc(peers & ((1u << tid) - 1));
+                if (lc >= 0) S.order[S.start[lc] + S.cur[lc] + rank] = j;
+                __syncwarp();
+                if (lc >= 0 && rank == 0) S.cur[lc] += __popc(peers);
+                __syncwarp();
             }
         }
         __syncthreads();
@@ -387,20 +482,34 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
                         }
                     }
                 }
+                if (DIRECT) unit_blocks<D>(rlo, cx + a, cy, cz, 1, ext, tc, &S.blockmask);
 #pragma unroll
                 for (int b = 0; b < 4; ++b)
 #pragma unroll
                     for (int cc = 0; cc < 4; ++cc) {
                         const int idx = b * 4 + cc;
-                        const int nd = (cx + a) + G::NR * ((cy + b) + G::NR * (cz + cc));
                         const long long q0 = to_fixed(am[idx], C.sm, status);
                         const long long q1 = to_fixed(a0[idx], C.sp, status);
                         const long long q2 = to_fixed(a1[idx], C.sp, status);
                         const long long q3 = to_fixed(a2[idx], C.sp, status);
-                        if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
-                        if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
-                        if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
-                        if (q3) atomicAdd(&S.tile[3 * G::NN + nd], (unsigned long long)q3);
+                        if (DIRECT) {
+                            const int gx = rlo[0] - 1 + cx + a, gy = rlo[1] - 1 + cy + b, gz = rlo[2] - 1 + cz + cc;
+                            if (gx < 0 || gx > ext[0] || gy < 0 || gy > ext[1] || gz < 0 || gz > ext[2]) {
+                                if (q0 | q1 | q2 | q3) raise_flag(status, 4u);
+                                continue;
+                            }
+                            const long long gid = ((long long)gz * C.ny + gy) * C.nx + gx;
+                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
+                            if (q1) atomicAdd(&acc[1 * C.nodes + gid], (unsigned long long)q1);
+                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
+                            if (q3) atomicAdd(&acc[3 * C.nodes + gid], (unsigned long long)q3);
+                        } else {
+                            const int nd = (cx + a) + G::NR * ((cy + b) + G::NR * (cz + cc));
+                            if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
+                            if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
+                            if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
+                            if (q3) atomicAdd(&S.tile[3 * G::NN + nd], (unsigned long long)q3);
+                        }
                     }
             } else {
                 const int cx = c % G::R, cy = c / G::R;
@@ -429,18 +538,31 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
                         }
                     }
                 }
+                if (DIRECT) unit_blocks<D>(rlo, cx, cy, 0, 4, ext, tc, &S.blockmask);
 #pragma unroll
                 for (int aa = 0; aa < 4; ++aa)
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
                         const int idx = aa * 4 + b;
-                        const int nd = (cx + aa) + G::NR * (cy + b);
                         const long long q0 = to_fixed(am[idx], C.sm, status);
                         const long long q1 = to_fixed(a0[idx], C.sp, status);
                         const long long q2 = to_fixed(a1[idx], C.sp, status);
-                        if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
-                        if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
-                        if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
+                        if (DIRECT) {
+                            const int gx = rlo[0] - 1 + cx + aa, gy = rlo[1] - 1 + cy + b;
+                            if (gx < 0 || gx > ext[0] || gy < 0 || gy > ext[1]) {
+                                if (q0 | q1 | q2) raise_flag(status, 4u);
+                                continue;
+                            }
+                            const long long gid = (long long)gy * C.nx + gx;
+                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
+                            if (q1) atomicAdd(&acc[1 * C.nodes + gid], (unsigned long long)q1);
+                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
+                        } else {
+                            const int nd = (cx + aa) + G::NR * (cy + b);
+                            if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
+                            if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
+                            if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
+                        }
                     }
             }
         }
@@ -452,7 +574,7 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, const i
 #pragma unroll
         for (int k = 0; k < D; ++k) nlo[k] = rlo[k] - 1;
         bool outside = false;
-        for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) {
+        for (int e = tid; !DIRECT && e < (1 + D) * G::NN; e += blockDim.x) {
             const unsigned long long v = S.tile[e];
             if (v == 0ull) continue;
             S.tile[e] = 0ull;

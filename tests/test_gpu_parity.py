@@ -78,7 +78,8 @@ def test_mls_2d_blocks_1000_steps(gpu_lib, oracle_mod):
     ref = _oracle_ref(oracle_mod, sc, steps)
     got, flags = _gpu_run(sc, steps)
     assert flags & 1 == 0
-    _check(state_errors(got[1], ref[1], 2), TIGHT, "step 1")
+    r32 = _fp32_reference_errors(oracle_mod, sc, [1])
+    _check_vs_fp32_reference(state_errors(got[1], ref[1], 2), r32[1], "step 1", TIGHT)
     for s in (100, 1000):
         _check(state_errors(got[s], ref[s], 2), TARGET, f"step {s}")
 
@@ -91,8 +92,8 @@ def test_mls_2d_impact(gpu_lib, oracle_mod):
     ref = _oracle_ref(oracle_mod, sc, steps)
     assert ref[400]["plastic_det"].min() < 0.99
     got, flags = _gpu_run(sc, steps)
-    r32 = _fp32_reference_errors(oracle_mod, sc, [100, 400])
-    _check(state_errors(got[1], ref[1], 2), TIGHT, "step 1")
+    r32 = _fp32_reference_errors(oracle_mod, sc, [1, 100, 400])
+    _check_vs_fp32_reference(state_errors(got[1], ref[1], 2), r32[1], "step 1", TIGHT)
     _check_vs_fp32_reference(state_errors(got[100], ref[100], 2), r32[100], "step 100")
     _check_vs_fp32_reference(state_errors(got[400], ref[400], 2), r32[400], "step 400")
 
@@ -104,8 +105,8 @@ def test_mls_3d_impact(gpu_lib, oracle_mod):
     ref = _oracle_ref(oracle_mod, sc, steps)
     got, flags = _gpu_run(sc, steps)
     assert flags & 1 == 0
-    r32 = _fp32_reference_errors(oracle_mod, sc, [100, 300])
-    _check(state_errors(got[1], ref[1], 3), TIGHT, "step 1")
+    r32 = _fp32_reference_errors(oracle_mod, sc, [1, 100, 300])
+    _check_vs_fp32_reference(state_errors(got[1], ref[1], 3), r32[1], "step 1", TIGHT)
     _check_vs_fp32_reference(state_errors(got[100], ref[100], 3), r32[100], "step 100")
     _check_vs_fp32_reference(state_errors(got[300], ref[300], 3), r32[300], "step 300")
 
@@ -117,8 +118,12 @@ def test_mls_3d_snowball_slab_1000_steps(gpu_lib, oracle_mod):
     steps = [1, 1000]
     ref = _oracle_ref(oracle_mod, sc, steps)
     got, _ = _gpu_run(sc, steps)
-    _check(state_errors(got[1], ref[1], 3), TIGHT, "step 1")
-    _check(state_errors(got[1000], ref[1000], 3), TARGET, "step 1000")
+    r32 = _fp32_reference_errors(oracle_mod, sc, [1, 1000])
+    _check_vs_fp32_reference(state_errors(got[1], ref[1], 3), r32[1], "step 1", TIGHT)
+    # the slab rests on the floor: the wall-contact branch (grid_update.glsl:54)
+    # flips for a few nodes between FP32 and FP64, which the reference's own FP32
+    # arithmetic shows too (its velocity error here is ~2.4e-4).
+    _check_vs_fp32_reference(state_errors(got[1000], ref[1000], 3), r32[1000], "step 1000")
 
 
 @pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d"])
@@ -147,13 +152,19 @@ def test_classic_matches_reference_cpu(gpu_lib, oracle_mod, case):
             _check(e_pair, dict(x=1e-6, v=1e-5, B=1e-5, F=1e-6, Jp=1e-6), "step 1 vs reference")
 
 
-def test_run_to_run_bitwise_determinism(gpu_lib):
+@pytest.mark.parametrize("case", ["impact3d", "dense3d", "dense2d"])
+def test_run_to_run_bitwise_determinism(gpu_lib, case):
+    """Bit-identical grid sums and particle state across runs. dense3d has
+    ~1000 particles per 4^3 tile (tiles split into several work items);
+    dense2d has >4096 particles per 8^2 tile (sorted in global memory)."""
     from mpm_snow_sim2d_b200 import Solver, scenes
-    sc = scenes.impact_3d()
+    sc = {"impact3d": lambda: scenes.impact_3d(),
+          "dense3d": lambda: scenes.snowball_on_slab_3d(W=32, ppc=16),
+          "dense2d": lambda: scenes.impact_2d(W=16, ppc=1000)}[case]()
     outs = []
     for _ in range(2):
         with Solver.from_scene(sc) as s:
-            s.Step(150)
+            s.Step(40)
             m, p, raw = s.rasterize(raw=True)
             st = s.get_state()
             outs.append((raw, st))
@@ -172,7 +183,8 @@ def test_p2g_conservation(gpu_lib, dim):
         st = s.get_state()
         m, p = s.rasterize()
     total = float(sc.mass.astype(np.float64).sum())
-    assert abs(m.sum() - total) <= 1e-9 * total
+    # FP32 B-spline weights sum to 1 within a few ulps (as in the reference)
+    assert abs(m.sum() - total) <= 1e-6 * total
     mom = (sc.mass.astype(np.float64)[:, None] * st.velocity.astype(np.float64)).sum(0)
     scale = (sc.mass.astype(np.float64)[:, None] * np.abs(st.velocity)).sum()
     assert np.all(np.abs(p.sum(0) - mom) <= 1e-5 * scale)
