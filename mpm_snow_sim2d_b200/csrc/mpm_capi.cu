@@ -25,7 +25,7 @@ struct mpm_solver {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     // particles (SoA)
-    float *x = nullptr, *v = nullptr, *B = nullptr, *Fe = nullptr, *Jp = nullptr;
+    float *x = nullptr, *v = nullptr, *B = nullptr, *Fe = nullptr, *Jp = nullptr, *A = nullptr;
     float *mass = nullptr, *vol = nullptr;
     float mass_u = 0.f, vol_u = 0.f;
     int* id = nullptr;
@@ -48,6 +48,7 @@ struct mpm_solver {
     TileInfo ti{};
     SortBuffers alt{};
     bool p2g_direct = false;  // P2G flush per unit to global (else via a shared tile)
+    bool needs_affine = true; // A must be recomputed from the state before the next P2G
     SlowQueue q{};
 };
 
@@ -92,14 +93,14 @@ template <typename T> cudaError_t dalloc(T** p, size_t count) {
 }
 
 void release(mpm_solver* s) {
-    float* fl[] = {s->x, s->v, s->B, s->Fe, s->Jp, s->mass, s->vol, s->staging};
+    float* fl[] = {s->x, s->v, s->B, s->Fe, s->Jp, s->A, s->mass, s->vol, s->staging};
     for (float* p : fl)
         if (p) cudaFree(p);
     if (s->id) cudaFree(s->id);
     if (s->acc) cudaFree(s->acc);
     if (s->gv) cudaFree(s->gv);
     if (s->status) cudaFree(s->status);
-    float* al[] = {s->alt.x, s->alt.v, s->alt.B, s->alt.Fe, s->alt.Jp, s->alt.mass, s->alt.vol};
+    float* al[] = {s->alt.x, s->alt.v, s->alt.B, s->alt.Fe, s->alt.Jp, s->alt.A, s->alt.mass, s->alt.vol};
     for (float* p : al)
         if (p) cudaFree(p);
     if (s->alt.id) cudaFree(s->alt.id);
@@ -118,7 +119,7 @@ void release(mpm_solver* s) {
 
 Particles particle_view(mpm_solver* s) {
     Particles P;
-    P.x = s->x; P.v = s->v; P.B = s->B; P.Fe = s->Fe; P.Jp = s->Jp;
+    P.x = s->x; P.v = s->v; P.B = s->B; P.Fe = s->Fe; P.Jp = s->Jp; P.A = s->A;
     P.mass = s->mass; P.vol = s->vol; P.mass_u = s->mass_u; P.vol_u = s->vol_u;
     P.n = s->n;
     return P;
@@ -162,6 +163,7 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
     std::swap(s->B, s->alt.B);
     std::swap(s->Fe, s->alt.Fe);
     std::swap(s->Jp, s->alt.Jp);
+    std::swap(s->A, s->alt.A);
     std::swap(s->id, s->alt.id);
     if (s->mass) std::swap(s->mass, s->alt.mass);
     if (s->vol) std::swap(s->vol, s->alt.vol);
@@ -191,7 +193,17 @@ template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
     return cudaGetLastError();
 }
 
+template <int D> cudaError_t prepare_affine(mpm_solver* s) {
+    if (!s->needs_affine || s->n == 0) { s->needs_affine = false; return cudaSuccess; }
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_prepare_affine<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C);
+    s->needs_affine = false;
+    return cudaGetLastError();
+}
+
 template <int D> cudaError_t launch_p2g_tiled(mpm_solver* s) {
+    cudaError_t e0 = prepare_affine<D>(s);
+    if (e0 != cudaSuccess) return e0;
     if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) {
         cudaError_t e = launch_sort<D>(s);
         if (e != cudaSuccess) return e;
@@ -283,7 +295,8 @@ mpm_status setup_tiled(mpm_solver* s) {
         dalloc(&ti.perm, (size_t)n) || dalloc(&ti.tile_list, (size_t)ti.n_tiles) || dalloc(&ti.n_tile_list, 1) ||
         dalloc(&ti.skey, (size_t)n) || dalloc(&ti.sval, (size_t)n) ||
         dalloc(&s->alt.x, (size_t)n * D) || dalloc(&s->alt.v, (size_t)n * D) || dalloc(&s->alt.B, (size_t)n * D * D) ||
-        dalloc(&s->alt.Fe, (size_t)n * D * D) || dalloc(&s->alt.Jp, (size_t)n) || dalloc(&s->alt.id, (size_t)n)) {
+        dalloc(&s->alt.Fe, (size_t)n * D * D) || dalloc(&s->alt.Jp, (size_t)n) || dalloc(&s->alt.id, (size_t)n) ||
+        dalloc(&s->A, (size_t)n * D * D) || dalloc(&s->alt.A, (size_t)n * D * D)) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
     }
@@ -432,6 +445,8 @@ template <int D, int FORM> cudaError_t stage(mpm_solver* s, int k) {
 }
 template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
     if (k == 0) {
+        cudaError_t e = prepare_affine<D>(s);
+        if (e != cudaSuccess) return e;
         if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) return launch_sort<D>(s);
         return cudaSuccess;
     }
@@ -667,6 +682,7 @@ mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
     if (st->elastic_f && (r = import_field(s, s->Fe, D * D, st->elastic_f)) != MPM_OK) return r;
     if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
     s->needs_sort = true;
+    s->needs_affine = true;
     return MPM_OK;
 }
 

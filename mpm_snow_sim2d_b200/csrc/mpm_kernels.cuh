@@ -33,6 +33,7 @@ struct Particles {
     float* B;
     float* Fe;
     float* Jp;
+    float* A;           // MLS path: P2G affine matrix of the next step (nullptr elsewhere)
     const float* mass;  // nullptr: uniform mass_u
     const float* vol;   // nullptr: uniform vol_u
     float mass_u, vol_u;
@@ -472,12 +473,41 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 }
 
 // ---------------------------------------------------------------------------
+// MLS affine matrix of one particle, the per-particle factor of the P2G
+// scatter (src/gpu/shaders/2d/p2g.glsl:44-90): A = 3 m B - 3 dt V sigma(F_E, J_p),
+// so that a node receives w (m v + A (x_i - x_p)). Computed by G2P for the next
+// step (and by k_prepare_affine after any state upload), always with this one
+// function, so the value depends on (B, F_E, J_p, m, V) alone.
+template <int D>
+__device__ __forceinline__ void mls_affine(const StepConsts& C, const float* B, const float* Fe, float Jp, float mass,
+                                           float vol, float* A) {
+    float sig[D * D];
+    hardened_stress_polar<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) A[k] = 3.f * mass * B[k] - 3.f * C.dt * vol * sig[k];
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_prepare_affine(Particles P, StepConsts C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    float B[D * D], Fe[D * D], A[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
+    mls_affine<D>(C, B, Fe, P.Jp[i], P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
+}
+
+// ---------------------------------------------------------------------------
 // G2P split in two for the MLS path. k_g2p_gather does the gather, APIC
 // update and the return map of every particle whose trial F is proven inside
-// the elastic band by the FP32 Gershgorin test (the map is then the identity);
-// the others are queued with their trial F for k_g2p_plastic, which runs the
-// full return map (FP64 band test, else the SVD). The split keeps the SVD's
-// registers out of the gather kernel so that it runs at higher occupancy.
+// the elastic band by the FP32 Gershgorin test (the map is then the identity),
+// and writes the next step's affine matrix; the others are queued with their
+// trial F for k_g2p_plastic, which runs the full return map (FP64 band test,
+// else the SVD) and then writes theirs. The split keeps the SVD's registers out
+// of the gather kernel so that it runs at higher occupancy.
 struct SlowQueue {
     int* list;    // slots needing the full return map
     int* count;   // device scalar
@@ -485,51 +515,111 @@ struct SlowQueue {
     int capacity;
 };
 
+// Interior gather: every stencil node inside the grid. The sums
+//   v = sum w vf,  B = sum w vf (x_i - x_p)^T,  x' = x + sum w (x_i - x_p) + dt sum w vc
+// are contracted axis by axis (z, then y, then x) with the separable weights.
 template <int D>
-__global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
-                                                       SlowQueue Q, unsigned* __restrict__ status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const int n = P.n;
-    float x[D];
+__device__ __forceinline__ void gather_interior(const StepConsts& C, const float4* __restrict__ gv, const int* base,
+                                                const float (*wk)[4], const float (*off)[4], float* nv, float* nB,
+                                                float* nx) {
+    float wd[3][4];
 #pragma unroll
-    for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
-    const int ext[3] = {C.W, C.H, C.Dp};
-    int base[3] = {0, 0, 0};
-    float wk[3][4], off[3][4];
+    for (int k = 0; k < D; ++k)
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-        base[k] = stencil_base(x[k], ext[k]);
+        for (int o = 0; o < 4; ++o) wd[k][o] = wk[k][o] * off[k][o];
+    const long long sy = C.nx, sz = (long long)C.nx * C.ny;
+    const long long c0 = (D == 3 ? base[2] * sz : 0) + base[1] * sy + base[0];
+    float vc[D];
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
-            const float dist = x[k] - float(base[k] + o);
-            wk[k][o] = bspline_n(dist);
-            off[k][o] = -dist;
+    for (int r = 0; r < D; ++r) { nv[r] = 0.f; vc[r] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        float Q[D], Qy[D], Qz[D], Qc[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r) { Q[r] = 0.f; Qy[r] = 0.f; Qz[r] = 0.f; Qc[r] = 0.f; }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            if constexpr (D == 3) {
+                float Pv[3] = {0.f, 0.f, 0.f}, Pd[3] = {0.f, 0.f, 0.f}, Pc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const long long cid = c0 + a + b * sy + c * sz;
+                    const float4 g0 = __ldg(&gv[2 * cid]), g1 = __ldg(&gv[2 * cid + 1]);
+                    const float z = wk[2][c], zd = wd[2][c];
+                    Pv[0] += z * g0.x; Pv[1] += z * g0.y; Pv[2] += z * g0.z;
+                    Pd[0] += zd * g0.x; Pd[1] += zd * g0.y; Pd[2] += zd * g0.z;
+                    Pc[0] += z * g1.x; Pc[1] += z * g1.y; Pc[2] += z * g1.z;
+                }
+                const float y = wk[1][b], yd = wd[1][b];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    Q[r] += y * Pv[r];
+                    Qy[r] += yd * Pv[r];
+                    Qz[r] += y * Pd[r];
+                    Qc[r] += y * Pc[r];
+                }
+            } else {
+                const long long cid = c0 + a + b * sy;
+                const float4 g = __ldg(&gv[cid]);
+                const float y = wk[1][b], yd = wd[1][b];
+                Q[0] += y * g.x; Q[1] += y * g.y;
+                Qy[0] += yd * g.x; Qy[1] += yd * g.y;
+                Qc[0] += y * g.z; Qc[1] += y * g.w;
+            }
+        }
+        const float x = wk[0][a], xd = wd[0][a];
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            nv[r] += x * Q[r];
+            nB[r * D + 0] += xd * Q[r];
+            nB[r * D + 1] += x * Qy[r];
+            if (D == 3) nB[r * D + 2] += x * Qz[r];
+            vc[r] += x * Qc[r];
         }
     }
-    float nv[D], nx[D], nB[D * D];
+    // sum w (x_i - x_p) per axis is separable: (sum wd_k) prod_{l != k} (sum w_l)
+    float sw[3], swd[3];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        sw[k] = (wk[k][0] + wk[k][1]) + (wk[k][2] + wk[k][3]);
+        swd[k] = (wd[k][0] + wd[k][1]) + (wd[k][2] + wd[k][3]);
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+        float t = swd[r];
+#pragma unroll
+        for (int l = 0; l < D; ++l)
+            if (l != r) t *= sw[l];
+        nx[r] = t + C.dt * vc[r];
+    }
+}
+
+// General gather (stencil partly outside the grid: those nodes are skipped,
+// as in the reference, and the partial weight sum is returned).
+template <int D>
+__device__ __forceinline__ float gather_clipped(const StepConsts& C, const float4* __restrict__ gv, const int* base,
+                                             const float (*wk)[4], const float (*off)[4], float* nv, float* nB,
+                                             float* nx) {
+    const int ext[3] = {C.W, C.H, C.Dp};
 #pragma unroll
     for (int k = 0; k < D; ++k) { nv[k] = 0.f; nx[k] = 0.f; }
 #pragma unroll
     for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
-    const int nzs = (D == 3) ? 4 : 1;
     float wsum = 0.f;
-    bool clipped = false;
-#pragma unroll
+    const int nzs = (D == 3) ? 4 : 1;
     for (int a = 0; a < 4; ++a) {
         const int ix = base[0] + a;
-        if (ix < 0 || ix > ext[0]) { clipped = true; continue; }
-#pragma unroll
+        if (ix < 0 || ix > ext[0]) continue;
         for (int b = 0; b < 4; ++b) {
             const int iy = base[1] + b;
-            if (iy < 0 || iy > ext[1]) { clipped = true; continue; }
-            const float wab = wk[0][a] * wk[1][b];
-#pragma unroll
+            if (iy < 0 || iy > ext[1]) continue;
             for (int c = 0; c < nzs; ++c) {
                 const int iz = (D == 3) ? base[2] + c : 0;
-                if (D == 3 && (iz < 0 || iz > ext[2])) { clipped = true; continue; }
+                if (D == 3 && (iz < 0 || iz > ext[2])) continue;
                 const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
-                const float w = (D == 3) ? wab * wk[2][c] : wab;
+                const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
                 const float d[3] = {off[0][a], off[1][b], D == 3 ? off[2][c] : 0.f};
                 wsum += w;
                 float vf[3], vc[3];
@@ -540,21 +630,57 @@ __global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C
                     const float4 g0 = __ldg(&gv[2 * cid]), g1 = __ldg(&gv[2 * cid + 1]);
                     vf[0] = g0.x; vf[1] = g0.y; vf[2] = g0.z; vc[0] = g1.x; vc[1] = g1.y; vc[2] = g1.z;
                 }
-#pragma unroll
                 for (int r = 0; r < D; ++r) {
                     const float wv = w * vf[r];
                     nv[r] += wv;
-#pragma unroll
                     for (int k = 0; k < D; ++k) nB[r * D + k] += wv * d[k];
                     nx[r] += (d[r] + C.dt * vc[r]) * w;
                 }
             }
         }
     }
+    return wsum;
+}
+
+template <int D>
+__global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+                                                       SlowQueue Q, unsigned* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int n = P.n;
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
+    int base[3] = {0, 0, 0};
+    float wk[3][4], off[3][4];
+    bool interior = true;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+        base[k] = stencil_base(x[k], ext);
+        interior = interior && base[k] >= 0 && base[k] + 3 <= ext;
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const float dist = x[k] - float(base[k] + o);
+            wk[k][o] = bspline_n(dist);
+            off[k][o] = -dist;
+        }
+    }
+    float nv[D], nx[D], nB[D * D];
+    float xs[D];
+    if (interior) {
+        gather_interior<D>(C, gv, base, wk, off, nv, nB, nx);
+#pragma unroll
+        for (int k = 0; k < D; ++k) xs[k] = x[k];
+    } else {
+        const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, nB, nx);
+#pragma unroll
+        for (int k = 0; k < D; ++k) xs[k] = x[k] * wsum;
+    }
     bool finite = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        const float xn = (clipped ? x[k] * wsum : x[k]) + nx[k];
+        const float xn = xs[k] + nx[k];
         P.v[k * n + i] = nv[k];
         P.x[k * n + i] = xn;
         finite = finite && isfinite(xn);
@@ -576,6 +702,10 @@ __global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C
     if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s)) {
 #pragma unroll
         for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fh[k];
+        float A[D * D];
+        mls_affine<D>(C, nB, Fh, P.Jp[i], P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
     } else {
         const unsigned act = __activemask();
         const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
@@ -596,14 +726,17 @@ __global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, 
     const int n = P.n;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const int i = Q.list[e];
-        float Fh[D * D], Fe[D * D];
+        float Fh[D * D], Fe[D * D], B[D * D], A[D * D];
 #pragma unroll
-        for (int k = 0; k < D * D; ++k) Fh[k] = Q.fh[k * Q.capacity + e];
+        for (int k = 0; k < D * D; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
         float Jp = P.Jp[i];
         plasticity<D, kMLS>(C, Fh, Fe, Jp, status);
 #pragma unroll
         for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
         P.Jp[i] = Jp;
+        mls_affine<D>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
         if (!isfinite(Jp)) raise_flag(status, 1u);
     }
 }

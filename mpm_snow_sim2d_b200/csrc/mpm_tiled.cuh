@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
 }
 
 struct SortBuffers {
-    float *x, *v, *B, *Fe, *Jp, *mass, *vol;
+    float *x, *v, *B, *Fe, *Jp, *A, *mass, *vol;
     int* id;
 };
 
@@ -203,7 +203,11 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
 #pragma unroll
             for (int k = 0; k < D; ++k) { dst.x[k * n + s] = P.x[k * n + src]; dst.v[k * n + s] = P.v[k * n + src]; }
 #pragma unroll
-            for (int k = 0; k < D * D; ++k) { dst.B[k * n + s] = P.B[k * n + src]; dst.Fe[k * n + s] = P.Fe[k * n + src]; }
+            for (int k = 0; k < D * D; ++k) {
+                dst.B[k * n + s] = P.B[k * n + src];
+                dst.Fe[k * n + s] = P.Fe[k * n + src];
+                dst.A[k * n + s] = P.A[k * n + src];
+            }
             dst.Jp[s] = P.Jp[src];
             dst.id[s] = id_src[src];
             if (P.mass) dst.mass[s] = P.mass[src];
@@ -349,40 +353,33 @@ __global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, StepCon
         if (tid == 0) { S.n_ne = 0; S.blockmask = 0u; }
         __syncthreads();
 
-        // Phase A: per-particle payload (stress via the polar rotation).
+        // Phase A: per-particle payload: weights, m v and the affine matrix A
+        // that the previous G2P (or k_prepare_affine) computed.
         for (int j = tid; j < it.z; j += blockDim.x) {
             const int i = it.y + j;
-            float x[D], v[D], B[D * D], Fe[D * D];
-#pragma unroll
-            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
-            const float Jp = P.Jp[i];
+            float x[D], A[D * D], mv[D], f[D], wk[3][4];
             const float mass = P.mass ? P.mass[i] : P.mass_u;
             const float vol = P.vol ? P.vol[i] : P.vol_u;
             S.lcell[j] = -1;
             if (vol == 0.f) continue;  // p2g.glsl:42
-            float sig[D * D];
-            hardened_stress_polar<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
-            float A[D * D], mv[D], f[D], wk[3][4];
+#pragma unroll
+            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; mv[k] = mass * P.v[k * n + i]; }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
             int base[3] = {0, 0, 0}, lc = 0;
             bool inreg = true;
 #pragma unroll
             for (int k = D - 1; k >= 0; --k) {
-                base[k] = stencil_base(x[k], ext[k]);
+                const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                const int rlok = k == 0 ? rlo[0] : (k == 1 ? rlo[1] : rlo[2]);
+                base[k] = stencil_base(x[k], extk);
                 const int cell = base[k] + 1;
                 f[k] = x[k] - float(cell);
 #pragma unroll
                 for (int o = 0; o < 4; ++o) wk[k][o] = bspline_n(x[k] - float(base[k] + o));
-                const int l = cell - rlo[k];
+                const int l = cell - rlok;
                 inreg = inreg && l >= 0 && l < G::R;
                 lc = lc * G::R + l;
-            }
-#pragma unroll
-            for (int r = 0; r < D; ++r) {
-                mv[r] = mass * v[r];
-#pragma unroll
-                for (int c = 0; c < D; ++c) A[r * D + c] = 3.f * mass * B[r * D + c] - 3.f * C.dt * vol * sig[r * D + c];
             }
             if (inreg) {
                 float* q = S.pay + j * G::PS;
