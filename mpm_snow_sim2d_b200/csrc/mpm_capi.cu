@@ -48,6 +48,8 @@ struct mpm_solver {
     TileInfo ti{};
     SortBuffers alt{};
     bool p2g_direct = false;  // P2G flush per unit to global (else via a shared tile)
+    int p2g_mode = 2;         // 2: warp chunks (default); else tile items
+    int p2g_warp_grid = 0;
     bool needs_affine = true; // A must be recomputed from the state before the next P2G
     SlowQueue q{};
 };
@@ -172,6 +174,11 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
 }
 
 template <int D> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
+    if (s->p2g_mode == 2) {
+        k_p2g_warp<D><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D>), s->stream>>>(particle_view(s), s->C,
+                                                                                              s->ti, s->acc, s->status);
+        return cudaGetLastError();
+    }
     if (s->p2g_direct)
         k_p2g_tiled<D, true><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D, true>), s->stream>>>(
             particle_view(s), s->C, s->ti, s->acc, s->status);
@@ -189,7 +196,7 @@ template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
     if (e != cudaSuccess) return e;
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
     k_g2p_gather<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
-    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->q, s->status);
+    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
     return cudaGetLastError();
 }
 
@@ -315,6 +322,19 @@ mpm_status setup_tiled(mpm_solver* s) {
     s->sms = sms > 0 ? sms : 148;
     const char* env = std::getenv("MPM_P2G_DIRECT");
     s->p2g_direct = env && env[0] == '1';
+    const char* envm = std::getenv("MPM_P2G_MODE");
+    s->p2g_mode = envm ? std::atoi(envm) : 2;
+    {
+        const size_t wsm = D == 3 ? sizeof(P2GWarpSmem<3>) : sizeof(P2GWarpSmem<2>);
+        cudaError_t ew = D == 3 ? cudaFuncSetAttribute(k_p2g_warp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm)
+                                : cudaFuncSetAttribute(k_p2g_warp<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+        int per = 0;
+        if (ew == cudaSuccess)
+            ew = D == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g_warp<3>, kP2GWarps * 32, wsm)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g_warp<2>, kP2GWarps * 32, wsm);
+        if (ew != cudaSuccess || per < 1) return MPM_ERR_CUDA;
+        s->p2g_warp_grid = s->sms * per;
+    }
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
     if (D == 3) e = p2g_occupancy<3>(s->p2g_direct, &per_sm);

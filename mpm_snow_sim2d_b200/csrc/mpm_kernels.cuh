@@ -482,7 +482,7 @@ template <int D>
 __device__ __forceinline__ void mls_affine(const StepConsts& C, const float* B, const float* Fe, float Jp, float mass,
                                            float vol, float* A) {
     float sig[D * D];
-    hardened_stress_polar<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+    hardened_stress_fast<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) A[k] = 3.f * mass * B[k] - 3.f * C.dt * vol * sig[k];
 }
@@ -642,8 +642,16 @@ __device__ __forceinline__ float gather_clipped(const StepConsts& C, const float
     return wsum;
 }
 
+__device__ __forceinline__ int queue_slot(const SlowQueue& Q) {
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
+    int slot = 0;
+    if (lane == leader) slot = atomicAdd(Q.count, __popc(act));
+    return __shfl_sync(act, slot, leader) + __popc(act & ((1u << lane) - 1));
+}
+
 template <int D>
-__global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+__global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                        SlowQueue Q, unsigned* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
@@ -666,21 +674,16 @@ __global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C
             off[k][o] = -dist;
         }
     }
-    float nv[D], nx[D], nB[D * D];
-    float xs[D];
-    if (interior) {
-        gather_interior<D>(C, gv, base, wk, off, nv, nB, nx);
-#pragma unroll
-        for (int k = 0; k < D; ++k) xs[k] = x[k];
-    } else {
-        const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, nB, nx);
-#pragma unroll
-        for (int k = 0; k < D; ++k) xs[k] = x[k] * wsum;
+    if (!interior) {  // stencil partly outside the grid: the general kernel does it all
+        Q.list[queue_slot(Q)] = -1 - i;
+        return;
     }
+    float nv[D], nx[D], nB[D * D];
+    gather_interior<D>(C, gv, base, wk, off, nv, nB, nx);
     bool finite = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        const float xn = xs[k] + nx[k];
+        const float xn = x[k] + nx[k];
         P.v[k * n + i] = nv[k];
         P.x[k * n + i] = xn;
         finite = finite && isfinite(xn);
@@ -699,19 +702,18 @@ __global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C
             for (int k = 0; k < D; ++k) s += (C.dt * 3.f * nB[r * D + k]) * Fe[k * D + c];
             Fh[r * D + c] = s;
         }
-    if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s)) {
+    float sig[D * D];
+    const float Jp = P.Jp[i];
+    if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s) &&
+        hardened_stress_series<D>(Fh, Jp, C.mu0, C.la0, C.xi, sig)) {
+        const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
 #pragma unroll
-        for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fh[k];
-        float A[D * D];
-        mls_affine<D>(C, nB, Fh, P.Jp[i], P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
+        for (int k = 0; k < D * D; ++k) {
+            P.Fe[k * n + i] = Fh[k];
+            P.A[k * n + i] = 3.f * mass * nB[k] - 3.f * C.dt * vol * sig[k];
+        }
     } else {
-        const unsigned act = __activemask();
-        const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
-        int slot = 0;
-        if (lane == leader) slot = atomicAdd(Q.count, __popc(act));
-        slot = __shfl_sync(act, slot, leader) + __popc(act & ((1u << lane) - 1));
+        const int slot = queue_slot(Q);
         Q.list[slot] = i;
 #pragma unroll
         for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
@@ -719,16 +721,60 @@ __global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C
     if (!finite) raise_flag(status, 1u);
 }
 
+// Queued particles: the full return map for out-of-band trial F (entry i), or
+// the whole G2P with a grid-clipped stencil (entry -1 - i).
 template <int D>
-__global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, SlowQueue Q,
-                                                     unsigned* __restrict__ status) {
+__global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, const float4* __restrict__ gv,
+                                                     SlowQueue Q, unsigned* __restrict__ status) {
     const int m = *Q.count;
     const int n = P.n;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
-        const int i = Q.list[e];
+        const int entry = Q.list[e];
+        const int i = entry >= 0 ? entry : -1 - entry;
         float Fh[D * D], Fe[D * D], B[D * D], A[D * D];
+        if (entry >= 0) {
 #pragma unroll
-        for (int k = 0; k < D * D; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
+            for (int k = 0; k < D * D; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
+        } else {
+            float x[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
+            int base[3] = {0, 0, 0};
+            float wk[3][4], off[3][4];
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                base[k] = stencil_base(x[k], ext);
+#pragma unroll
+                for (int o = 0; o < 4; ++o) {
+                    const float dist = x[k] - float(base[k] + o);
+                    wk[k][o] = bspline_n(dist);
+                    off[k][o] = -dist;
+                }
+            }
+            float nv[D], nx[D];
+            const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, B, nx);
+            bool finite = true;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const float xn = x[k] * wsum + nx[k];
+                P.v[k * n + i] = nv[k];
+                P.x[k * n + i] = xn;
+                finite = finite && isfinite(xn);
+            }
+            if (!finite) raise_flag(status, 1u);
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) { P.B[k * n + i] = B[k]; Fe[k] = P.Fe[k * n + i]; }
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    float s = Fe[r * D + c];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) s += (C.dt * 3.f * B[r * D + k]) * Fe[k * D + c];
+                    Fh[r * D + c] = s;
+                }
+        }
         float Jp = P.Jp[i];
         plasticity<D, kMLS>(C, Fh, Fe, Jp, status);
 #pragma unroll

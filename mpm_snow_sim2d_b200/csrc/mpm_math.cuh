@@ -326,6 +326,81 @@ template <int D, int FORM> __device__ __forceinline__ void hardened_stress_polar
         }
 }
 
+// Hardened stress through the left stretch (3D): for det F > 0, F = V R with
+// V = sqrt(F F^T), so (F - R) F^T = F F^T - V. With E = F F^T - I,
+//   F F^T - sqrt(F F^T) = E/2 + E^2/8 - E^3/16 + 5E^4/128 - 7E^5/256 + ...
+// (the binomial series of sqrt(1 + x) subtracted from 1 + x), evaluated on the
+// symmetric E without forming R and without the cancellation of F F^T - V.
+// Applies when ||E||_F <= 0.1 (8 terms: truncation below 1e-10 ||E||; every F
+// inside the default elastic band qualifies). 2D: the closed-form polar
+// rotation. Returns false (nothing written) when it does not apply.
+template <int D>
+__device__ __forceinline__ bool hardened_stress_series(const float* Fe, float Jp, float mu0, float la0, float xi,
+                                                       float* sig) {
+    if constexpr (D == 3) {
+        const float J = det<3>(Fe);
+        // symmetric E = F F^T - I : (00, 11, 22, 01, 02, 12)
+        float e[6];
+        e[0] = Fe[0] * Fe[0] + Fe[1] * Fe[1] + Fe[2] * Fe[2] - 1.f;
+        e[1] = Fe[3] * Fe[3] + Fe[4] * Fe[4] + Fe[5] * Fe[5] - 1.f;
+        e[2] = Fe[6] * Fe[6] + Fe[7] * Fe[7] + Fe[8] * Fe[8] - 1.f;
+        e[3] = Fe[0] * Fe[3] + Fe[1] * Fe[4] + Fe[2] * Fe[5];
+        e[4] = Fe[0] * Fe[6] + Fe[1] * Fe[7] + Fe[2] * Fe[8];
+        e[5] = Fe[3] * Fe[6] + Fe[4] * Fe[7] + Fe[5] * Fe[8];
+        const float n2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + 2.f * (e[3] * e[3] + e[4] * e[4] + e[5] * e[5]);
+        if (!(J > 0.f && n2 <= 0.01f)) return false;
+        // coefficients of E^k in 1 + x - sqrt(1 + x), k = 1..8
+        const float d[8] = {0.5f, 0.125f, -0.0625f, 0.0390625f, -0.02734375f, 0.0205078125f, -0.01611328125f,
+                            0.013092041015625f};
+        float t[6], p[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { p[q] = e[q]; t[q] = d[0] * e[q]; }
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            // p <- p E (powers of one symmetric matrix commute: symmetric)
+            float r[6];
+            r[0] = p[0] * e[0] + p[3] * e[3] + p[4] * e[4];
+            r[1] = p[3] * e[3] + p[1] * e[1] + p[5] * e[5];
+            r[2] = p[4] * e[4] + p[5] * e[5] + p[2] * e[2];
+            r[3] = p[0] * e[3] + p[3] * e[1] + p[4] * e[5];
+            r[4] = p[0] * e[4] + p[3] * e[5] + p[4] * e[2];
+            r[5] = p[3] * e[4] + p[1] * e[5] + p[5] * e[2];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { p[q] = r[q]; t[q] += d[k] * r[q]; }
+        }
+        const float h = expf(xi * (1.f - Jp));
+        const float mu2 = 2.f * mu0 * h, diag = la0 * h * (J - 1.f) * J;
+        sig[0] = mu2 * t[0] + diag; sig[4] = mu2 * t[1] + diag; sig[8] = mu2 * t[2] + diag;
+        sig[1] = sig[3] = mu2 * t[3];
+        sig[2] = sig[6] = mu2 * t[4];
+        sig[5] = sig[7] = mu2 * t[5];
+        return true;
+    } else {
+        float Rm[4];
+        if (!polar_rotation<2>(Fe, Rm)) return false;
+        const float Je = det<2>(Fe);
+        const float h = expf(xi * (1.f - Jp));
+        const float mu = mu0 * h, la = la0 * h;
+        const float diag = la * (Je - 1.f) * Je;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const float s = (Fe[i * 2] - Rm[i * 2]) * Fe[j * 2] + (Fe[i * 2 + 1] - Rm[i * 2 + 1]) * Fe[j * 2 + 1];
+                sig[i * 2 + j] = 2.f * mu * s + (i == j ? diag : 0.f);
+            }
+        return true;
+    }
+}
+
+// The stress of the MLS path: the series / closed form above when it applies,
+// else the polar rotation (Newton, then the reference's SVD).
+template <int D, int FORM> __device__ __forceinline__ void hardened_stress_fast(const float* Fe, float Jp, float mu0,
+                                                                               float la0, float xi, float* sig) {
+    if (FORM == kMLS && hardened_stress_series<D>(Fe, Jp, mu0, la0, xi, sig)) return;
+    hardened_stress_polar<D, FORM>(Fe, Jp, mu0, la0, xi, sig);
+}
+
 // True when every singular value of F lies in [t0, t1] and det F > 0, proven
 // with margin: then the return map clamps nothing and is the identity
 // (F_E' = F, J_p' = J_p), so the SVD can be skipped. First Gershgorin discs of

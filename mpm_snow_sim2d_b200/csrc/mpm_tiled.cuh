@@ -631,3 +631,224 @@ __global__ void __launch_bounds__(256) k_grid_marked(StepConsts C, TileInfo TI, 
 __global__ void k_reset_marks(TileInfo TI) { *TI.n_marked = 0; }
 
 }  // namespace mpm
+
+namespace mpm {
+
+// ---------------------------------------------------------------------------
+// Warp-chunk P2G (MLS). The sorted slot array is cut into fixed chunks of
+// kChunk<D> slots; each warp takes one chunk at a time, with no CTA-wide
+// synchronisation. In the chunk, maximal runs of consecutive slots whose
+// particles share their current cell are grouped; one thread per (run,
+// x-offset) [3D] or per run [2D] accumulates the run's 16 nodes x (1 + D)
+// channels in FP32 registers, in slot order, and adds them as int64 fixed
+// point to the global sums. The grouping is a function of the slot order (the
+// deterministic sort order, kept between sorts), so the sums are bit-identical
+// run to run; particles that drifted to another cell since the last sort just
+// form shorter runs.
+template <int D> struct WarpGeom;
+template <> struct WarpGeom<3> { static constexpr int CHUNK = 48, SPLIT = 4, PS = 29; };
+template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 17; };
+constexpr int kP2GWarps = 8;
+
+template <int D> struct P2GWarpSmem {
+    using W = WarpGeom<D>;
+    float pay[kP2GWarps][W::CHUNK * W::PS];
+    int key[kP2GWarps][W::CHUNK];
+    int run[kP2GWarps][W::CHUNK + 1];
+};
+
+__device__ __forceinline__ void mark_block_once(const TileInfo& TI, int b) {
+    if (TI.mark[b] == 0) mark_block(TI, b);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
+                                                              unsigned long long* __restrict__ acc,
+                                                              unsigned* __restrict__ status) {
+    using W = WarpGeom<D>;
+    using O = PayOff<D>;
+    constexpr int T = TileGeom<D>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P2GWarpSmem<D>& S = *reinterpret_cast<P2GWarpSmem<D>*>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* pay = S.pay[wid];
+    int* key = S.key[wid];
+    int* run = S.run[wid];
+    const int n = P.n;
+    const int nchunks = (n + W::CHUNK - 1) / W::CHUNK;
+    for (int chunk = blockIdx.x * kP2GWarps + wid; chunk < nchunks; chunk += gridDim.x * kP2GWarps) {
+        const int s0 = chunk * W::CHUNK;
+        const int cnt = min(W::CHUNK, n - s0);
+        // payload of every particle of the chunk
+        for (int j = lane; j < cnt; j += 32) {
+            const int i = s0 + j;
+            const float mass = P.mass ? P.mass[i] : P.mass_u;
+            const float vol = P.vol ? P.vol[i] : P.vol_u;
+            if (vol == 0.f) { key[j] = -1; continue; }  // p2g.glsl:42
+            float* q = pay + j * W::PS;
+            int k3 = 0;
+#pragma unroll
+            for (int k = D - 1; k >= 0; --k) {
+                const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                const float x = P.x[k * n + i];
+                const int base = stencil_base(x, extk);
+#pragma unroll
+                for (int o = 0; o < 4; ++o) q[4 * k + o] = bspline_n(x - float(base + o));
+                q[O::F + k] = x - float(base + 1);
+                q[O::MV + k] = mass * P.v[k * n + i];
+                // cell key (base + 1 in [-8, ext + 8]) shifted to be non-negative
+                k3 = k3 * (extk + 18) + (base + 9);
+            }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) q[O::A + k] = P.A[k * n + i];
+            q[O::M] = mass;
+            key[j] = k3;
+        }
+        __syncwarp();
+        // runs of equal key in slot order
+        int nruns = 0;
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            const int j = j0 + lane;
+            const bool start = j < cnt && (j == 0 || key[j] != key[j - 1]);
+            const unsigned b = __ballot_sync(0xffffffffu, start);
+            if (start) run[nruns + __popc(b & ((1u << lane) - 1))] = j;
+            nruns += __popc(b);
+        }
+        if (lane == 0) run[nruns] = cnt;
+        __syncwarp();
+        for (int u = lane; u < nruns * W::SPLIT; u += 32) {
+            const int r = u / W::SPLIT, a = u % W::SPLIT;
+            const int j0 = run[r], j1 = run[r + 1];
+            int kk = key[j0];
+            if (kk < 0) continue;
+            int cell[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                cell[k] = kk % (extk + 18) - 8;  // stored base + 9; cell = base + 1
+                kk /= (extk + 18);
+            }
+            if constexpr (D == 3) {
+                float am[16], a0[16], a1[16], a2[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
+                for (int j = j0; j < j1; ++j) {
+                    const float* pp = pay + j * W::PS;
+                    const float alpha = pp[a];
+                    const float beta = alpha * (float(a - 1) - pp[O::F + 0]);
+                    const float fy = pp[O::F + 1], fz = pp[O::F + 2];
+                    const float* Am = pp + O::A;
+                    const float e0 = alpha * pp[O::MV + 0] + beta * Am[0];
+                    const float e1 = alpha * pp[O::MV + 1] + beta * Am[3];
+                    const float e2 = alpha * pp[O::MV + 2] + beta * Am[6];
+                    const float f0 = alpha * Am[1], f1 = alpha * Am[4], f2 = alpha * Am[7];
+                    const float g0 = alpha * Am[2], g1 = alpha * Am[5], g2 = alpha * Am[8];
+                    const float ma = pp[O::M] * alpha;
+                    float Z[4], Zd[4];
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) { Z[cc] = pp[8 + cc]; Zd[cc] = Z[cc] * (float(cc - 1) - fz); }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const float Y = pp[4 + b], Yd = Y * (float(b - 1) - fy);
+                        const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
+                        const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int idx = b * 4 + cc;
+                            am[idx] += mY * Z[cc];
+                            a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
+                            a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
+                            a2[idx] += h2 * Z[cc] + k2 * Zd[cc];
+                        }
+                    }
+                }
+                const int gx = cell[0] - 1 + a;
+                bool outside = false;
+                if (gx >= 0 && gx <= C.W) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int gy = cell[1] - 1 + b;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int gz = cell[2] - 1 + cc;
+                            const int idx = b * 4 + cc;
+                            if (gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
+                            const long long gid = ((long long)gz * C.ny + gy) * C.nx + gx;
+                            const long long q0 = to_fixed(am[idx], C.sm, status);
+                            const long long q1 = to_fixed(a0[idx], C.sp, status);
+                            const long long q2 = to_fixed(a1[idx], C.sp, status);
+                            const long long q3 = to_fixed(a2[idx], C.sp, status);
+                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
+                            if (q1) atomicAdd(&acc[C.nodes + gid], (unsigned long long)q1);
+                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
+                            if (q3) atomicAdd(&acc[3 * C.nodes + gid], (unsigned long long)q3);
+                        }
+                    }
+                    // node blocks holding the unit's in-grid nodes (empty range: none)
+                    const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
+                    const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + 2);
+                    if (y0 <= y1 && z0 <= z1)
+                        for (int bz = z0 / T; bz <= z1 / T; ++bz)
+                            for (int by = y0 / T; by <= y1 / T; ++by)
+                                mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
+                } else {
+                    outside = true;
+                }
+                if (outside) raise_flag(status, 4u);
+            } else {
+                float am[16], a0[16], a1[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
+                for (int j = j0; j < j1; ++j) {
+                    const float* pp = pay + j * W::PS;
+                    const float fx = pp[O::F + 0], fy = pp[O::F + 1];
+                    const float* Am = pp + O::A;
+                    const float mv0 = pp[O::MV + 0], mv1 = pp[O::MV + 1], m = pp[O::M];
+                    float Y[4], Yd[4];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) { Y[b] = pp[4 + b]; Yd[b] = Y[b] * (float(b - 1) - fy); }
+#pragma unroll
+                    for (int aa = 0; aa < 4; ++aa) {
+                        const float X = pp[aa], Xd = X * (float(aa - 1) - fx);
+                        const float e0 = mv0 * X + Am[0] * Xd, e1 = mv1 * X + Am[2] * Xd;
+                        const float f0 = Am[1] * X, f1 = Am[3] * X, mX = m * X;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            const int idx = aa * 4 + b;
+                            am[idx] += mX * Y[b];
+                            a0[idx] += e0 * Y[b] + f0 * Yd[b];
+                            a1[idx] += e1 * Y[b] + f1 * Yd[b];
+                        }
+                    }
+                }
+                bool outside = false;
+#pragma unroll
+                for (int aa = 0; aa < 4; ++aa) {
+                    const int gx = cell[0] - 1 + aa;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int gy = cell[1] - 1 + b;
+                        const int idx = aa * 4 + b;
+                        if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
+                        const long long gid = (long long)gy * C.nx + gx;
+                        const long long q0 = to_fixed(am[idx], C.sm, status);
+                        const long long q1 = to_fixed(a0[idx], C.sp, status);
+                        const long long q2 = to_fixed(a1[idx], C.sp, status);
+                        if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
+                        if (q1) atomicAdd(&acc[C.nodes + gid], (unsigned long long)q1);
+                        if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
+                    }
+                }
+                const int x0 = max(0, cell[0] - 1), x1 = min(C.W, cell[0] + 2);
+                const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
+                if (x0 <= x1 && y0 <= y1)
+                    for (int by = y0 / T; by <= y1 / T; ++by)
+                        for (int bx = x0 / T; bx <= x1 / T; ++bx) mark_block_once(TI, by * TI.nblk[0] + bx);
+                if (outside) raise_flag(status, 4u);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace mpm
