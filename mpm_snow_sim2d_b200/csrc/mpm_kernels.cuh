@@ -534,7 +534,7 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
     for (int r = 0; r < D; ++r) { nv[r] = 0.f; vc[r] = 0.f; }
 #pragma unroll
     for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
-#pragma unroll
+#pragma unroll 1
     for (int a = 0; a < 4; ++a) {
         float Q[D], Qy[D], Qz[D], Qc[D];
 #pragma unroll
@@ -569,7 +569,8 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
                 Qc[0] += y * g.z; Qc[1] += y * g.w;
             }
         }
-        const float x = wk[0][a], xd = wd[0][a];
+        const float x = a == 0 ? wk[0][0] : a == 1 ? wk[0][1] : a == 2 ? wk[0][2] : wk[0][3];
+        const float xd = a == 0 ? wd[0][0] : a == 1 ? wd[0][1] : a == 2 ? wd[0][2] : wd[0][3];
 #pragma unroll
         for (int r = 0; r < D; ++r) {
             nv[r] += x * Q[r];
@@ -651,7 +652,7 @@ __device__ __forceinline__ int queue_slot(const SlowQueue& Q) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(256, 3) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+__global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                        SlowQueue Q, unsigned* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;

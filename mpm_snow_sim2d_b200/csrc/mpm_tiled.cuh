@@ -636,23 +636,28 @@ namespace mpm {
 
 // ---------------------------------------------------------------------------
 // Warp-chunk P2G (MLS). The sorted slot array is cut into fixed chunks of
-// kChunk<D> slots; each warp takes one chunk at a time, with no CTA-wide
-// synchronisation. In the chunk, maximal runs of consecutive slots whose
-// particles share their current cell are grouped; one thread per (run,
+// WarpGeom<D>::CHUNK slots; each warp takes one chunk at a time, with no
+// CTA-wide synchronisation. In the chunk, maximal runs of consecutive slots
+// whose particles share their current cell are grouped; one thread per (run,
 // x-offset) [3D] or per run [2D] accumulates the run's 16 nodes x (1 + D)
 // channels in FP32 registers, in slot order, and adds them as int64 fixed
 // point to the global sums. The grouping is a function of the slot order (the
 // deterministic sort order, kept between sorts), so the sums are bit-identical
 // run to run; particles that drifted to another cell since the last sort just
 // form shorter runs.
+//
+// Payload per particle (float4-aligned, conflict-free for 8 distinct
+// particles per load):
+//   3D (28): wx[4] | wy[4] | wz[4] | fx fy fz m | mv0 mv1 mv2 A00 | A01 A02 A10 A11 | A12 A20 A21 A22
+//   2D (20): wx[4] | wy[4] | fx fy m mv0 | mv1 A00 A01 A10 | A11 pad pad pad
 template <int D> struct WarpGeom;
-template <> struct WarpGeom<3> { static constexpr int CHUNK = 48, SPLIT = 4, PS = 29; };
-template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 17; };
+template <> struct WarpGeom<3> { static constexpr int CHUNK = 40, SPLIT = 4, PS = 28; };
+template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
 constexpr int kP2GWarps = 8;
 
 template <int D> struct P2GWarpSmem {
     using W = WarpGeom<D>;
-    float pay[kP2GWarps][W::CHUNK * W::PS];
+    float4 pay[kP2GWarps][W::CHUNK * W::PS / 4];
     int key[kP2GWarps][W::CHUNK];
     int run[kP2GWarps][W::CHUNK + 1];
 };
@@ -661,17 +666,22 @@ __device__ __forceinline__ void mark_block_once(const TileInfo& TI, int b) {
     if (TI.mark[b] == 0) mark_block(TI, b);
 }
 
+// int64 fixed-point add of a unit's sums; the range is checked once per unit.
+__device__ __forceinline__ void red_fixed(unsigned long long* p, float v, float scale) {
+    atomicAdd(p, (unsigned long long)__float2ll_rn(v * scale));
+}
+
 template <int D>
 __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
                                                               unsigned long long* __restrict__ acc,
                                                               unsigned* __restrict__ status) {
     using W = WarpGeom<D>;
-    using O = PayOff<D>;
     constexpr int T = TileGeom<D>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2GWarpSmem<D>& S = *reinterpret_cast<P2GWarpSmem<D>*>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* pay = S.pay[wid];
+    float4* pay = S.pay[wid];
+    float* payf = reinterpret_cast<float*>(pay);
     int* key = S.key[wid];
     int* run = S.run[wid];
     const int n = P.n;
@@ -679,14 +689,14 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
     for (int chunk = blockIdx.x * kP2GWarps + wid; chunk < nchunks; chunk += gridDim.x * kP2GWarps) {
         const int s0 = chunk * W::CHUNK;
         const int cnt = min(W::CHUNK, n - s0);
-        // payload of every particle of the chunk
         for (int j = lane; j < cnt; j += 32) {
             const int i = s0 + j;
             const float mass = P.mass ? P.mass[i] : P.mass_u;
             const float vol = P.vol ? P.vol[i] : P.vol_u;
             if (vol == 0.f) { key[j] = -1; continue; }  // p2g.glsl:42
-            float* q = pay + j * W::PS;
+            float* q = payf + j * W::PS;
             int k3 = 0;
+            float f[3], mv[3];
 #pragma unroll
             for (int k = D - 1; k >= 0; --k) {
                 const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
@@ -694,18 +704,23 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                 const int base = stencil_base(x, extk);
 #pragma unroll
                 for (int o = 0; o < 4; ++o) q[4 * k + o] = bspline_n(x - float(base + o));
-                q[O::F + k] = x - float(base + 1);
-                q[O::MV + k] = mass * P.v[k * n + i];
-                // cell key (base + 1 in [-8, ext + 8]) shifted to be non-negative
-                k3 = k3 * (extk + 18) + (base + 9);
+                f[k] = x - float(base + 1);
+                mv[k] = mass * P.v[k * n + i];
+                k3 = k3 * (extk + 18) + (base + 9);  // cell key: base + 9 >= 0
             }
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) q[O::A + k] = P.A[k * n + i];
-            q[O::M] = mass;
+            if constexpr (D == 3) {
+                reinterpret_cast<float4*>(q)[3] = make_float4(f[0], f[1], f[2], mass);
+                reinterpret_cast<float4*>(q)[4] = make_float4(mv[0], mv[1], mv[2], P.A[i]);
+                reinterpret_cast<float4*>(q)[5] = make_float4(P.A[n + i], P.A[2 * n + i], P.A[3 * n + i], P.A[4 * n + i]);
+                reinterpret_cast<float4*>(q)[6] = make_float4(P.A[5 * n + i], P.A[6 * n + i], P.A[7 * n + i], P.A[8 * n + i]);
+            } else {
+                reinterpret_cast<float4*>(q)[2] = make_float4(f[0], f[1], mass, mv[0]);
+                reinterpret_cast<float4*>(q)[3] = make_float4(mv[1], P.A[i], P.A[n + i], P.A[2 * n + i]);
+                reinterpret_cast<float4*>(q)[4] = make_float4(P.A[3 * n + i], 0.f, 0.f, 0.f);
+            }
             key[j] = k3;
         }
         __syncwarp();
-        // runs of equal key in slot order
         int nruns = 0;
         for (int j0 = 0; j0 < cnt; j0 += 32) {
             const int j = j0 + lane;
@@ -732,24 +747,27 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                 float am[16], a0[16], a1[16], a2[16];
 #pragma unroll
                 for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
+                const float da = float(a - 1);
                 for (int j = j0; j < j1; ++j) {
-                    const float* pp = pay + j * W::PS;
-                    const float alpha = pp[a];
-                    const float beta = alpha * (float(a - 1) - pp[O::F + 0]);
-                    const float fy = pp[O::F + 1], fz = pp[O::F + 2];
-                    const float* Am = pp + O::A;
-                    const float e0 = alpha * pp[O::MV + 0] + beta * Am[0];
-                    const float e1 = alpha * pp[O::MV + 1] + beta * Am[3];
-                    const float e2 = alpha * pp[O::MV + 2] + beta * Am[6];
-                    const float f0 = alpha * Am[1], f1 = alpha * Am[4], f2 = alpha * Am[7];
-                    const float g0 = alpha * Am[2], g1 = alpha * Am[5], g2 = alpha * Am[8];
-                    const float ma = pp[O::M] * alpha;
-                    float Z[4], Zd[4];
+                    const float4* pp = pay + j * (W::PS / 4);
+                    const float alpha = payf[j * W::PS + a];
+                    const float4 wy = pp[1], wz = pp[2], fm = pp[3], p4 = pp[4], p5 = pp[5], p6 = pp[6];
+                    // A = (p4.w p5.x p5.y | p5.z p5.w p6.x | p6.y p6.z p6.w)
+                    const float beta = alpha * (da - fm.x);
+                    const float e0 = alpha * p4.x + beta * p4.w;
+                    const float e1 = alpha * p4.y + beta * p5.z;
+                    const float e2 = alpha * p4.z + beta * p6.y;
+                    const float f0 = alpha * p5.x, f1 = alpha * p5.w, f2 = alpha * p6.z;
+                    const float g0 = alpha * p5.y, g1 = alpha * p6.x, g2 = alpha * p6.w;
+                    const float ma = fm.w * alpha;
+                    const float Z[4] = {wz.x, wz.y, wz.z, wz.w};
+                    const float Yv[4] = {wy.x, wy.y, wy.z, wy.w};
+                    float Zd[4];
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) { Z[cc] = pp[8 + cc]; Zd[cc] = Z[cc] * (float(cc - 1) - fz); }
+                    for (int cc = 0; cc < 4; ++cc) Zd[cc] = Z[cc] * (float(cc - 1) - fm.z);
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
-                        const float Y = pp[4 + b], Yd = Y * (float(b - 1) - fy);
+                        const float Y = Yv[b], Yd = Y * (float(b - 1) - fm.y);
                         const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
                         const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
 #pragma unroll
@@ -762,28 +780,47 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                         }
                     }
                 }
-                const int gx = cell[0] - 1 + a;
-                bool outside = false;
-                if (gx >= 0 && gx <= C.W) {
+                float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int gy = cell[1] - 1 + b;
+                for (int k = 0; k < 16; ++k) {
+                    mx_m = fmaxf(mx_m, fabsf(am[k]));
+                    mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fmaxf(fabsf(a1[k]), fabsf(a2[k]))));
+                }
+                if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
+                    raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
+                const int gx = cell[0] - 1 + a;
+                const bool inside = gx >= 0 && gx <= C.W && cell[1] >= 1 && cell[1] + 2 <= C.H && cell[2] >= 1 &&
+                                    cell[2] + 2 <= C.Dp;
+                if (inside) {
+                    const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1)) * C.nx + gx;
+                    const long long sy = C.nx, sz = (long long)C.nx * C.ny;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) {
-                            const int gz = cell[2] - 1 + cc;
                             const int idx = b * 4 + cc;
-                            if (gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
-                            const long long gid = ((long long)gz * C.ny + gy) * C.nx + gx;
-                            const long long q0 = to_fixed(am[idx], C.sm, status);
-                            const long long q1 = to_fixed(a0[idx], C.sp, status);
-                            const long long q2 = to_fixed(a1[idx], C.sp, status);
-                            const long long q3 = to_fixed(a2[idx], C.sp, status);
-                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
-                            if (q1) atomicAdd(&acc[C.nodes + gid], (unsigned long long)q1);
-                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
-                            if (q3) atomicAdd(&acc[3 * C.nodes + gid], (unsigned long long)q3);
+                            unsigned long long* p0 = acc + (g0 + b * sy + cc * sz);
+                            red_fixed(p0, am[idx], C.sm);
+                            red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                            red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                            red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
                         }
-                    }
+                } else {
+                    bool outside = false;
+                    for (int b = 0; b < 4; ++b)
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int gy = cell[1] - 1 + b, gz = cell[2] - 1 + cc;
+                            if (gx < 0 || gx > C.W || gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
+                            const int idx = b * 4 + cc;
+                            unsigned long long* p0 = acc + (((long long)gz * C.ny + gy) * C.nx + gx);
+                            red_fixed(p0, am[idx], C.sm);
+                            red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                            red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                            red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
+                        }
+                    if (outside) raise_flag(status, 4u);
+                }
+                if (gx >= 0 && gx <= C.W) {
                     // node blocks holding the unit's in-grid nodes (empty range: none)
                     const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
                     const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + 2);
@@ -791,27 +828,25 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                         for (int bz = z0 / T; bz <= z1 / T; ++bz)
                             for (int by = y0 / T; by <= y1 / T; ++by)
                                 mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
-                } else {
-                    outside = true;
                 }
-                if (outside) raise_flag(status, 4u);
             } else {
                 float am[16], a0[16], a1[16];
 #pragma unroll
                 for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
                 for (int j = j0; j < j1; ++j) {
-                    const float* pp = pay + j * W::PS;
-                    const float fx = pp[O::F + 0], fy = pp[O::F + 1];
-                    const float* Am = pp + O::A;
-                    const float mv0 = pp[O::MV + 0], mv1 = pp[O::MV + 1], m = pp[O::M];
-                    float Y[4], Yd[4];
+                    const float4* pp = pay + j * (W::PS / 4);
+                    const float4 wx = pp[0], wy = pp[1], p2 = pp[2], p3 = pp[3], p4 = pp[4];
+                    // f = (p2.x, p2.y), m = p2.z, mv = (p2.w, p3.x), A = (p3.y p3.z | p3.w p4.x)
+                    const float Xv[4] = {wx.x, wx.y, wx.z, wx.w};
+                    const float Y[4] = {wy.x, wy.y, wy.z, wy.w};
+                    float Yd[4];
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) { Y[b] = pp[4 + b]; Yd[b] = Y[b] * (float(b - 1) - fy); }
+                    for (int b = 0; b < 4; ++b) Yd[b] = Y[b] * (float(b - 1) - p2.y);
 #pragma unroll
                     for (int aa = 0; aa < 4; ++aa) {
-                        const float X = pp[aa], Xd = X * (float(aa - 1) - fx);
-                        const float e0 = mv0 * X + Am[0] * Xd, e1 = mv1 * X + Am[2] * Xd;
-                        const float f0 = Am[1] * X, f1 = Am[3] * X, mX = m * X;
+                        const float X = Xv[aa], Xd = X * (float(aa - 1) - p2.x);
+                        const float e0 = p2.w * X + p3.y * Xd, e1 = p3.x * X + p3.w * Xd;
+                        const float f0 = p3.z * X, f1 = p4.x * X, mX = p2.z * X;
 #pragma unroll
                         for (int b = 0; b < 4; ++b) {
                             const int idx = aa * 4 + b;
@@ -821,30 +856,46 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                         }
                     }
                 }
-                bool outside = false;
+                float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
-                for (int aa = 0; aa < 4; ++aa) {
-                    const int gx = cell[0] - 1 + aa;
+                for (int k = 0; k < 16; ++k) {
+                    mx_m = fmaxf(mx_m, fabsf(am[k]));
+                    mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fabsf(a1[k])));
+                }
+                if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
+                    raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
+                const bool inside = cell[0] >= 1 && cell[0] + 2 <= C.W && cell[1] >= 1 && cell[1] + 2 <= C.H;
+                if (inside) {
+                    const long long g0 = (long long)(cell[1] - 1) * C.nx + (cell[0] - 1);
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int gy = cell[1] - 1 + b;
-                        const int idx = aa * 4 + b;
-                        if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
-                        const long long gid = (long long)gy * C.nx + gx;
-                        const long long q0 = to_fixed(am[idx], C.sm, status);
-                        const long long q1 = to_fixed(a0[idx], C.sp, status);
-                        const long long q2 = to_fixed(a1[idx], C.sp, status);
-                        if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
-                        if (q1) atomicAdd(&acc[C.nodes + gid], (unsigned long long)q1);
-                        if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
-                    }
+                    for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            const int idx = aa * 4 + b;
+                            unsigned long long* p0 = acc + (g0 + aa + (long long)b * C.nx);
+                            red_fixed(p0, am[idx], C.sm);
+                            red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                            red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                        }
+                } else {
+                    bool outside = false;
+                    for (int aa = 0; aa < 4; ++aa)
+                        for (int b = 0; b < 4; ++b) {
+                            const int gx = cell[0] - 1 + aa, gy = cell[1] - 1 + b;
+                            if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
+                            const int idx = aa * 4 + b;
+                            unsigned long long* p0 = acc + ((long long)gy * C.nx + gx);
+                            red_fixed(p0, am[idx], C.sm);
+                            red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                            red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                        }
+                    if (outside) raise_flag(status, 4u);
                 }
                 const int x0 = max(0, cell[0] - 1), x1 = min(C.W, cell[0] + 2);
                 const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
                 if (x0 <= x1 && y0 <= y1)
                     for (int by = y0 / T; by <= y1 / T; ++by)
                         for (int bx = x0 / T; bx <= x1 / T; ++bx) mark_block_once(TI, by * TI.nblk[0] + bx);
-                if (outside) raise_flag(status, 4u);
             }
         }
         __syncwarp();
