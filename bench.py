@@ -213,6 +213,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--budget-s", type=float, default=60.0, help="CPU time cap of the reference arm")
+    ap.add_argument("--sort-period", type=int, default=0, help="steps between particle re-sorts (0: solver default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -240,7 +241,7 @@ def main():
     scene = make_scene(args.workload)
     d = scene.dim
     stream = torch.cuda.Stream()
-    solver = Solver.from_scene(scene)
+    solver = Solver.from_scene(scene, sort_period=args.sort_period)
     solver.set_stream(stream.cuda_stream)
 
     # warm-up, then active-node count (untimed P2G-only pass)

@@ -50,6 +50,12 @@ struct mpm_solver {
     bool p2g_direct = false;  // P2G flush per unit to global (else via a shared tile)
     int p2g_mode = 2;         // 2: warp chunks (default); else tile items
     int p2g_warp_grid = 0;
+    // CUDA graphs of one sort period (sort + sort_period steps), one per
+    // buffer parity (the sort swaps the particle buffers).
+    cudaGraphExec_t period_graph[2] = {nullptr, nullptr};
+    cudaStream_t graph_stream[2] = {nullptr, nullptr};
+    int parity = 0;
+    bool use_graphs = true;
     bool needs_affine = true; // A must be recomputed from the state before the next P2G
     SlowQueue q{};
 };
@@ -113,6 +119,8 @@ void release(mpm_solver* s) {
     for (int* p : ti)
         if (p) cudaFree(p);
     if (s->ti.items) cudaFree(s->ti.items);
+    for (auto& g : s->period_graph)
+        if (g) cudaGraphExecDestroy(g);
     if (s->q.list) cudaFree(s->q.list);
     if (s->q.count) cudaFree(s->q.count);
     if (s->q.fh) cudaFree(s->q.fh);
@@ -151,15 +159,7 @@ template <int D, int FORM> cudaError_t launch_g2p(mpm_solver* s) {
 // Counting sort of the particle state by cell tile into the alternate
 // buffers, then swap. Called every sort_period steps (and after any state
 // upload) on the tiled path.
-template <int D> cudaError_t launch_sort(mpm_solver* s) {
-    if (s->n == 0) { s->needs_sort = false; return cudaMemsetAsync(s->ti.n_items, 0, sizeof(int), s->stream); }
-    const int threads = 256, blocks = (s->n + threads - 1) / threads;
-    k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
-    k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
-    k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
-    k_tile_sort<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+void swap_buffers(mpm_solver* s) {
     std::swap(s->x, s->alt.x);
     std::swap(s->v, s->alt.v);
     std::swap(s->B, s->alt.B);
@@ -169,6 +169,19 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
     std::swap(s->id, s->alt.id);
     if (s->mass) std::swap(s->mass, s->alt.mass);
     if (s->vol) std::swap(s->vol, s->alt.vol);
+    s->parity ^= 1;
+}
+
+template <int D> cudaError_t launch_sort(mpm_solver* s) {
+    if (s->n == 0) { s->needs_sort = false; return cudaMemsetAsync(s->ti.n_items, 0, sizeof(int), s->stream); }
+    const int threads = 256, blocks = (s->n + threads - 1) / threads;
+    k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
+    k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
+    k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
+    k_tile_sort<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    swap_buffers(s);
     s->needs_sort = false;
     return cudaSuccess;
 }
@@ -485,6 +498,61 @@ cudaError_t dispatch_stage(mpm_solver* s, int k) {
 }
 }  // namespace
 
+namespace {
+// Replays (capturing on first use) the graph of one sort period: the sort and
+// sort_period steps. The captured kernels hold the buffer pointers of the
+// current parity; the host-side buffer swap the sort performs is re-applied on
+// every replay.
+// Returns 1 when the period ran, 0 when graphs are unavailable (the caller then
+// steps without them), -1 on a CUDA error (s->err set).
+int run_period_graph(mpm_solver* s) {
+    const int par = s->parity;
+    if (!s->period_graph[par]) {
+        cudaStream_t cap = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            s->use_graphs = false;
+            return 0;
+        }
+        cudaStream_t saved = s->stream;
+        const long long step0 = s->step;
+        const bool ns = s->needs_sort;
+        s->stream = cap;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            s->needs_sort = true;  // the period starts with a sort
+            for (int k = 0; k < s->sort_period && e == cudaSuccess; ++k) {
+                e = dispatch_step(s);
+                ++s->step;
+            }
+            cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+        // undo the host-side effects of the capture (nothing ran)
+        s->stream = saved;
+        s->step = step0;
+        s->needs_sort = ns;
+        if (s->parity != par) swap_buffers(s);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&s->period_graph[par], g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess) {  // no graph: step without one
+            s->period_graph[par] = nullptr;
+            s->use_graphs = false;
+            cudaGetLastError();
+            return 0;
+        }
+    }
+    cudaError_t e = cudaGraphLaunch(s->period_graph[par], s->stream);
+    if (e != cudaSuccess) { cuda_fail(s, e, "graph launch"); return -1; }
+    swap_buffers(s);
+    s->needs_sort = false;
+    s->step += s->sort_period;
+    return 1;
+}
+}  // namespace
+
 extern "C" {
 
 void mpm_params_default(mpm_params* out, int32_t dim) {
@@ -626,10 +694,22 @@ mpm_status mpm_destroy(mpm_solver* s) {
 
 mpm_status mpm_step(mpm_solver* s, int32_t nsteps) {
     if (!s || nsteps < 0) return fail(s, MPM_ERR_INVALID_ARGUMENT, "nsteps must be >= 0");
-    for (int32_t k = 0; k < nsteps; ++k) {
+    int32_t k = 0;
+    while (k < nsteps) {
+        const int K = s->sort_period;
+        if (s->tiled && s->use_graphs && K > 0 && nsteps - k >= K && s->step % K == 0 && !s->needs_sort &&
+            !s->needs_affine) {
+            const int r = run_period_graph(s);
+            if (r < 0) return MPM_ERR_CUDA;
+            if (r > 0) {
+                k += K;
+                continue;
+            }
+        }
         cudaError_t e = dispatch_step(s);
         if (e != cudaSuccess) return cuda_fail(s, e, "step launch");
         ++s->step;
+        ++k;
     }
     return MPM_OK;
 }
