@@ -360,7 +360,7 @@ mpm_status setup_tiled(mpm_solver* s) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
     }
-    s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 8;
+    s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 16;
     s->needs_sort = true;
     return MPM_OK;
 }

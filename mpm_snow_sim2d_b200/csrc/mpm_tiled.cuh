@@ -88,42 +88,44 @@ __global__ void __launch_bounds__(256) k_sort_count(Particles P, StepConsts C, T
 // (a tile with n particles is ceil(n / kItem) items); writes the item list,
 // clears count/cursor for the next sort.
 __global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
-    __shared__ int s_cnt[1024], s_itm[1024];
+    __shared__ int s_cnt[1024], s_itm[1024], s_ne[1024];
     const int nt = TI.n_tiles, tid = threadIdx.x;
     const int chunk = (nt + 1023) / 1024;
     const int lo = min(nt, tid * chunk), hi = min(nt, lo + chunk);
-    int c = 0, it = 0;
+    int c = 0, it = 0, ne = 0;
     for (int t = lo; t < hi; ++t) {
         const int n = TI.tile_count[t];
         c += n;
         it += (n + kItem - 1) / kItem;
+        ne += n > 0;
     }
     s_cnt[tid] = c;
     s_itm[tid] = it;
+    s_ne[tid] = ne;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
+    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scans
         const int a = tid >= off ? s_cnt[tid - off] : 0;
         const int b = tid >= off ? s_itm[tid - off] : 0;
+        const int d = tid >= off ? s_ne[tid - off] : 0;
         __syncthreads();
         s_cnt[tid] += a;
         s_itm[tid] += b;
+        s_ne[tid] += d;
         __syncthreads();
     }
-    int base = s_cnt[tid] - c, ibase = s_itm[tid] - it;
+    int base = s_cnt[tid] - c, ibase = s_itm[tid] - it, lbase = s_ne[tid] - ne;
     for (int t = lo; t < hi; ++t) {
         const int n = TI.tile_count[t];
         TI.tile_start[t] = base;
         TI.tile_cursor[t] = 0;
         for (int j = 0; j < n; j += kItem) TI.items[ibase++] = make_int4(t, base + j, min(kItem, n - j), 0);
+        if (n > 0) TI.tile_list[lbase++] = t;  // non-empty tiles in tile order
         base += n;
     }
-    if (tid == 1023) *TI.n_items = s_itm[1023];
-    // list of the non-empty tiles (any order; each tile is sorted independently)
-    __syncthreads();
-    if (tid == 0) *TI.n_tile_list = 0;
-    __syncthreads();
-    for (int t = lo; t < hi; ++t)
-        if (TI.tile_count[t] > 0) TI.tile_list[atomicAdd(TI.n_tile_list, 1)] = t;
+    if (tid == 1023) {
+        *TI.n_items = s_itm[1023];
+        *TI.n_tile_list = s_ne[1023];
+    }
 }
 
 struct SortBuffers {
