@@ -206,6 +206,51 @@ MPM_API const char* mpm_stage_name(const mpm_solver* solver, int32_t stage);
 /* Fixed-point scales in use (log2), for diagnostics. */
 MPM_API mpm_status mpm_get_fixed_point(const mpm_solver* solver, int32_t* log2_mass, int32_t* log2_momentum);
 
+/* ------------------------------------------------------------------------
+ * Learned plasticity surrogate (no counterpart in the reference, which always
+ * runs the SVD return map of g2p.glsl:74-104). A 10 -> 64 -> 64 -> 64 -> 10
+ * GELU MLP, BF16 weights/activations, FP32 accumulation on the tensor cores,
+ * FP32 master weights trained with AdamW on the GPU. Inputs: trial F_hat - I and
+ * log J_p; outputs: F_E' - F_hat and log J_p' - log J_p (normalised per feature).
+ * Used only for particles whose trial F is outside the elastic band; a
+ * residual check with per-particle fallback to the exact SVD guards every
+ * prediction. Pairs are rows of 20 floats: F_hat[9] J_p F_E'[9] J_p'. */
+struct mpm_mlp;
+typedef struct mpm_mlp mpm_mlp;
+
+MPM_API int32_t mpm_mlp_param_count(void);
+MPM_API mpm_status mpm_mlp_create(uint64_t seed, mpm_mlp** out);
+MPM_API mpm_status mpm_mlp_destroy(mpm_mlp* mlp);
+MPM_API const char* mpm_mlp_last_error(const mpm_mlp* mlp);
+/* FP32 master parameters, layout W1[64][16] b1[64] W2[64][64] b2[64] W3[64][64]
+ * b3[64] W4[16][64] b4[16] (row-major W[out][in], padding zero). */
+MPM_API mpm_status mpm_mlp_set_params(mpm_mlp* mlp, const float* params, size_t count);
+MPM_API mpm_status mpm_mlp_get_params(mpm_mlp* mlp, float* out, size_t cap);
+MPM_API mpm_status mpm_mlp_set_normalization(mpm_mlp* mlp, const float* in_mean, const float* in_std,
+                                             const float* out_mean, const float* out_std);
+/* Upload training pairs (n rows of 20 floats) to the device. */
+MPM_API mpm_status mpm_mlp_load_pairs(mpm_mlp* mlp, const float* pairs, int64_t n);
+/* `steps` AdamW steps on random batches of the loaded pairs (MSE on the
+ * normalised outputs, cosine learning-rate decay); per-step loss into loss_out. */
+MPM_API mpm_status mpm_mlp_train(mpm_mlp* mlp, int32_t steps, int32_t batch, float lr, float weight_decay,
+                                 uint32_t seed, float* loss_out);
+/* Mean-squared loss and its parameter gradient on the given pairs (no update). */
+MPM_API mpm_status mpm_mlp_gradient(mpm_mlp* mlp, const float* pairs, int64_t n, float* grad_out, float* loss_out);
+/* Denormalised outputs for rows whose first 10 floats are F_hat[9], J_p. */
+MPM_API mpm_status mpm_mlp_predict(mpm_mlp* mlp, const float* inputs, int64_t n, int32_t stride, float* out);
+
+/* Return map of a solver: MPM_PLASTIC_EXACT, or MPM_PLASTIC_MLP with `mlp`
+ * (3D MLS) and the residual-check tolerance (1e-3). The network must outlive
+ * its use by the solver. */
+MPM_API mpm_status mpm_set_plasticity(mpm_solver* solver, int32_t mode, mpm_mlp* mlp, float tolerance);
+/* Particles the network handled (accepted) and those the residual check sent
+ * to the exact SVD (rejected), since the mode was set. */
+MPM_API mpm_status mpm_get_mlp_stats(mpm_solver* solver, uint64_t* accepted, uint64_t* rejected);
+/* Log of exact return-map pairs for out-of-band particles (3D MLS); capacity 0
+ * disables. Read copies up to cap_pairs logged pairs and restarts the log. */
+MPM_API mpm_status mpm_pair_log_enable(mpm_solver* solver, int64_t capacity);
+MPM_API mpm_status mpm_pair_log_read(mpm_solver* solver, float* out, int64_t cap_pairs, int64_t* n_pairs);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -84,6 +84,21 @@ SIGNATURES = {
     "mpm_step_profiled": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_double), C.c_int32]),
     "mpm_stage_count": (C.c_int32, [_P]),
     "mpm_stage_name": (C.c_char_p, [_P, C.c_int32]),
+    "mpm_mlp_param_count": (C.c_int32, []),
+    "mpm_mlp_create": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
+    "mpm_mlp_destroy": (C.c_int, [_P]),
+    "mpm_mlp_last_error": (C.c_char_p, [_P]),
+    "mpm_mlp_set_params": (C.c_int, [_P, C.POINTER(C.c_float), C.c_size_t]),
+    "mpm_mlp_get_params": (C.c_int, [_P, C.POINTER(C.c_float), C.c_size_t]),
+    "mpm_mlp_set_normalization": (C.c_int, [_P] + [C.POINTER(C.c_float)] * 4),
+    "mpm_mlp_load_pairs": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64]),
+    "mpm_mlp_train": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(C.c_float)]),
+    "mpm_mlp_gradient": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mpm_mlp_predict": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.c_int32, C.POINTER(C.c_float)]),
+    "mpm_set_plasticity": (C.c_int, [_P, C.c_int32, _P, C.c_float]),
+    "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),
+    "mpm_pair_log_read": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

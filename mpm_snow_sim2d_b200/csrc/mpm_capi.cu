@@ -3,6 +3,7 @@
 // CPU fallback: without a usable sm_100 device every create fails.
 #include <cmath>
 #include <cstdlib>
+#include <random>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -13,8 +14,25 @@
 #include "mpm/mpm.h"
 #include "mpm_kernels.cuh"
 #include "mpm_tiled.cuh"
+#include "mpm_mlp.cuh"
 
 using namespace mpm;
+
+struct mpm_mlp {
+    int device = 0;
+    float* w = nullptr;            // fp32 master parameters
+    __nv_bfloat16* wbf = nullptr;  // bf16 copy used by the kernels
+    float* grad = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    float* loss = nullptr;         // per training step
+    int loss_cap = 0;
+    float* pairs = nullptr;        // device training pairs [n][20]
+    long long n_pairs = 0;
+    long long step = 0;            // AdamW steps taken
+    MlpNorm norm{};
+    std::string err;
+};
 
 struct mpm_solver {
     mpm_params params{};
@@ -56,6 +74,15 @@ struct mpm_solver {
     cudaStream_t graph_stream[2] = {nullptr, nullptr};
     int parity = 0;
     bool use_graphs = true;
+    // plasticity: exact return map, or the learned surrogate with exact fallback
+    int plasticity = MPM_PLASTIC_EXACT;
+    mpm_mlp* mlp = nullptr;
+    float mlp_tol = 1e-3f;
+    unsigned long long* mlp_counters = nullptr;  // accepted, rejected
+    // exact return-map pairs for training
+    float* log_data = nullptr;
+    unsigned long long* log_n = nullptr;
+    long long log_cap = 0;
     bool needs_affine = true; // A must be recomputed from the state before the next P2G
     SlowQueue q{};
 };
@@ -121,6 +148,9 @@ void release(mpm_solver* s) {
     if (s->ti.items) cudaFree(s->ti.items);
     for (auto& g : s->period_graph)
         if (g) cudaGraphExecDestroy(g);
+    if (s->mlp_counters) cudaFree(s->mlp_counters);
+    if (s->log_data) cudaFree(s->log_data);
+    if (s->log_n) cudaFree(s->log_n);
     if (s->q.list) cudaFree(s->q.list);
     if (s->q.count) cudaFree(s->q.count);
     if (s->q.fh) cudaFree(s->q.fh);
@@ -172,6 +202,14 @@ void swap_buffers(mpm_solver* s) {
     s->parity ^= 1;
 }
 
+// Captured period graphs bake in kernel choices and pointers: drop them when
+// the plasticity mode or the pair log changes.
+void invalidate_graphs(mpm_solver* s) {
+    cudaStreamSynchronize(s->stream);
+    for (auto& g : s->period_graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 template <int D> cudaError_t launch_sort(mpm_solver* s) {
     if (s->n == 0) { s->needs_sort = false; return cudaMemsetAsync(s->ti.n_items, 0, sizeof(int), s->stream); }
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
@@ -209,7 +247,14 @@ template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
     if (e != cudaSuccess) return e;
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
     k_g2p_gather<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
-    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
+    if (D == 3 && s->plasticity == MPM_PLASTIC_MLP && s->mlp) {
+        MlpParams ML{s->mlp->wbf, s->mlp->w, s->mlp->norm, s->mlp_tol, s->mlp_counters};
+        k_g2p_plastic_mlp<<<s->sms * 4, 128, sizeof(MlpInferSmem), s->stream>>>(particle_view(s), s->C, s->gv, s->q, ML,
+                                                                               s->status);
+    } else {
+        PairLog L{s->log_data, s->log_n, s->log_cap};
+        k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, L, s->status);
+    }
     return cudaGetLastError();
 }
 
@@ -950,6 +995,271 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
         s->needs_sort = false;
     }
     s->step = step;
+    return MPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Learned plasticity surrogate.
+
+int32_t mpm_mlp_param_count(void) { return MlpOff::total; }
+
+mpm_status mpm_mlp_create(uint64_t seed, mpm_mlp** out) {
+    if (!out) return MPM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return MPM_ERR_NO_DEVICE; }
+    mpm_mlp* m = new mpm_mlp();
+    cudaGetDevice(&m->device);
+    const int P = MlpOff::total;
+    if (dalloc(&m->w, P) || dalloc(&m->wbf, P) || dalloc(&m->grad, P) || dalloc(&m->m1, P) || dalloc(&m->m2, P)) {
+        mpm_mlp_destroy(m);
+        return MPM_ERR_OUT_OF_MEMORY;
+    }
+    // uniform initialisation with variance 1/fan_in (output layer x0.1), zero biases and padding
+    std::vector<float> w(P, 0.f);
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<float> U(-1.f, 1.f);
+    auto fill = [&](int off, int rows, int cols, int used_rows, int used_cols, float gain) {
+        const float a = gain * std::sqrt(3.f / float(used_cols));
+        for (int r = 0; r < rows; ++r)
+            for (int c = 0; c < cols; ++c) w[off + r * cols + c] = (r < used_rows && c < used_cols) ? a * U(rng) : 0.f;
+    };
+    fill(MlpOff::W1, kMlpHid, kMlpInPad, kMlpHid, kMlpIn, 1.f);
+    fill(MlpOff::W2, kMlpHid, kMlpHid, kMlpHid, kMlpHid, 1.f);
+    fill(MlpOff::W3, kMlpHid, kMlpHid, kMlpHid, kMlpHid, 1.f);
+    fill(MlpOff::W4, kMlpOutPad, kMlpHid, kMlpOut, kMlpHid, 0.1f);
+    for (int k = 0; k < kMlpIn; ++k) { m->norm.in_mean[k] = 0.f; m->norm.in_std[k] = 1.f; }
+    for (int k = 0; k < kMlpOut; ++k) { m->norm.out_mean[k] = 0.f; m->norm.out_std[k] = 1.f; }
+    mpm_status st = mpm_mlp_set_params(m, w.data(), (size_t)P);
+    if (st != MPM_OK) { mpm_mlp_destroy(m); return st; }
+    *out = m;
+    return MPM_OK;
+}
+
+mpm_status mpm_mlp_destroy(mpm_mlp* m) {
+    if (!m) return MPM_ERR_INVALID_ARGUMENT;
+    void* ptrs[] = {m->w, m->wbf, m->grad, m->m1, m->m2, m->loss, m->pairs};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete m;
+    return MPM_OK;
+}
+
+const char* mpm_mlp_last_error(const mpm_mlp* m) { return m ? m->err.c_str() : "null network"; }
+
+mpm_status mpm_mlp_set_params(mpm_mlp* m, const float* params, size_t count) {
+    if (!m || !params || count != (size_t)MlpOff::total) return MPM_ERR_INVALID_ARGUMENT;
+    std::vector<__nv_bfloat16> b(count);
+    for (size_t i = 0; i < count; ++i) b[i] = __float2bfloat16_rn(params[i]);
+    if (cudaMemcpy(m->w, params, sizeof(float) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->wbf, b.data(), sizeof(__nv_bfloat16) * count, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m->grad, 0, sizeof(float) * count) != cudaSuccess ||
+        cudaMemset(m->m1, 0, sizeof(float) * count) != cudaSuccess ||
+        cudaMemset(m->m2, 0, sizeof(float) * count) != cudaSuccess) {
+        cudaGetLastError();
+        m->err = "parameter upload failed";
+        return MPM_ERR_CUDA;
+    }
+    m->step = 0;
+    return MPM_OK;
+}
+
+mpm_status mpm_mlp_get_params(mpm_mlp* m, float* out, size_t cap) {
+    if (!m || !out) return MPM_ERR_INVALID_ARGUMENT;
+    if (cap < (size_t)MlpOff::total) return MPM_ERR_CAPACITY;
+    if (cudaMemcpy(out, m->w, sizeof(float) * MlpOff::total, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return MPM_ERR_CUDA;
+    }
+    return MPM_OK;
+}
+
+mpm_status mpm_mlp_set_normalization(mpm_mlp* m, const float* in_mean, const float* in_std, const float* out_mean,
+                                     const float* out_std) {
+    if (!m || !in_mean || !in_std || !out_mean || !out_std) return MPM_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < kMlpIn; ++k) {
+        if (!(in_std[k] > 0.f)) return MPM_ERR_INVALID_ARGUMENT;
+        m->norm.in_mean[k] = in_mean[k];
+        m->norm.in_std[k] = in_std[k];
+    }
+    for (int k = 0; k < kMlpOut; ++k) {
+        if (!(out_std[k] > 0.f)) return MPM_ERR_INVALID_ARGUMENT;
+        m->norm.out_mean[k] = out_mean[k];
+        m->norm.out_std[k] = out_std[k];
+    }
+    return MPM_OK;
+}
+
+mpm_status mpm_mlp_load_pairs(mpm_mlp* m, const float* pairs, int64_t n) {
+    if (!m || n < 0 || (n > 0 && !pairs)) return MPM_ERR_INVALID_ARGUMENT;
+    if (m->pairs) cudaFree(m->pairs);
+    m->pairs = nullptr;
+    m->n_pairs = 0;
+    if (n == 0) return MPM_OK;
+    if (dalloc(&m->pairs, (size_t)n * 20)) { cudaGetLastError(); return MPM_ERR_OUT_OF_MEMORY; }
+    if (cudaMemcpy(m->pairs, pairs, sizeof(float) * 20 * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        return MPM_ERR_CUDA;
+    }
+    m->n_pairs = n;
+    return MPM_OK;
+}
+
+static mpm_status mlp_launch_grad(mpm_mlp* m, const float* dpairs, long long np, const int* didx, int rows,
+                                  unsigned seed, float* dloss) {
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpTrainSmem)) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return MPM_ERR_CUDA;
+        }
+        attr = true;
+    }
+    const int blocks = (rows + kMlpTrainRows - 1) / kMlpTrainRows;
+    k_mlp_train<<<blocks, 128, sizeof(MlpTrainSmem)>>>(dpairs, np, didx, rows, seed, m->wbf, m->w, m->norm, m->grad,
+                                                        dloss);
+    return cudaGetLastError() == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+mpm_status mpm_mlp_train(mpm_mlp* m, int32_t steps, int32_t batch, float lr, float weight_decay, uint32_t seed,
+                         float* loss_out) {
+    if (!m || steps < 0 || batch < 1) return MPM_ERR_INVALID_ARGUMENT;
+    if (m->n_pairs <= 0) { m->err = "no training pairs loaded"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (steps > m->loss_cap) {
+        if (m->loss) cudaFree(m->loss);
+        m->loss = nullptr;
+        if (dalloc(&m->loss, (size_t)steps)) { cudaGetLastError(); return MPM_ERR_OUT_OF_MEMORY; }
+        m->loss_cap = steps;
+    }
+    if (cudaMemset(m->loss, 0, sizeof(float) * steps) != cudaSuccess) return MPM_ERR_CUDA;
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (int it = 0; it < steps; ++it) {
+        // cosine decay to lr / 20
+        const float frac = steps > 1 ? float(it) / float(steps - 1) : 0.f;
+        const float lr_t = lr * (0.05f + 0.95f * 0.5f * (1.f + std::cos(3.14159265f * frac)));
+        mpm_status st = mlp_launch_grad(m, m->pairs, m->n_pairs, nullptr, batch, seed * 2654435761u + (unsigned)it,
+                                        m->loss + it);
+        if (st != MPM_OK) return st;
+        ++m->step;
+        const float bc1 = 1.f - std::pow(b1, (float)m->step), bc2 = 1.f - std::pow(b2, (float)m->step);
+        k_mlp_adam<<<(MlpOff::total + 255) / 256, 256>>>(m->w, m->wbf, m->grad, m->m1, m->m2, lr_t, b1, b2, 1e-8f,
+                                                          weight_decay, bc1, bc2);
+        if (cudaGetLastError() != cudaSuccess) return MPM_ERR_CUDA;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) { cudaGetLastError(); return MPM_ERR_CUDA; }
+    if (loss_out && steps > 0 &&
+        cudaMemcpy(loss_out, m->loss, sizeof(float) * steps, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    return MPM_OK;
+}
+
+mpm_status mpm_mlp_gradient(mpm_mlp* m, const float* pairs, int64_t n, float* grad_out, float* loss_out) {
+    if (!m || !pairs || n < 1 || n > (1 << 24) || !grad_out) return MPM_ERR_INVALID_ARGUMENT;
+    float *dp = nullptr, *dl = nullptr;
+    int* di = nullptr;
+    std::vector<int> idx((size_t)n);
+    for (int64_t i = 0; i < n; ++i) idx[i] = (int)i;
+    mpm_status st = MPM_OK;
+    if (dalloc(&dp, (size_t)n * 20) || dalloc(&dl, 1) || dalloc(&di, (size_t)n)) st = MPM_ERR_OUT_OF_MEMORY;
+    if (st == MPM_OK && (cudaMemcpy(dp, pairs, sizeof(float) * 20 * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                         cudaMemcpy(di, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                         cudaMemset(dl, 0, sizeof(float)) != cudaSuccess ||
+                         cudaMemset(m->grad, 0, sizeof(float) * MlpOff::total) != cudaSuccess))
+        st = MPM_ERR_CUDA;
+    if (st == MPM_OK) st = mlp_launch_grad(m, dp, n, di, (int)n, 0u, dl);
+    if (st == MPM_OK && cudaDeviceSynchronize() != cudaSuccess) st = MPM_ERR_CUDA;
+    if (st == MPM_OK && cudaMemcpy(grad_out, m->grad, sizeof(float) * MlpOff::total, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = MPM_ERR_CUDA;
+    if (st == MPM_OK && loss_out && cudaMemcpy(loss_out, dl, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = MPM_ERR_CUDA;
+    cudaMemset(m->grad, 0, sizeof(float) * MlpOff::total);
+    if (dp) cudaFree(dp);
+    if (dl) cudaFree(dl);
+    if (di) cudaFree(di);
+    cudaGetLastError();
+    return st;
+}
+
+mpm_status mpm_mlp_predict(mpm_mlp* m, const float* inputs, int64_t n, int32_t stride, float* out) {
+    if (!m || !inputs || !out || n < 1 || stride < 10 || n > (1 << 26)) return MPM_ERR_INVALID_ARGUMENT;
+    float *di = nullptr, *dout = nullptr;
+    mpm_status st = MPM_OK;
+    if (dalloc(&di, (size_t)n * stride) || dalloc(&dout, (size_t)n * kMlpOut)) st = MPM_ERR_OUT_OF_MEMORY;
+    if (st == MPM_OK && cudaMemcpy(di, inputs, sizeof(float) * n * stride, cudaMemcpyHostToDevice) != cudaSuccess)
+        st = MPM_ERR_CUDA;
+    if (st == MPM_OK) {
+        k_mlp_forward<<<(unsigned)((n + kMlpTrainRows - 1) / kMlpTrainRows), 128, sizeof(MlpInferSmem)>>>(
+            di, stride, (int)n, m->wbf, m->w, m->norm, dout);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = MPM_ERR_CUDA;
+    }
+    if (st == MPM_OK && cudaMemcpy(out, dout, sizeof(float) * n * kMlpOut, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = MPM_ERR_CUDA;
+    if (di) cudaFree(di);
+    if (dout) cudaFree(dout);
+    cudaGetLastError();
+    return st;
+}
+
+mpm_status mpm_set_plasticity(mpm_solver* s, int32_t mode, mpm_mlp* mlp, float tolerance) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    if (mode != MPM_PLASTIC_EXACT && mode != MPM_PLASTIC_MLP) return fail(s, MPM_ERR_INVALID_ARGUMENT, "unknown plasticity mode");
+    if (mode == MPM_PLASTIC_MLP) {
+        if (!mlp) return fail(s, MPM_ERR_INVALID_ARGUMENT, "MLP plasticity needs a network");
+        if (s->dim != 3 || !s->tiled) return fail(s, MPM_ERR_UNSUPPORTED, "the learned return map is 3D MLS only");
+        if (!(tolerance > 0.f)) return fail(s, MPM_ERR_INVALID_ARGUMENT, "tolerance must be > 0");
+        if (!s->mlp_counters) {
+            MPM_CUDA(s, dalloc(&s->mlp_counters, 2));
+            MPM_CUDA(s, cudaMemset(s->mlp_counters, 0, 2 * sizeof(unsigned long long)));
+        }
+        s->mlp_tol = tolerance;
+    }
+    invalidate_graphs(s);
+    s->plasticity = mode;
+    s->mlp = mode == MPM_PLASTIC_MLP ? mlp : nullptr;
+    return MPM_OK;
+}
+
+mpm_status mpm_get_mlp_stats(mpm_solver* s, uint64_t* accepted, uint64_t* rejected) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    unsigned long long h[2] = {0, 0};
+    if (s->mlp_counters) {
+        MPM_CUDA(s, cudaMemcpyAsync(h, s->mlp_counters, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+        MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    }
+    if (accepted) *accepted = h[0];
+    if (rejected) *rejected = h[1];
+    return MPM_OK;
+}
+
+mpm_status mpm_pair_log_enable(mpm_solver* s, int64_t capacity) {
+    if (!s || capacity < 0) return MPM_ERR_INVALID_ARGUMENT;
+    if (s->dim != 3 || !s->tiled) return fail(s, MPM_ERR_UNSUPPORTED, "pair logging is 3D MLS only");
+    invalidate_graphs(s);
+    if (s->log_data) cudaFree(s->log_data);
+    s->log_data = nullptr;
+    s->log_cap = 0;
+    if (capacity == 0) return MPM_OK;
+    if (!s->log_n) MPM_CUDA(s, dalloc(&s->log_n, 1));
+    MPM_CUDA(s, dalloc(&s->log_data, (size_t)capacity * 20));
+    MPM_CUDA(s, cudaMemset(s->log_n, 0, sizeof(unsigned long long)));
+    s->log_cap = capacity;
+    return MPM_OK;
+}
+
+mpm_status mpm_pair_log_read(mpm_solver* s, float* out, int64_t cap_pairs, int64_t* n_pairs) {
+    if (!s || !n_pairs || cap_pairs < 0 || (cap_pairs > 0 && !out)) return MPM_ERR_INVALID_ARGUMENT;
+    unsigned long long n = 0;
+    if (s->log_n) {
+        MPM_CUDA(s, cudaMemcpyAsync(&n, s->log_n, sizeof(n), cudaMemcpyDeviceToHost, s->stream));
+        MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    }
+    const long long avail = (long long)n < s->log_cap ? (long long)n : s->log_cap;
+    const long long take = avail < cap_pairs ? avail : cap_pairs;
+    if (take > 0)
+        MPM_CUDA(s, cudaMemcpy(out, s->log_data, sizeof(float) * 20 * (size_t)take, cudaMemcpyDeviceToHost));
+    if (s->log_n) MPM_CUDA(s, cudaMemset(s->log_n, 0, sizeof(unsigned long long)));
+    *n_pairs = take;
     return MPM_OK;
 }
 

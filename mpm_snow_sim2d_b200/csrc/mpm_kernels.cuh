@@ -722,70 +722,95 @@ __global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C
     if (!finite) raise_flag(status, 1u);
 }
 
-// Queued particles: the full return map for out-of-band trial F (entry i), or
-// the whole G2P with a grid-clipped stencil (entry -1 - i).
+// Optional log of exact return-map pairs (F_hat[9], J_p, F_E'[9], J_p') for
+// training the learned surrogate; appended while room is left.
+struct PairLog {
+    float* data;            // [capacity][20]
+    unsigned long long* n;  // device counter (may exceed capacity: excess dropped)
+    long long capacity;
+};
+
+// One queued particle: the full return map for an out-of-band trial F (entry
+// i), or the whole G2P with a grid-clipped stencil (entry -1 - i).
+template <int D>
+__device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepConsts& C, const float4* __restrict__ gv,
+                                                 const SlowQueue& Q, int e, unsigned* __restrict__ status,
+                                                 PairLog L = PairLog{nullptr, nullptr, 0}) {
+    const int n = P.n;
+    const int entry = Q.list[e];
+    const int i = entry >= 0 ? entry : -1 - entry;
+    float Fh[D * D], Fe[D * D], B[D * D], A[D * D];
+    if (entry >= 0) {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
+    } else {
+        float x[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
+        int base[3] = {0, 0, 0};
+        float wk[3][4], off[3][4];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+            base[k] = stencil_base(x[k], ext);
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                const float dist = x[k] - float(base[k] + o);
+                wk[k][o] = bspline_n(dist);
+                off[k][o] = -dist;
+            }
+        }
+        float nv[D], nx[D];
+        const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, B, nx);
+        bool finite = true;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const float xn = x[k] * wsum + nx[k];
+            P.v[k * n + i] = nv[k];
+            P.x[k * n + i] = xn;
+            finite = finite && isfinite(xn);
+        }
+        if (!finite) raise_flag(status, 1u);
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) { P.B[k * n + i] = B[k]; Fe[k] = P.Fe[k * n + i]; }
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                float s = Fe[r * D + c];
+#pragma unroll
+                for (int k = 0; k < D; ++k) s += (C.dt * 3.f * B[r * D + k]) * Fe[k * D + c];
+                Fh[r * D + c] = s;
+            }
+    }
+    const float Jp0 = P.Jp[i];
+    float Jp = Jp0;
+    plasticity<D, kMLS>(C, Fh, Fe, Jp, status);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
+    P.Jp[i] = Jp;
+    mls_affine<D>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
+    if (!isfinite(Jp)) raise_flag(status, 1u);
+    if (D == 3 && L.data && entry >= 0) {
+        const unsigned long long slot = atomicAdd(L.n, 1ull);
+        if ((long long)slot < L.capacity) {
+            float* d = L.data + slot * 20;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) { d[k] = Fh[k]; d[10 + k] = Fe[k]; }
+            d[9] = Jp0;
+            d[19] = Jp;
+        }
+    }
+}
+
 template <int D>
 __global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, const float4* __restrict__ gv,
-                                                     SlowQueue Q, unsigned* __restrict__ status) {
+                                                     SlowQueue Q, PairLog L, unsigned* __restrict__ status) {
     const int m = *Q.count;
-    const int n = P.n;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
-        const int entry = Q.list[e];
-        const int i = entry >= 0 ? entry : -1 - entry;
-        float Fh[D * D], Fe[D * D], B[D * D], A[D * D];
-        if (entry >= 0) {
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
-        } else {
-            float x[D];
-#pragma unroll
-            for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
-            int base[3] = {0, 0, 0};
-            float wk[3][4], off[3][4];
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-                base[k] = stencil_base(x[k], ext);
-#pragma unroll
-                for (int o = 0; o < 4; ++o) {
-                    const float dist = x[k] - float(base[k] + o);
-                    wk[k][o] = bspline_n(dist);
-                    off[k][o] = -dist;
-                }
-            }
-            float nv[D], nx[D];
-            const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, B, nx);
-            bool finite = true;
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const float xn = x[k] * wsum + nx[k];
-                P.v[k * n + i] = nv[k];
-                P.x[k * n + i] = xn;
-                finite = finite && isfinite(xn);
-            }
-            if (!finite) raise_flag(status, 1u);
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) { P.B[k * n + i] = B[k]; Fe[k] = P.Fe[k * n + i]; }
-#pragma unroll
-            for (int r = 0; r < D; ++r)
-#pragma unroll
-                for (int c = 0; c < D; ++c) {
-                    float s = Fe[r * D + c];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) s += (C.dt * 3.f * B[r * D + k]) * Fe[k * D + c];
-                    Fh[r * D + c] = s;
-                }
-        }
-        float Jp = P.Jp[i];
-        plasticity<D, kMLS>(C, Fh, Fe, Jp, status);
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
-        P.Jp[i] = Jp;
-        mls_affine<D>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
-        if (!isfinite(Jp)) raise_flag(status, 1u);
-    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
+        g2p_queued_exact<D>(P, C, gv, Q, e, status, L);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,125 @@
+"""Train the learned plasticity surrogate on pairs logged by the plain solver.
+
+    python -m mpm_snow_sim2d_b200.mlp_train [--pairs 4000000] [--steps 4000] [--out PATH]
+
+Data: seeded snowball-on-slab impacts (the 3D workload's set-up, 64^3 grid so
+that contact starts at once) with impact speeds drawn from U(1, 8) m/s; every
+step logs the exact return map (F_hat, J_p) -> (F_E', J_p') of each particle
+whose trial F left the elastic band (mpm_pair_log_*). Training: the library's
+own GPU kernels (BF16 tensor-core forward/backward, AdamW). Writes the FP32
+parameters and the feature normalisation to an .npz.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+from . import Solver, _lib, scenes
+from .mlp import DEFAULT_WEIGHTS, Mlp, features, normalization, targets
+
+
+def impact_scene(speed: float, seed: int, W: int = 64, steps: int = 200):
+    """A snowball launched at `speed` m/s into a slab, touching it at the start."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    radius = rng.uniform(0.1, 0.16)
+    slab = 0.1
+    m = scenes.MARGIN * dx
+    top = m + slab
+    cy = top + radius + 0.5 * dx
+    ang = rng.uniform(-0.5, 0.5)
+    ball = scenes._ball(rng, (rng.uniform(0.35, 0.65), cy, rng.uniform(0.35, 0.65)), radius, 8, dx)
+    box = scenes._box(rng, (m, m, m), (1.0 - m, top, 1.0 - m), 8, dx)
+    pos = np.concatenate([ball, box])
+    vel = np.zeros_like(pos)
+    vel[: ball.shape[0], 0] = speed * np.sin(ang)
+    vel[: ball.shape[0], 1] = -speed * np.cos(ang)
+    return scenes._scene(f"impact_v{speed:.2f}", 3, W, 5e-5, steps, pos, vel, 8, dict(seed=seed))
+
+
+def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 200, per_scene: int = 1_000_000,
+                  verbose: bool = True) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    chunks, total, k = [], 0, 0
+    while total < n_pairs:
+        speed = float(rng.uniform(1.0, 8.0))
+        sc = impact_scene(speed, seed * 1000 + k, W=W, steps=steps)
+        cap = min(per_scene, n_pairs - total)
+        with Solver.from_scene(sc) as s:
+            s.pair_log_enable(cap)
+            taken = []
+            for _ in range(steps // 10):
+                s.Step(10)
+                got = s.pair_log_read(cap)
+                if got.shape[0]:
+                    taken.append(got)
+                    cap -= got.shape[0]
+                if cap <= 0:
+                    break
+            s.pair_log_enable(0)
+        p = np.concatenate(taken) if taken else np.empty((0, 20), np.float32)
+        p = p[np.isfinite(p).all(1) & (p[:, 9] > 0) & (p[:, 19] > 0)]
+        chunks.append(p)
+        total += p.shape[0]
+        k += 1
+        if verbose:
+            print(f"scene {k}: speed {speed:.2f} m/s, {sc.count} particles, {p.shape[0]} pairs (total {total})")
+    return np.concatenate(chunks)[:n_pairs]
+
+
+def evaluate(mlp: Mlp, pairs: np.ndarray):
+    """Relative error of the predicted F_E' against the exact one, per pair."""
+    pred = mlp.predict(pairs)
+    F_pred = pairs[:, :9].astype(np.float64) + pred[:, :9]
+    F_true = pairs[:, 10:19].astype(np.float64)
+    err = np.linalg.norm(F_pred - F_true, axis=1) / np.linalg.norm(F_true, axis=1)
+    base = np.linalg.norm(pairs[:, :9] - F_true, axis=1) / np.linalg.norm(F_true, axis=1)
+    return err, base
+
+
+def train(pairs: np.ndarray, steps: int = 4000, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
+          holdout: float = 0.02):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    perm = rng.permutation(pairs.shape[0])
+    n_hold = max(1, int(holdout * pairs.shape[0]))
+    test, tr = pairs[perm[:n_hold]], pairs[perm[n_hold:]]
+    mlp = Mlp(seed)
+    mlp.set_normalization(*normalization(tr))
+    mlp.load_pairs(tr)
+    t0 = time.perf_counter()
+    loss = mlp.train(steps, batch=batch, lr=lr, seed=seed + 1)
+    dt = time.perf_counter() - t0
+    err, base = evaluate(mlp, test)
+    return mlp, dict(loss=loss, train_seconds=dt, heldout_rel_err_median=float(np.median(err)),
+                     heldout_rel_err_p99=float(np.percentile(err, 99)),
+                     identity_rel_err_median=float(np.median(base)), n_train=int(tr.shape[0]),
+                     n_test=int(test.shape[0]))
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=4_000_000)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
+    args = ap.parse_args(argv)
+    _lib.load()
+    t0 = time.perf_counter()
+    pairs = collect_pairs(args.pairs, seed=args.seed)
+    print(f"collected {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
+    mlp, info = train(pairs, steps=args.steps, batch=args.batch, lr=args.lr, seed=args.seed)
+    print({k: v for k, v in info.items() if k != "loss"}, "loss first/last", float(info["loss"][0]),
+          float(info["loss"][-1]))
+    from pathlib import Path
+    Path(args.out).parent.mkdir(parents=True, exist_ok=True)
+    mlp.save(args.out)
+    print("saved", args.out)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -156,6 +156,27 @@ class Solver:
         check(self._lib.mpm_step_profiled(self._h, int(nsteps), ms, n), self._h)
         return {self._lib.mpm_stage_name(self._h, k).decode(): float(ms[k]) for k in range(n)}
 
+    # -- learned plasticity ---------------------------------------------------
+    def set_plasticity(self, mode: int, mlp=None, tolerance: float = 1e-3) -> None:
+        """_lib.PLASTIC_EXACT, or _lib.PLASTIC_MLP with an Mlp (kept alive by the caller)."""
+        self._mlp_ref = mlp
+        check(self._lib.mpm_set_plasticity(self._h, int(mode), mlp._h if mlp is not None else None,
+                                           float(tolerance)), self._h)
+
+    def mlp_stats(self):
+        a, r = C.c_uint64(), C.c_uint64()
+        check(self._lib.mpm_get_mlp_stats(self._h, C.byref(a), C.byref(r)), self._h)
+        return int(a.value), int(r.value)
+
+    def pair_log_enable(self, capacity: int) -> None:
+        check(self._lib.mpm_pair_log_enable(self._h, int(capacity)), self._h)
+
+    def pair_log_read(self, cap: int) -> np.ndarray:
+        out = np.empty((cap, 20), np.float32)
+        n = C.c_int64()
+        check(self._lib.mpm_pair_log_read(self._h, fptr(out), cap, C.byref(n)), self._h)
+        return out[: n.value].copy()
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.mpm_destroy(self._h)
