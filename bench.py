@@ -43,6 +43,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-updates/s (P2G+grid+G2P), plain vs MLP-plasticity, 1 B200, % HBM peak"
 UNIT = "particle-updates/s"
+DEFAULT_SORT_PERIOD = 16  # the solver's re-sort interval when mpm_params.sort_period is 0
 
 # Algorithmic bytes (minimal FP32 SoA state, uniform mass/volume).
 # Per particle-step: P2G reads x, v, B, F_E, J_p; G2P reads x, F_E, J_p and
@@ -140,6 +141,54 @@ def make_scene(name):
     return scenes.workload(name)
 
 
+def kernel_launches(steps, step0, sort_period):
+    """Kernels the tiled 3D/2D MLS step enqueues for steps [step0, step0 + steps):
+    P2G, grid update, G2P gather and G2P plastic every step, plus the four sort
+    kernels (count, scan, bucket, per-tile sort) on multiples of sort_period."""
+    sorts = sum(1 for k in range(step0, step0 + steps) if sort_period > 0 and k % sort_period == 0)
+    return 4 * steps + 4 * sorts
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def mlp_vs_plain(args, torch, stream):
+    """The learned return map against the exact one on the same seeded inputs:
+    per-stage device time over the whole run (G2P = gather + return map), and
+    the relative L2 error of x, v, F_E after it."""
+    from mpm_snow_sim2d_b200 import Solver, _lib
+    from mpm_snow_sim2d_b200.mlp import DEFAULT_WEIGHTS, Mlp
+    scene = make_scene(args.mlp_workload)
+    net = Mlp.load(DEFAULT_WEIGHTS)
+    res, states = {}, {}
+    for mode in ("exact", "mlp"):
+        s = Solver.from_scene(scene)
+        s.set_stream(stream.cuda_stream)
+        if mode == "mlp":
+            s.set_plasticity(_lib.PLASTIC_MLP, net, args.mlp_tolerance)
+        stages = s.step_profiled(args.mlp_steps)
+        torch.cuda.synchronize()
+        states[mode] = s.get_state()
+        r = {"stages_ms": {k: v / args.mlp_steps for k, v in stages.items()},
+             "ms_per_step": sum(stages.values()) / args.mlp_steps, "status_flags": s.status()}
+        if mode == "mlp":
+            acc, rej = s.mlp_stats()
+            r.update(accepted=acc, fell_back=rej, accepted_frac=acc / max(acc + rej, 1))
+        s.close()
+        res[mode] = r
+    a, b = states["mlp"], states["exact"]
+    return {
+        "workload": f"{args.mlp_workload}: {WORKLOADS[args.mlp_workload]}", "particles": scene.count,
+        "steps": args.mlp_steps, "tolerance": args.mlp_tolerance, "plain": res["exact"], "mlp": res["mlp"],
+        "g2p_speedup": res["exact"]["stages_ms"]["g2p"] / res["mlp"]["stages_ms"]["g2p"],
+        "step_speedup": res["exact"]["ms_per_step"] / res["mlp"]["ms_per_step"],
+        "rel_l2_vs_plain": {"F_E": rel_l2(a.elastic_f, b.elastic_f), "x": rel_l2(a.position, b.position),
+                            "v": rel_l2(a.velocity, b.velocity), "J_p": rel_l2(a.plastic_det, b.plastic_det)},
+        "timing": "CUDA events between stages every step (no graph replay), whole run",
+    }
+
+
 def cpu_port_time(scene, target_s=12.0, max_steps=20):
     """FP32 OpenMP port of the reference MLS step on all host cores."""
     from oracle import oracle as O
@@ -214,6 +263,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--budget-s", type=float, default=60.0, help="CPU time cap of the reference arm")
     ap.add_argument("--sort-period", type=int, default=0, help="steps between particle re-sorts (0: solver default)")
+    ap.add_argument("--mlp-workload", default="c5", choices=sorted(WORKLOADS))
+    ap.add_argument("--mlp-steps", type=int, default=1000)
+    ap.add_argument("--mlp-tolerance", type=float, default=1e-3)
+    ap.add_argument("--no-mlp", action="store_true", help="skip the learned-plasticity comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -247,6 +300,8 @@ def main():
     # warm-up, then active-node count (untimed P2G-only pass)
     solver.Step(args.warmup)
     torch.cuda.synchronize()
+    step0 = solver.step_count()
+    sort_period = args.sort_period if args.sort_period > 0 else DEFAULT_SORT_PERIOD
     m, _ = solver.rasterize()
     active = int((m > 0).sum())
 
@@ -317,6 +372,13 @@ def main():
                 "step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
                          "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
 
+    mlp = None
+    if world == 1 and not args.no_mlp and d == 3:
+        try:
+            mlp = mlp_vs_plain(args, torch, stream)
+        except Exception as e:  # reported next to the headline, never required for it
+            mlp = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -337,10 +399,11 @@ def main():
             "stages_ms": stage_avg,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": ke},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": kernel_launches(args.steps, step0, sort_period),
             "clocks": clocks.summary(),
             "status_flags": flags,
             "cpu_baseline": cpu,
+            "mlp_vs_plain": mlp,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -338,8 +338,14 @@ namespace mpm {
 // [t0^2, t1^2], and in each common eigendirection either m = 1 (unclamped) or
 // q is at a band edge with m on the right side of 1:
 //   (M - I)(Q - t0^2 I)(Q - t1^2 I) = 0,  (M - I)(Q - t0^2 I) >= 0,  (M - I)(Q - t1^2 I) >= 0.
-// These conditions characterise the map; the prediction is accepted when each
-// holds to a relative tolerance `tol` (1e-3). Any failure sends the particle to
+// These conditions characterise the map (with M > 0, so that S_hat = M S keeps
+// the sign of S). `tol` bounds the relative error of the predicted F_E': an
+// error E in F_E' moves M and Q by O(|E|), so each condition is tested to the
+// slack that |E| = tol |F_E'| can produce (asymmetry and commutator relative
+// to |M| and |M||Q|; Q's eigenvalues to 2 tol outside the band; the sign
+// conditions to -tol (w + 2|M - I|), w = t1^2 - t0^2). Semidefiniteness is
+// tested by Gershgorin first and, when that is inconclusive, by Sylvester's
+// criterion in FP64 on the shifted matrix. Any failure sends the particle to
 // the exact SVD.
 __device__ __forceinline__ bool gersh_min_ge(const float* S, float bound) {
 #pragma unroll
@@ -351,6 +357,16 @@ __device__ __forceinline__ bool gersh_min_ge(const float* S, float bound) {
         if (S[i * 4] - r < bound) return false;
     }
     return true;
+}
+
+// A symmetric 3x3 S satisfies S >= bound I (bound <= 0): Gershgorin, else
+// Sylvester's criterion on S - 1.0001 bound I in FP64.
+__device__ __forceinline__ bool sym_min_ge(const float* S, float bound) {
+    if (gersh_min_ge(S, bound)) return true;
+    double D[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) D[k] = double(S[k]) - (k % 4 == 0 ? 1.0001 * double(bound) : 0.0);
+    return D[0] > 0.0 && D[0] * D[4] - D[1] * D[3] > 0.0 && det<3>(D) > 0.0;
 }
 
 __device__ __forceinline__ bool mlp_residual_ok(const float* Fh, const float* Fe, float t0, float t1, float tol) {
@@ -398,17 +414,8 @@ __device__ __forceinline__ bool mlp_residual_ok(const float* Fh, const float* Fe
     float Ql[9], Qh[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) { Ql[k] = Q[k] - (k % 4 == 0 ? a0 : 0.f); Qh[k] = (k % 4 == 0 ? a1 : 0.f) - Q[k]; }
-    if (!gersh_min_ge(Ql, -tol * w) || !gersh_min_ge(Qh, -tol * w)) {
-        // Gershgorin is conservative: fall back to Sylvester in FP64 before rejecting
-        double Dl[9], Dh[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            Dl[k] = double(Ql[k]) + (k % 4 == 0 ? double(tol * w) : 0.0);
-            Dh[k] = double(Qh[k]) + (k % 4 == 0 ? double(tol * w) : 0.0);
-        }
-        if (!(Dl[0] > 0.0 && Dl[0] * Dl[4] - Dl[1] * Dl[3] > 0.0 && det<3>(Dl) > 0.0)) return false;
-        if (!(Dh[0] > 0.0 && Dh[0] * Dh[4] - Dh[1] * Dh[3] > 0.0 && det<3>(Dh) > 0.0)) return false;
-    }
+    if (!sym_min_ge(Ql, -2.f * tol) || !sym_min_ge(Qh, -2.f * tol)) return false;
+    if (!gersh_min_ge(Ms, 0.5f)) return false;
     // (M - I)(Q - t0^2)(Q - t1^2) = 0 and the sign conditions
     float GL[9], GH[9], P[9];
     float Qh_neg[9];
@@ -429,8 +436,8 @@ __device__ __forceinline__ bool mlp_residual_ok(const float* Fh, const float* Fe
             GLs[i * 3 + j] = 0.5f * (GL[i * 3 + j] + GL[j * 3 + i]);
             GHs[i * 3 + j] = 0.5f * (GH[i * 3 + j] + GH[j * 3 + i]);
         }
-    const float sg = -tol * (sqrtf(ng) + tol) * w;
-    if (!gersh_min_ge(GLs, sg) || !gersh_min_ge(GHs, sg)) return false;
+    const float sg = -tol * (w + 2.f * sqrtf(ng));
+    if (!sym_min_ge(GLs, sg) || !sym_min_ge(GHs, sg)) return false;
     return true;
 }
 

@@ -1,11 +1,12 @@
 """Train the learned plasticity surrogate on pairs logged by the plain solver.
 
-    python -m mpm_snow_sim2d_b200.mlp_train [--pairs 4000000] [--steps 4000] [--out PATH]
+    python -m mpm_snow_sim2d_b200.mlp_train [--pairs 50000000] [--steps 20000] [--out PATH]
 
 Data: seeded snowball-on-slab impacts (the 3D workload's set-up, 64^3 grid so
-that contact starts at once) with impact speeds drawn from U(1, 8) m/s; every
-step logs the exact return map (F_hat, J_p) -> (F_E', J_p') of each particle
-whose trial F left the elastic band (mpm_pair_log_*). Training: the library's
+that contact starts at once) with impact speeds drawn from U(1, 8) m/s, 1000 steps
+each; every step logs the exact return map (F_hat, J_p) -> (F_E', J_p') of
+each particle whose trial F left the elastic band (mpm_pair_log_*), and a
+uniform subset of each 10-step window is kept. Training: the library's
 own GPU kernels (BF16 tensor-core forward/backward, AdamW). Writes the FP32
 parameters and the feature normalisation to an .npz.
 """
@@ -39,25 +40,29 @@ def impact_scene(speed: float, seed: int, W: int = 64, steps: int = 200):
     return scenes._scene(f"impact_v{speed:.2f}", 3, W, 5e-5, steps, pos, vel, 8, dict(seed=seed))
 
 
-def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 200, per_scene: int = 1_000_000,
-                  verbose: bool = True) -> np.ndarray:
+def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 1000, per_scene: int = 1_000_000,
+                  every: int = 10, verbose: bool = True) -> np.ndarray:
+    """Exact return-map pairs from seeded impacts, spread over each whole run:
+    the log holds every out-of-band particle of `every` steps, and each read
+    keeps a uniform random subset of per_scene / (steps / every) rows."""
     rng = np.random.Generator(np.random.PCG64(seed))
     chunks, total, k = [], 0, 0
+    reads = max(1, steps // every)
     while total < n_pairs:
         speed = float(rng.uniform(1.0, 8.0))
         sc = impact_scene(speed, seed * 1000 + k, W=W, steps=steps)
-        cap = min(per_scene, n_pairs - total)
+        keep = max(1, min(per_scene, n_pairs - total) // reads)
+        log_cap = every * sc.count
+        taken = []
         with Solver.from_scene(sc) as s:
-            s.pair_log_enable(cap)
-            taken = []
-            for _ in range(steps // 10):
-                s.Step(10)
-                got = s.pair_log_read(cap)
+            s.pair_log_enable(log_cap)
+            for _ in range(reads):
+                s.Step(every)
+                got = s.pair_log_read(log_cap)
+                if got.shape[0] > keep:
+                    got = got[rng.choice(got.shape[0], keep, replace=False)]
                 if got.shape[0]:
                     taken.append(got)
-                    cap -= got.shape[0]
-                if cap <= 0:
-                    break
             s.pair_log_enable(0)
         p = np.concatenate(taken) if taken else np.empty((0, 20), np.float32)
         p = p[np.isfinite(p).all(1) & (p[:, 9] > 0) & (p[:, 19] > 0)]
@@ -65,7 +70,8 @@ def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 200, pe
         total += p.shape[0]
         k += 1
         if verbose:
-            print(f"scene {k}: speed {speed:.2f} m/s, {sc.count} particles, {p.shape[0]} pairs (total {total})")
+            print(f"scene {k}: speed {speed:.2f} m/s, {sc.count} particles, {p.shape[0]} pairs (total {total})",
+                  flush=True)
     return np.concatenate(chunks)[:n_pairs]
 
 
@@ -100,8 +106,8 @@ def train(pairs: np.ndarray, steps: int = 4000, batch: int = 8192, lr: float = 2
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--pairs", type=int, default=4_000_000)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--pairs", type=int, default=50_000_000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=7)

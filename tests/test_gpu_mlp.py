@@ -92,3 +92,26 @@ def test_solver_with_learned_return_map(mlp_mod):
     # every accepted prediction passed the residual check at 1e-3; a useful
     # network takes most out-of-band particles off the SVD
     assert acc > rej
+
+
+def test_pretrained_weights_take_particles_off_the_svd(mlp_mod):
+    """The shipped network (mpm_snow_sim2d_b200/data) on an impact it was not
+    trained on: most out-of-band particles skip the SVD, and F stays within
+    1e-3 of the exact return map's run."""
+    from mpm_snow_sim2d_b200 import Solver, _lib
+    from mpm_snow_sim2d_b200 import mlp_train
+    net = mlp_mod.Mlp.load(mlp_mod.DEFAULT_WEIGHTS)
+    sc = mlp_train.impact_scene(6.5, seed=777001, W=48, steps=300)
+    with Solver.from_scene(sc) as plain:
+        t_plain = plain.step_profiled(300)
+        ref = plain.get_state()
+    with Solver.from_scene(sc) as s:
+        s.set_plasticity(_lib.PLASTIC_MLP, net, 1e-3)
+        t_mlp = s.step_profiled(300)
+        got = s.get_state()
+        acc, rej = s.mlp_stats()
+    rel_F = np.linalg.norm(got.elastic_f - ref.elastic_f) / np.linalg.norm(ref.elastic_f)
+    print(f"pretrained: accepted {acc}, fell back {rej}, rel F {rel_F:.2e}, "
+          f"G2P {t_plain['g2p']:.2f} ms -> {t_mlp['g2p']:.2f} ms over 300 steps")
+    assert acc > 4 * rej
+    assert rel_F <= 1e-3
