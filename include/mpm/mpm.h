@@ -197,8 +197,11 @@ MPM_API const char* mpm_status_string(mpm_status status);
 
 /* Per-stage device timing: runs `nsteps` steps like mpm_step with a CUDA
  * event after every stage and adds each stage's device time in milliseconds to
- * stage_ms[s] for s < min(nstages, mpm_stage_count()). Synchronises. The
- * reference has no timers (src/main.cpp:11 includes <chrono> unused). */
+ * stage_ms[s] for s < min(nstages, mpm_stage_count()). Synchronises. Stages:
+ * "sort", "p2g", "grid_update", "g2p" (gather, APIC update and the in-band
+ * return map) and "return_map" (the full return map of the particles whose
+ * trial F left the elastic band, exact or learned). The reference has no
+ * timers (src/main.cpp:11 includes <chrono> unused). */
 MPM_API mpm_status mpm_step_profiled(mpm_solver* solver, int32_t nsteps, double* stage_ms, int32_t nstages);
 MPM_API int32_t mpm_stage_count(const mpm_solver* solver);
 MPM_API const char* mpm_stage_name(const mpm_solver* solver, int32_t stage);

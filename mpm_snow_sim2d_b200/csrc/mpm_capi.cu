@@ -239,23 +239,43 @@ template <int D> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
     return cudaGetLastError();
 }
 
-// G2P of the tiled MLS path: gather + in-band return map, then the queued
-// particles' full return map.
-template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
+// G2P of the tiled MLS path: gather + in-band return map (stage "g2p"), then
+// the queued particles' full return map (stage "return_map").
+template <int D> cudaError_t launch_g2p_gather(mpm_solver* s) {
     if (s->n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
     k_g2p_gather<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
+    return cudaGetLastError();
+}
+
+// The warp-tiled inference kernels use more than the default 48 KB of dynamic
+// shared memory; the opt-in is per device and set outside any stream capture.
+cudaError_t mlp_kernel_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(k_return_map_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(MlpWarpSmem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpWarpSmem));
+}
+
+template <int D> cudaError_t launch_return_map(mpm_solver* s) {
+    if (s->n == 0) return cudaSuccess;
+    PairLog L{s->log_data, s->log_n, s->log_cap};
     if (D == 3 && s->plasticity == MPM_PLASTIC_MLP && s->mlp) {
         MlpParams ML{s->mlp->wbf, s->mlp->w, s->mlp->norm, s->mlp_tol, s->mlp_counters};
-        k_g2p_plastic_mlp<<<s->sms * 4, 128, sizeof(MlpInferSmem), s->stream>>>(particle_view(s), s->C, s->gv, s->q, ML,
-                                                                               s->status);
-    } else {
-        PairLog L{s->log_data, s->log_n, s->log_cap};
-        k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, L, s->status);
+        k_return_map_mlp<<<s->sms * 2, kMlpWarps * 32, sizeof(MlpWarpSmem), s->stream>>>(particle_view(s), s->C, s->q,
+                                                                                       ML);
+        L = PairLog{nullptr, nullptr, 0};
     }
+    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, L, s->status);
     return cudaGetLastError();
+}
+
+template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
+    cudaError_t e = launch_g2p_gather<D>(s);
+    if (e != cudaSuccess) return e;
+    return launch_return_map<D>(s);
 }
 
 template <int D> cudaError_t prepare_affine(mpm_solver* s) {
@@ -512,14 +532,15 @@ uint64_t params_hash(const mpm_params& p) {
 }  // namespace
 
 namespace {
-const char* kStageNames[] = {"sort", "p2g", "grid_update", "g2p"};
-constexpr int kStages = 4;
+const char* kStageNames[] = {"sort", "p2g", "grid_update", "g2p", "return_map"};
+constexpr int kStages = 5;
 
 template <int D, int FORM> cudaError_t stage(mpm_solver* s, int k) {
     if (k == 0) return cudaSuccess;
     if (k == 1) return launch_p2g<D, FORM>(s);
     if (k == 2) return launch_grid<D, FORM>(s);
-    return launch_g2p<D, FORM>(s);
+    if (k == 3) return launch_g2p<D, FORM>(s);
+    return cudaSuccess;  // the untiled G2P includes its return map
 }
 template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
     if (k == 0) {
@@ -534,7 +555,8 @@ template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
         if (e != cudaSuccess) return e;
         return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
     }
-    return launch_g2p_split<D>(s);
+    if (k == 3) return launch_g2p_gather<D>(s);
+    return launch_return_map<D>(s);
 }
 cudaError_t dispatch_stage(mpm_solver* s, int k) {
     if (s->tiled) return s->dim == 2 ? stage_tiled<2>(s, k) : stage_tiled<3>(s, k);
@@ -1189,8 +1211,11 @@ mpm_status mpm_mlp_predict(mpm_mlp* m, const float* inputs, int64_t n, int32_t s
     if (st == MPM_OK && cudaMemcpy(di, inputs, sizeof(float) * n * stride, cudaMemcpyHostToDevice) != cudaSuccess)
         st = MPM_ERR_CUDA;
     if (st == MPM_OK) {
-        k_mlp_forward<<<(unsigned)((n + kMlpTrainRows - 1) / kMlpTrainRows), 128, sizeof(MlpInferSmem)>>>(
-            di, stride, (int)n, m->wbf, m->w, m->norm, dout);
+        const long long rows = kMlpWarps * 32;
+        if (mlp_kernel_attrs() != cudaSuccess) st = MPM_ERR_CUDA;
+        else
+            k_mlp_forward<<<(unsigned)((n + rows - 1) / rows), kMlpWarps * 32, sizeof(MlpWarpSmem)>>>(
+                di, stride, (int)n, m->wbf, m->w, m->norm, dout);
         if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = MPM_ERR_CUDA;
     }
     if (st == MPM_OK && cudaMemcpy(out, dout, sizeof(float) * n * kMlpOut, cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1208,6 +1233,7 @@ mpm_status mpm_set_plasticity(mpm_solver* s, int32_t mode, mpm_mlp* mlp, float t
         if (!mlp) return fail(s, MPM_ERR_INVALID_ARGUMENT, "MLP plasticity needs a network");
         if (s->dim != 3 || !s->tiled) return fail(s, MPM_ERR_UNSUPPORTED, "the learned return map is 3D MLS only");
         if (!(tolerance > 0.f)) return fail(s, MPM_ERR_INVALID_ARGUMENT, "tolerance must be > 0");
+        MPM_CUDA(s, mlp_kernel_attrs());
         if (!s->mlp_counters) {
             MPM_CUDA(s, dalloc(&s->mlp_counters, 2));
             MPM_CUDA(s, cudaMemset(s->mlp_counters, 0, 2 * sizeof(unsigned long long)));

@@ -508,6 +508,10 @@ __global__ void __launch_bounds__(256) k_prepare_affine(Particles P, StepConsts 
 // trial F for k_g2p_plastic, which runs the full return map (FP64 band test,
 // else the SVD) and then writes theirs. The split keeps the SVD's registers out
 // of the gather kernel so that it runs at higher occupancy.
+// Queue entry already finished by the learned return map (never a slot: the
+// clipped-stencil entries are -1 - slot >= -n).
+constexpr int kQueueDone = -2147483647 - 1;
+
 struct SlowQueue {
     int* list;    // slots needing the full return map
     int* count;   // device scalar
@@ -810,7 +814,7 @@ __global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, 
                                                      SlowQueue Q, PairLog L, unsigned* __restrict__ status) {
     const int m = *Q.count;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
-        g2p_queued_exact<D>(P, C, gv, Q, e, status, L);
+        if (Q.list[e] != kQueueDone) g2p_queued_exact<D>(P, C, gv, Q, e, status, L);
 }
 
 // ---------------------------------------------------------------------------

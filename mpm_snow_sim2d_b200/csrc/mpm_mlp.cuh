@@ -64,9 +64,24 @@ __device__ __forceinline__ void mma_tile(float* acc, const __nv_bfloat16* A, int
     mma_bf16(acc, a, b);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016):
+//   gelu(x) = x/2 (1 + tanh(c (x + 0.044715 x^3))),  c = sqrt(2/pi),
+// with the hardware tanh (PTX tanh.approx.f32, relative error ~2^-11, below the
+// bf16 rounding of the stored activations). Training and inference share it.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+    const float th = tanh_hw(kGeluC * x * fmaf(kGeluA, x * x, 1.f));
+    return 0.5f * x * (1.f + th);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
+    const float x2 = x * x;
+    const float th = tanh_hw(kGeluC * x * fmaf(kGeluA, x2, 1.f));
+    return 0.5f * (1.f + th) + 0.5f * x * (1.f - th * th) * kGeluC * fmaf(3.f * kGeluA, x2, 1.f);
 }
 
 // Raw pair -> normalised network input (row of kMlpInPad bf16) and target.
@@ -267,65 +282,6 @@ __global__ void k_mlp_adam(float* __restrict__ w, __nv_bfloat16* __restrict__ wb
     wbf[i] = __float2bfloat16_rn(x);
 }
 
-// ---------------------------------------------------------------------------
-// Inference on a tile of up to 64 particles (4 warps x 16 rows) held in
-// shared memory: in (bf16 [64][16]) -> out (fp32 [64][16], normalised).
-struct MlpInferSmem {
-    __nv_bfloat16 w[MlpOff::total];
-    float b1[kMlpHid], b2[kMlpHid], b3[kMlpHid], b4[kMlpOutPad];
-    __nv_bfloat16 x0[kMlpTrainRows * kMlpInPad];
-    __nv_bfloat16 h[2][kMlpTrainRows * kMlpHid];
-    float out[kMlpTrainRows * kMlpOutPad];
-};
-
-__device__ __forceinline__ void mlp_load_weights(MlpInferSmem& S, const __nv_bfloat16* wbf, const float* wf32) {
-    for (int i = threadIdx.x; i < MlpOff::total; i += blockDim.x) S.w[i] = wbf[i];
-    for (int i = threadIdx.x; i < kMlpHid; i += blockDim.x) {
-        S.b1[i] = wf32[MlpOff::b1 + i];
-        S.b2[i] = wf32[MlpOff::b2 + i];
-        S.b3[i] = wf32[MlpOff::b3 + i];
-    }
-    for (int i = threadIdx.x; i < kMlpOutPad; i += blockDim.x) S.b4[i] = wf32[MlpOff::b4 + i];
-}
-
-__device__ __forceinline__ void mlp_infer_tile(MlpInferSmem& S) {
-    const int m0 = (threadIdx.x >> 5) * 16;
-    mlp_layer_fwd(S.x0, kMlpInPad, kMlpInPad, S.w + MlpOff::W1, S.b1, kMlpHid, m0, nullptr, 0, S.h[0], kMlpHid, true);
-    __syncwarp();
-    mlp_layer_fwd(S.h[0], kMlpHid, kMlpHid, S.w + MlpOff::W2, S.b2, kMlpHid, m0, nullptr, 0, S.h[1], kMlpHid, true);
-    __syncwarp();
-    mlp_layer_fwd(S.h[1], kMlpHid, kMlpHid, S.w + MlpOff::W3, S.b3, kMlpHid, m0, nullptr, 0, S.h[0], kMlpHid, true);
-    __syncwarp();
-    mlp_layer_fwd(S.h[0], kMlpHid, kMlpHid, S.w + MlpOff::W4, S.b4, kMlpOutPad, m0, S.out, kMlpOutPad, nullptr, 0,
-                  false);
-    __syncwarp();
-}
-
-// Batched inference on raw pairs' inputs (testing / evaluation): out[n][10]
-// = denormalised (F_E' - F_hat, log J_p' - log J_p).
-__global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ inputs, int stride, int n,
-                                                     const __nv_bfloat16* __restrict__ wbf,
-                                                     const float* __restrict__ wf32, MlpNorm N,
-                                                     float* __restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    MlpInferSmem& S = *reinterpret_cast<MlpInferSmem*>(smem_raw);
-    mlp_load_weights(S, wbf, wf32);
-    const int row0 = blockIdx.x * kMlpTrainRows;
-    for (int r = threadIdx.x; r < kMlpTrainRows; r += blockDim.x) {
-        float in[kMlpIn];
-        const bool valid = row0 + r < n;
-        if (valid) mlp_features(inputs + (long long)(row0 + r) * stride, inputs[(long long)(row0 + r) * stride + 9], N, in);
-        for (int k = 0; k < kMlpInPad; ++k) S.x0[r * kMlpInPad + k] = __float2bfloat16_rn(valid && k < kMlpIn ? in[k] : 0.f);
-    }
-    __syncthreads();
-    mlp_infer_tile(S);
-    __syncthreads();
-    for (int e = threadIdx.x; e < kMlpTrainRows * kMlpOut; e += blockDim.x) {
-        const int r = e / kMlpOut, c = e % kMlpOut;
-        if (row0 + r < n) out[(long long)(row0 + r) * kMlpOut + c] = S.out[r * kMlpOutPad + c] * N.out_std[c] + N.out_mean[c];
-    }
-}
-
 }  // namespace mpm
 
 namespace mpm {
@@ -449,76 +405,231 @@ struct MlpParams {
     unsigned long long* counters;  // [0] accepted, [1] rejected (fell back to the SVD)
 };
 
-// Queued particles of the tiled MLS path with the learned return map: out-of-
-// band trial F goes through the network (64 per tile on the tensor cores) and
-// the residual check; failures and grid-clipped stencils take the exact path.
-__global__ void __launch_bounds__(128) k_g2p_plastic_mlp(Particles P, StepConsts C, const float4* __restrict__ gv,
-                                                         SlowQueue Q, MlpParams ML, unsigned* __restrict__ status) {
+// ---------------------------------------------------------------------------
+// Warp-tiled inference for the solver. Each warp takes 32 queued particles
+// (lane = particle) and runs the network on them as two 16-row tiles whose
+// activations never leave registers: the m16n8 accumulators of one layer,
+// after bias + GELU, are packed to bf16 pairs that are exactly the m16k16 A
+// fragments of the next layer (accumulator n-tiles 2kb, 2kb+1 = A k-block kb).
+// Weights sit in shared memory with rows padded by 8 bf16 so that the B
+// fragment loads of a warp hit 32 distinct banks.
+constexpr int kMwIn = kMlpInPad + 8;  // row stride (bf16) of W1 and of the input tile
+constexpr int kMwHid = kMlpHid + 8;   // row stride (bf16) of W2, W3, W4
+constexpr int kMwOut = kMlpOutPad + 2;  // row stride (fp32) of the output tile
+constexpr int kMlpWarps = 8;
+
+struct MlpWarpSmem {
+    __nv_bfloat16 W1[kMlpHid * kMwIn];
+    __nv_bfloat16 W2[kMlpHid * kMwHid];
+    __nv_bfloat16 W3[kMlpHid * kMwHid];
+    __nv_bfloat16 W4[kMlpOutPad * kMwHid];
+    float b1[kMlpHid], b2[kMlpHid], b3[kMlpHid], b4[kMlpOutPad];
+    __nv_bfloat16 x[kMlpWarps][32 * kMwIn];
+    float out[kMlpWarps][32 * kMwOut];
+};
+
+__device__ __forceinline__ void mlp_stage_matrix(__nv_bfloat16* dst, int ld_dst, const __nv_bfloat16* src, int rows,
+                                                 int cols) {
+    const int vpr = cols / 8;  // 16-byte vectors per row
+    for (int v = threadIdx.x; v < rows * vpr; v += blockDim.x) {
+        const int r = v / vpr, c = (v % vpr) * 8;
+        *reinterpret_cast<uint4*>(dst + r * ld_dst + c) = *reinterpret_cast<const uint4*>(src + r * cols + c);
+    }
+}
+
+__device__ __forceinline__ void mlp_stage_weights(MlpWarpSmem& S, const __nv_bfloat16* wbf, const float* wf32) {
+    mlp_stage_matrix(S.W1, kMwIn, wbf + MlpOff::W1, kMlpHid, kMlpInPad);
+    mlp_stage_matrix(S.W2, kMwHid, wbf + MlpOff::W2, kMlpHid, kMlpHid);
+    mlp_stage_matrix(S.W3, kMwHid, wbf + MlpOff::W3, kMlpHid, kMlpHid);
+    mlp_stage_matrix(S.W4, kMwHid, wbf + MlpOff::W4, kMlpOutPad, kMlpHid);
+    for (int i = threadIdx.x; i < kMlpHid; i += blockDim.x) {
+        S.b1[i] = wf32[MlpOff::b1 + i];
+        S.b2[i] = wf32[MlpOff::b2 + i];
+        S.b3[i] = wf32[MlpOff::b3 + i];
+    }
+    for (int i = threadIdx.x; i < kMlpOutPad; i += blockDim.x) S.b4[i] = wf32[MlpOff::b4 + i];
+}
+
+__device__ __forceinline__ uint32_t pack_f2_bf16(float lo, float hi) {
+    return pack_bf16(__float2bfloat16_rn(lo), __float2bfloat16_rn(hi));
+}
+
+// acc[j] (n-tile j of a 16 x 8*NT output) = A (16 x 16*KB, fragments a[kb]) * W^T,
+// W row-major [out][in] in shared memory with row stride ld.
+template <int KB, int NT>
+__device__ __forceinline__ void mlp_warp_layer(const uint32_t (*a)[4], const __nv_bfloat16* W, int ld, float (*acc)[4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+        const __nv_bfloat16* w = W + (j * 8 + g) * ld + 2 * t;
+#pragma unroll
+        for (int kb = 0; kb < KB; ++kb) {
+            uint32_t b[2];
+            b[0] = *reinterpret_cast<const uint32_t*>(w + kb * 16);
+            b[1] = *reinterpret_cast<const uint32_t*>(w + kb * 16 + 8);
+            mma_bf16(acc[j], a[kb], b);
+        }
+    }
+}
+
+// bias + GELU on a 16 x 64 accumulator, packed into the A fragments of the next layer.
+__device__ __forceinline__ void mlp_warp_activate(float (*acc)[4], const float* bias, uint32_t (*a)[4]) {
+    const int t = threadIdx.x & 3;
+#pragma unroll
+    for (int kb = 0; kb < kMlpHid / 16; ++kb)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = 2 * kb + h, c = j * 8 + 2 * t;
+            const float b0 = bias[c], b1 = bias[c + 1];
+            a[kb][2 * h] = pack_f2_bf16(gelu(acc[j][0] + b0), gelu(acc[j][1] + b1));
+            a[kb][2 * h + 1] = pack_f2_bf16(gelu(acc[j][2] + b0), gelu(acc[j][3] + b1));
+        }
+}
+
+// Network on the warp's 32-row input tile X (bf16, row stride kMwIn) -> O
+// (fp32, normalised outputs, row stride kMwOut).
+__device__ __forceinline__ void mlp_warp_forward(const MlpWarpSmem& S, const __nv_bfloat16* X, float* O) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt) {
+        const int r0 = mt * 16 + g;
+        uint32_t a[kMlpHid / 16][4];
+        a[0][0] = *reinterpret_cast<const uint32_t*>(X + r0 * kMwIn + 2 * t);
+        a[0][1] = *reinterpret_cast<const uint32_t*>(X + (r0 + 8) * kMwIn + 2 * t);
+        a[0][2] = *reinterpret_cast<const uint32_t*>(X + r0 * kMwIn + 2 * t + 8);
+        a[0][3] = *reinterpret_cast<const uint32_t*>(X + (r0 + 8) * kMwIn + 2 * t + 8);
+        float acc[kMlpHid / 8][4];
+        mlp_warp_layer<1, kMlpHid / 8>(a, S.W1, kMwIn, acc);
+        mlp_warp_activate(acc, S.b1, a);
+        mlp_warp_layer<kMlpHid / 16, kMlpHid / 8>(a, S.W2, kMwHid, acc);
+        mlp_warp_activate(acc, S.b2, a);
+        mlp_warp_layer<kMlpHid / 16, kMlpHid / 8>(a, S.W3, kMwHid, acc);
+        mlp_warp_activate(acc, S.b3, a);
+        float o[kMlpOutPad / 8][4];
+        mlp_warp_layer<kMlpHid / 16, kMlpOutPad / 8>(a, S.W4, kMwHid, o);
+#pragma unroll
+        for (int j = 0; j < kMlpOutPad / 8; ++j) {
+            const int c = j * 8 + 2 * t;
+            *reinterpret_cast<float2*>(O + r0 * kMwOut + c) = make_float2(o[j][0] + S.b4[c], o[j][1] + S.b4[c + 1]);
+            *reinterpret_cast<float2*>(O + (r0 + 8) * kMwOut + c) =
+                make_float2(o[j][2] + S.b4[c], o[j][3] + S.b4[c + 1]);
+        }
+    }
+}
+
+// Learned return map of the queued particles (3D tiled MLS path). Accepted
+// predictions write F_E', J_p' and the next step's affine matrix and mark
+// their queue entry kQueueDone; the rest (rejected by the residual check or
+// by the stress series, and grid-clipped stencils) stay queued for
+// k_g2p_plastic's exact return map, which runs next.
+__global__ void __launch_bounds__(kMlpWarps * 32) k_return_map_mlp(Particles P, StepConsts C, SlowQueue Q,
+                                                                   MlpParams ML) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MlpInferSmem& S = *reinterpret_cast<MlpInferSmem*>(smem_raw);
-    mlp_load_weights(S, ML.wbf, ML.wf32);
+    MlpWarpSmem& S = *reinterpret_cast<MlpWarpSmem*>(smem_raw);
+    mlp_stage_weights(S, ML.wbf, ML.wf32);
+    __syncthreads();
     const int m = *Q.count;
     const int n = P.n;
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __nv_bfloat16* X = S.x[wid];
+    float* O = S.out[wid];
     const float t0 = 1.f - C.theta_c, t1 = 1.f + C.theta_s;
-    unsigned long long acc_ok = 0, acc_bad = 0;
-    for (int base = blockIdx.x * kMlpTrainRows; base < m; base += gridDim.x * kMlpTrainRows) {
-        __syncthreads();
-        if (tid < kMlpTrainRows) {
-            const int e = base + tid;
-            float in[kMlpIn];
-            bool valid = e < m && Q.list[e] >= 0;
-            if (valid) {
-                float Fh[9];
+    unsigned n_ok = 0, n_bad = 0;
+    const int warps = gridDim.x * kMlpWarps;
+    for (int base = (blockIdx.x * kMlpWarps + wid) * 32; base < m; base += warps * 32) {
+        const int e = base + lane;
+        const int entry = e < m ? Q.list[e] : -1;
+        const bool valid = entry >= 0;
+        float Fh[9], Jp0 = 1.f;
+        float in[kMlpIn];
+        if (valid) {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) Fh[k] = Q.fh[k * Q.capacity + e];
-                mlp_features(Fh, P.Jp[Q.list[e]], ML.norm, in);
-            }
-#pragma unroll
-            for (int k = 0; k < kMlpInPad; ++k)
-                S.x0[tid * kMlpInPad + k] = __float2bfloat16_rn(valid && k < kMlpIn ? in[k] : 0.f);
+            for (int k = 0; k < 9; ++k) Fh[k] = Q.fh[k * Q.capacity + e];
+            Jp0 = P.Jp[entry];
+            mlp_features(Fh, Jp0, ML.norm, in);
         }
-        __syncthreads();
-        mlp_infer_tile(S);
-        __syncthreads();
-        if (tid < kMlpTrainRows && base + tid < m) {
-            const int e = base + tid;
-            const int entry = Q.list[e];
-            const int i = entry >= 0 ? entry : -1 - entry;
-            float Fh[9], Fe[9], B[9], A[9];
-            bool done = false;
-            if (entry >= 0) {
+        uint32_t* xr = reinterpret_cast<uint32_t*>(X + lane * kMwIn);
 #pragma unroll
-                for (int k = 0; k < 9; ++k) { Fh[k] = Q.fh[k * Q.capacity + e]; B[k] = P.B[k * n + i]; }
-                float Fp[9];
+        for (int k = 0; k < kMlpInPad / 2; ++k) {
+            const float lo = valid && 2 * k < kMlpIn ? in[2 * k] : 0.f;
+            const float hi = valid && 2 * k + 1 < kMlpIn ? in[2 * k + 1] : 0.f;
+            xr[k] = pack_f2_bf16(lo, hi);
+        }
+        __syncwarp();
+        if (__any_sync(0xffffffffu, valid)) mlp_warp_forward(S, X, O);
+        __syncwarp();
+        if (valid) {
+            const float* o = O + lane * kMwOut;
+            float Fp[9];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) Fp[k] = Fh[k] + (S.out[tid * kMlpOutPad + k] * ML.norm.out_std[k] + ML.norm.out_mean[k]);
-                const float dlj = S.out[tid * kMlpOutPad + 9] * ML.norm.out_std[9] + ML.norm.out_mean[9];
-                if (mlp_residual_ok(Fh, Fp, t0, t1, ML.tol)) {
-                    // J_p' = J_p det(F_hat) / det(F_E') (= J_p prod(S_hat / S)); the network's
-                    // log J_p' output must agree with it within the tolerance.
-                    const float ratio = det<3>(Fh) / det<3>(Fp);
-                    if (fabsf(logf(ratio) - dlj) <= ML.tol * (1.f + fabsf(dlj))) {
-                        float Jp = P.Jp[i] * ratio;
+            for (int k = 0; k < 9; ++k) Fp[k] = Fh[k] + (o[k] * ML.norm.out_std[k] + ML.norm.out_mean[k]);
+            const float dlj = o[9] * ML.norm.out_std[9] + ML.norm.out_mean[9];
+            bool ok = mlp_residual_ok(Fh, Fp, t0, t1, ML.tol);
+            float ratio = 1.f;
+            if (ok) {
+                // J_p' = J_p det(F_hat) / det(F_E') (= J_p prod(S_hat / S)); the
+                // network's log J_p' output must agree with it within the tolerance.
+                ratio = det<3>(Fh) / det<3>(Fp);
+                ok = fabsf(logf(ratio) - dlj) <= ML.tol * (1.f + fabsf(dlj));
+            }
+            float sig[9];
+            const float Jp = Jp0 * ratio;
+            if (ok) ok = hardened_stress_series<3>(Fp, Jp, C.mu0, C.la0, C.xi, sig);
+            if (ok) {
+                const float mass = P.mass ? P.mass[entry] : P.mass_u, vol = P.vol ? P.vol[entry] : P.vol_u;
 #pragma unroll
-                        for (int k = 0; k < 9; ++k) { P.Fe[k * n + i] = Fp[k]; Fe[k] = Fp[k]; }
-                        P.Jp[i] = Jp;
-                        mls_affine<3>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) P.A[k * n + i] = A[k];
-                        done = true;
-                        ++acc_ok;
-                    }
+                for (int k = 0; k < 9; ++k) {
+                    P.Fe[k * n + entry] = Fp[k];
+                    P.A[k * n + entry] = 3.f * mass * P.B[k * n + entry] - 3.f * C.dt * vol * sig[k];
                 }
-                if (!done) ++acc_bad;
+                P.Jp[entry] = Jp;
+                Q.list[e] = kQueueDone;
+                ++n_ok;
+            } else {
+                ++n_bad;
             }
-            if (!done) g2p_queued_exact<3>(P, C, gv, Q, e, status);
         }
+        __syncwarp();
     }
     if (ML.counters) {
-        if (acc_ok) atomicAdd(&ML.counters[0], acc_ok);
-        if (acc_bad) atomicAdd(&ML.counters[1], acc_bad);
+        n_ok = __reduce_add_sync(0xffffffffu, n_ok);
+        n_bad = __reduce_add_sync(0xffffffffu, n_bad);
+        if (lane == 0) {
+            if (n_ok) atomicAdd(&ML.counters[0], (unsigned long long)n_ok);
+            if (n_bad) atomicAdd(&ML.counters[1], (unsigned long long)n_bad);
+        }
     }
+}
+
+// Batched inference on raw pairs' inputs (evaluation and tests), through the
+// same warp-tiled path as the solver: out[n][10] = denormalised
+// (F_E' - F_hat, log J_p' - log J_p). Rows: input + stride * i, F_hat[9], J_p.
+__global__ void __launch_bounds__(kMlpWarps * 32) k_mlp_forward(const float* __restrict__ inputs, int stride, int n,
+                                                                const __nv_bfloat16* __restrict__ wbf,
+                                                                const float* __restrict__ wf32, MlpNorm N,
+                                                                float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpWarpSmem& S = *reinterpret_cast<MlpWarpSmem*>(smem_raw);
+    mlp_stage_weights(S, wbf, wf32);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __nv_bfloat16* X = S.x[wid];
+    float* O = S.out[wid];
+    const int row = (blockIdx.x * kMlpWarps + wid) * 32 + lane;
+    const bool valid = row < n;
+    float in[kMlpIn];
+    if (valid) mlp_features(inputs + (long long)row * stride, inputs[(long long)row * stride + 9], N, in);
+    uint32_t* xr = reinterpret_cast<uint32_t*>(X + lane * kMwIn);
+#pragma unroll
+    for (int k = 0; k < kMlpInPad / 2; ++k)
+        xr[k] = pack_f2_bf16(valid && 2 * k < kMlpIn ? in[2 * k] : 0.f, valid && 2 * k + 1 < kMlpIn ? in[2 * k + 1] : 0.f);
+    __syncwarp();
+    mlp_warp_forward(S, X, O);
+    __syncwarp();
+    if (valid)
+#pragma unroll
+        for (int c = 0; c < kMlpOut; ++c) out[(long long)row * kMlpOut + c] = O[lane * kMwOut + c] * N.out_std[c] + N.out_mean[c];
 }
 
 }  // namespace mpm

@@ -2,12 +2,12 @@
 
 Only tests/ use this module. It restates the network of
 mpm_snow_sim2d_b200/csrc/mpm_mlp.cuh in numpy (FP64 arithmetic):
-10 -> 64 -> 64 -> 64 -> 10, GELU (erf form), mean over samples of the summed
+10 -> 64 -> 64 -> 64 -> 10, GELU (tanh form), mean over samples of the summed
 squared error on the normalised outputs, and its exact gradient by backprop.
 With ``bf16=True`` values are rounded to bfloat16 (round to nearest even) at
 the points where the GPU kernels store bfloat16: network inputs, weights,
 hidden activations and the back-propagated pre-activation gradients; the
-gradient check then isolates accumulation order and the erf evaluation.
+gradient check then isolates accumulation order and the hardware tanh.
 """
 from __future__ import annotations
 
@@ -17,9 +17,6 @@ import numpy as np
 
 from mpm_snow_sim2d_b200.mlp import HID, OFF, features, targets
 
-_erf = np.vectorize(math.erf)
-
-
 def bf16(a: np.ndarray) -> np.ndarray:
     """Round float values to bfloat16 (nearest even), returned as float64."""
     f = np.ascontiguousarray(a, np.float32)
@@ -28,12 +25,18 @@ def bf16(a: np.ndarray) -> np.ndarray:
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+_C = math.sqrt(2.0 / math.pi)
+_A = 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (the kernels' activation)."""
+    return 0.5 * x * (1.0 + np.tanh(_C * (x + _A * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    th = np.tanh(_C * (x + _A * x ** 3))
+    return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * _C * (1.0 + 3.0 * _A * x * x)
 
 
 def unpack(params: np.ndarray):

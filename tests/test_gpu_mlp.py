@@ -112,6 +112,8 @@ def test_pretrained_weights_take_particles_off_the_svd(mlp_mod):
         acc, rej = s.mlp_stats()
     rel_F = np.linalg.norm(got.elastic_f - ref.elastic_f) / np.linalg.norm(ref.elastic_f)
     print(f"pretrained: accepted {acc}, fell back {rej}, rel F {rel_F:.2e}, "
-          f"G2P {t_plain['g2p']:.2f} ms -> {t_mlp['g2p']:.2f} ms over 300 steps")
+          f"return map {t_plain['return_map']:.2f} ms -> {t_mlp['return_map']:.2f} ms, "
+          f"G2P {t_plain['g2p'] + t_plain['return_map']:.2f} ms -> {t_mlp['g2p'] + t_mlp['return_map']:.2f} ms "
+          f"over 300 steps")
     assert acc > 4 * rej
     assert rel_F <= 1e-3
