@@ -156,28 +156,49 @@ def rel_l2(a, b):
 def mlp_vs_plain(args, torch, stream):
     """The learned return map against the exact one on the same seeded inputs:
     per-stage device time over the whole run (G2P = gather + return map), and
-    the relative L2 error of x, v, F_E after it."""
+    the relative L2 error of x, v, F_E, J_p at several horizons. A control run
+    of the exact solver from initial velocities perturbed by 1e-6 (relative)
+    shows how much any per-step difference of that size grows in this scene."""
     from mpm_snow_sim2d_b200 import Solver, _lib
     from mpm_snow_sim2d_b200.mlp import DEFAULT_WEIGHTS, Mlp
     scene = make_scene(args.mlp_workload)
     net = Mlp.load(DEFAULT_WEIGHTS)
-    res, states = {}, {}
-    for mode in ("exact", "mlp"):
+    rng = np.random.Generator(np.random.PCG64(99))
+    solvers = {}
+    for mode in ("exact", "mlp", "control"):
         s = Solver.from_scene(scene)
         s.set_stream(stream.cuda_stream)
         if mode == "mlp":
             s.set_plasticity(_lib.PLASTIC_MLP, net, args.mlp_tolerance)
-        stages = s.step_profiled(args.mlp_steps)
-        torch.cuda.synchronize()
-        states[mode] = s.get_state()
-        r = {"stages_ms": {k: v / args.mlp_steps for k, v in stages.items()},
-             "ms_per_step": sum(stages.values()) / args.mlp_steps, "status_flags": s.status()}
+        if mode == "control":
+            v0 = s.get_state().velocity
+            s.set_state(velocity=v0 * (1.0 + 1e-6 * rng.standard_normal(v0.shape)).astype(np.float32))
+        solvers[mode] = s
+    stages = {m: {} for m in solvers}
+    horizons, done, errs = sorted({h for h in (10, 100, 300, args.mlp_steps) if h <= args.mlp_steps}), 0, {}
+    for h in horizons:
+        st = {}
+        for mode, s in solvers.items():
+            for k, v in s.step_profiled(h - done).items():
+                stages[mode][k] = stages[mode].get(k, 0.0) + v
+            st[mode] = s.get_state()
+        done = h
+        errs[h] = {}
+        for name, other in (("mlp", "mlp"), ("control", "control")):
+            a, b = st[other], st["exact"]
+            errs[h][name] = {"F_E": rel_l2(a.elastic_f, b.elastic_f), "x": rel_l2(a.position, b.position),
+                             "v": rel_l2(a.velocity, b.velocity), "J_p": rel_l2(a.plastic_det, b.plastic_det)}
+    res = {}
+    for mode in ("exact", "mlp"):
+        s = solvers[mode]
+        r = {"stages_ms": {k: v / args.mlp_steps for k, v in stages[mode].items()},
+             "ms_per_step": sum(stages[mode].values()) / args.mlp_steps, "status_flags": s.status()}
         if mode == "mlp":
             acc, rej = s.mlp_stats()
             r.update(accepted=acc, fell_back=rej, accepted_frac=acc / max(acc + rej, 1))
-        s.close()
         res[mode] = r
-    a, b = states["mlp"], states["exact"]
+    for s in solvers.values():
+        s.close()
     g2p = lambda r: r["stages_ms"]["g2p"] + r["stages_ms"]["return_map"]
     return {
         "workload": f"{args.mlp_workload}: {WORKLOADS[args.mlp_workload]}", "particles": scene.count,
@@ -185,8 +206,8 @@ def mlp_vs_plain(args, torch, stream):
         "g2p_speedup": g2p(res["exact"]) / g2p(res["mlp"]),
         "return_map_speedup": res["exact"]["stages_ms"]["return_map"] / res["mlp"]["stages_ms"]["return_map"],
         "step_speedup": res["exact"]["ms_per_step"] / res["mlp"]["ms_per_step"],
-        "rel_l2_vs_plain": {"F_E": rel_l2(a.elastic_f, b.elastic_f), "x": rel_l2(a.position, b.position),
-                            "v": rel_l2(a.velocity, b.velocity), "J_p": rel_l2(a.plastic_det, b.plastic_det)},
+        "rel_l2_vs_plain": {str(h): e["mlp"] for h, e in errs.items()},
+        "control_rel_l2_vs_plain": {str(h): e["control"] for h, e in errs.items()},
         "timing": "CUDA events between stages every step (no graph replay), whole run",
     }
 

@@ -88,8 +88,8 @@ __device__ __forceinline__ float gelu_grad(float x) {
 // Pair layout (20 floats): F_hat[9] J_p[1] F_E'[9] J_p'[1].
 __device__ __forceinline__ void mlp_features(const float* Fh, float Jp, const MlpNorm& N, float* in) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) in[k] = ((Fh[k] - (k % 4 == 0 ? 1.f : 0.f)) - N.in_mean[k]) / N.in_std[k];
-    in[9] = (logf(Jp) - N.in_mean[9]) / N.in_std[9];
+    for (int k = 0; k < 9; ++k) in[k] = ((Fh[k] - (k % 4 == 0 ? 1.f : 0.f)) - N.in_mean[k]) * (1.f / N.in_std[k]);
+    in[9] = (logf(Jp) - N.in_mean[9]) * (1.f / N.in_std[9]);
 }
 __device__ __forceinline__ void mlp_targets(const float* pair, const MlpNorm& N, float* tg) {
 #pragma unroll
@@ -329,15 +329,16 @@ __device__ __forceinline__ bool mlp_residual_ok(const float* Fh, const float* Fe
     const float dE = det<3>(Fe);
     if (!(dE > 0.f) || !(det<3>(Fh) > 0.f)) return false;
     float inv[9];
-    inv[0] = (Fe[4] * Fe[8] - Fe[5] * Fe[7]) / dE;
-    inv[1] = (Fe[2] * Fe[7] - Fe[1] * Fe[8]) / dE;
-    inv[2] = (Fe[1] * Fe[5] - Fe[2] * Fe[4]) / dE;
-    inv[3] = (Fe[5] * Fe[6] - Fe[3] * Fe[8]) / dE;
-    inv[4] = (Fe[0] * Fe[8] - Fe[2] * Fe[6]) / dE;
-    inv[5] = (Fe[2] * Fe[3] - Fe[0] * Fe[5]) / dE;
-    inv[6] = (Fe[3] * Fe[7] - Fe[4] * Fe[6]) / dE;
-    inv[7] = (Fe[1] * Fe[6] - Fe[0] * Fe[7]) / dE;
-    inv[8] = (Fe[0] * Fe[4] - Fe[1] * Fe[3]) / dE;
+    const float r = 1.f / dE;
+    inv[0] = (Fe[4] * Fe[8] - Fe[5] * Fe[7]) * r;
+    inv[1] = (Fe[2] * Fe[7] - Fe[1] * Fe[8]) * r;
+    inv[2] = (Fe[1] * Fe[5] - Fe[2] * Fe[4]) * r;
+    inv[3] = (Fe[5] * Fe[6] - Fe[3] * Fe[8]) * r;
+    inv[4] = (Fe[0] * Fe[8] - Fe[2] * Fe[6]) * r;
+    inv[5] = (Fe[2] * Fe[3] - Fe[0] * Fe[5]) * r;
+    inv[6] = (Fe[3] * Fe[7] - Fe[4] * Fe[6]) * r;
+    inv[7] = (Fe[1] * Fe[6] - Fe[0] * Fe[7]) * r;
+    inv[8] = (Fe[0] * Fe[4] - Fe[1] * Fe[3]) * r;
     float M[9], Q[9];
     matmul<3>(Fh, inv, M);
 #pragma unroll

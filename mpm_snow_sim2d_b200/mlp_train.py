@@ -1,6 +1,6 @@
 """Train the learned plasticity surrogate on pairs logged by the plain solver.
 
-    python -m mpm_snow_sim2d_b200.mlp_train [--pairs 50000000] [--steps 20000] [--out PATH]
+    python -m mpm_snow_sim2d_b200.mlp_train [--pairs 50000000] [--steps 60000] [--batch 16384] [--lr 4e-3] [--out PATH]
 
 Data: seeded snowball-on-slab impacts (the 3D workload's set-up, 64^3 grid so
 that contact starts at once) with impact speeds drawn from U(1, 8) m/s, 1000 steps
@@ -107,9 +107,9 @@ def train(pairs: np.ndarray, steps: int = 4000, batch: int = 8192, lr: float = 2
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--pairs", type=int, default=50_000_000)
-    ap.add_argument("--steps", type=int, default=20000)
-    ap.add_argument("--batch", type=int, default=8192)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--steps", type=int, default=60000)
+    ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
     args = ap.parse_args(argv)
