@@ -242,6 +242,25 @@ MPM_API mpm_status mpm_mlp_gradient(mpm_mlp* mlp, const float* pairs, int64_t n,
 /* Denormalised outputs for rows whose first 10 floats are F_hat[9], J_p. */
 MPM_API mpm_status mpm_mlp_predict(mpm_mlp* mlp, const float* inputs, int64_t n, int32_t stride, float* out);
 
+/* mpm_mlp_predict without any device allocation (no counterpart in the
+ * reference). Some callers cannot allocate device memory at the moment they
+ * need an inference: a host process whose caching allocator has already
+ * reserved the device's memory, or a loop with kernels in flight on other
+ * streams, where cudaMalloc / cudaFree would fail or stall the whole device.
+ * This entry point stages rows and results in a fixed scratch array that is
+ * part of the library's device image (MPM_MLP_NOALLOC_MAX_ROWS rows, 5.2 MB
+ * per device), so it allocates nothing. n above that limit returns
+ * MPM_ERR_CAPACITY; split larger batches. The first call on a device does a
+ * one-time set-up (looks up the scratch address and opts the kernel into its
+ * shared memory); make that first call before any stream capture begins on
+ * the device. Nothing in the scratch has to start at zero: every element a
+ * call reads was written earlier in the same call. Calls share the scratch of
+ * their device, so two calls that overlap in time on the same device (from
+ * two host threads) race: serialise them. Synchronous; the network's device
+ * must be current. */
+#define MPM_MLP_NOALLOC_MAX_ROWS 65536
+MPM_API mpm_status mpm_mlp_predict_noalloc(mpm_mlp* mlp, const float* inputs, int64_t n, int32_t stride, float* out);
+
 /* Return map of a solver: MPM_PLASTIC_EXACT, or MPM_PLASTIC_MLP with `mlp`
  * (3D MLS) and the residual-check tolerance (1e-3). The network must outlive
  * its use by the solver. */

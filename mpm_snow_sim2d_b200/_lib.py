@@ -95,6 +95,7 @@ SIGNATURES = {
     "mpm_mlp_train": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(C.c_float)]),
     "mpm_mlp_gradient": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "mpm_mlp_predict": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.c_int32, C.POINTER(C.c_float)]),
+    "mpm_mlp_predict_noalloc": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.c_int32, C.POINTER(C.c_float)]),
     "mpm_set_plasticity": (C.c_int, [_P, C.c_int32, _P, C.c_float]),
     "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),

@@ -6,6 +6,7 @@
 #include <random>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1286,6 +1287,63 @@ mpm_status mpm_pair_log_read(mpm_solver* s, float* out, int64_t cap_pairs, int64
         MPM_CUDA(s, cudaMemcpy(out, s->log_data, sizeof(float) * 20 * (size_t)take, cudaMemcpyDeviceToHost));
     if (s->log_n) MPM_CUDA(s, cudaMemset(s->log_n, 0, sizeof(unsigned long long)));
     *n_pairs = take;
+    return MPM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Inference without allocation: fixed scratch in the device image.
+namespace {
+constexpr int kNoallocRows = MPM_MLP_NOALLOC_MAX_ROWS;
+// [rows][kMlpIn] staged inputs, then [rows][kMlpOut] outputs.
+__device__ __align__(256) float g_noalloc_scratch[(size_t)kNoallocRows * (kMlpIn + kMlpOut)];
+constexpr int kNoallocMaxDevices = 64;
+float* g_noalloc_ptr[kNoallocMaxDevices];
+cudaError_t g_noalloc_setup[kNoallocMaxDevices];
+std::once_flag g_noalloc_once[kNoallocMaxDevices];
+}  // namespace
+
+extern "C" {
+
+mpm_status mpm_mlp_predict_noalloc(mpm_mlp* m, const float* inputs, int64_t n, int32_t stride, float* out) {
+    if (!m || !inputs || !out || n < 1 || stride < kMlpIn) return MPM_ERR_INVALID_ARGUMENT;
+    if (n > kNoallocRows) {
+        m->err = "mpm_mlp_predict_noalloc: n = " + std::to_string(n) + " exceeds the scratch capacity of " +
+                 std::to_string(kNoallocRows) + " rows";
+        return MPM_ERR_CAPACITY;
+    }
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+        cudaGetLastError();
+        m->err = "mpm_mlp_predict_noalloc: no usable current device";
+        return MPM_ERR_CUDA;
+    }
+    std::call_once(g_noalloc_once[dev], [dev] {
+        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&g_noalloc_ptr[dev]), g_noalloc_scratch);
+        if (e == cudaSuccess) e = mlp_kernel_attrs();
+        g_noalloc_setup[dev] = e;
+    });
+    if (g_noalloc_setup[dev] != cudaSuccess) {
+        m->err = std::string("mpm_mlp_predict_noalloc: scratch set-up failed: ") + cudaGetErrorString(g_noalloc_setup[dev]);
+        return MPM_ERR_CUDA;
+    }
+    float* din = g_noalloc_ptr[dev];
+    float* dout = din + (size_t)kNoallocRows * kMlpIn;
+    cudaError_t e = cudaMemcpy2D(din, sizeof(float) * kMlpIn, inputs, sizeof(float) * (size_t)stride,
+                                 sizeof(float) * kMlpIn, (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const int64_t rows = kMlpWarps * 32;
+        k_mlp_forward<<<(unsigned)((n + rows - 1) / rows), kMlpWarps * 32, sizeof(MlpWarpSmem)>>>(
+            din, kMlpIn, (int)n, m->wbf, m->w, m->norm, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(float) * kMlpOut * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        m->err = std::string("mpm_mlp_predict_noalloc: ") + cudaGetErrorString(e);
+        return MPM_ERR_CUDA;
+    }
     return MPM_OK;
 }
 
