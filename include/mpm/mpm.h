@@ -273,6 +273,52 @@ MPM_API mpm_status mpm_get_mlp_stats(mpm_solver* solver, uint64_t* accepted, uin
 MPM_API mpm_status mpm_pair_log_enable(mpm_solver* solver, int64_t capacity);
 MPM_API mpm_status mpm_pair_log_read(mpm_solver* solver, float* out, int64_t cap_pairs, int64_t* n_pairs);
 
+/* ---- Batched scenes (2D MLS) -------------------------------------------
+ * Many independent scenes, each a full solver in the sense of mpm_create
+ * (the reference constructs one Solver per process, src/main.cpp:164-174),
+ * stepped together: every scene's grid lives in the shared memory of a
+ * cluster of 1-8 CTAs, and one persistent launch per cluster size runs all
+ * scenes from a work queue. Scenes: dim 2, MLS, at most 8 x 9,600 grid nodes
+ * ((W+1)(H+1) <= ~76,000, e.g. 257 x 257 cells); larger or 3D scenes return
+ * MPM_ERR_CAPACITY / MPM_ERR_UNSUPPORTED. */
+struct mpm_batch;
+typedef struct mpm_batch mpm_batch;
+
+typedef struct mpm_batch_config {
+    int32_t threads;           /* threads per CTA: 256 or 512 */
+    int32_t particles_per_cta; /* spread a scene over more CTAs while it has more particles per CTA than this
+                                  (0: only as many CTAs as its grid needs) */
+    int32_t max_cluster;       /* largest cluster: 1, 2, 4 or 8 */
+    int32_t reserved[5];
+} mpm_batch_config;
+
+/* Scene s uses params[s] (each validated as by mpm_create) and init[s]. */
+MPM_API mpm_status mpm_batch_create(const mpm_params* params, const mpm_particles_init* init, int32_t nscenes,
+                                    mpm_batch** batch);
+MPM_API mpm_status mpm_batch_destroy(mpm_batch* batch);
+MPM_API const char* mpm_batch_last_error(const mpm_batch* batch);
+MPM_API mpm_status mpm_batch_info(const mpm_batch* batch, int32_t* nscenes, int64_t* total_particles);
+/* Advance every scene by nsteps (asynchronous on the batch's stream; one CUDA
+ * graph per nsteps value, replayed). */
+MPM_API mpm_status mpm_batch_step(mpm_batch* batch, int32_t nsteps);
+MPM_API mpm_status mpm_batch_set_stream(mpm_batch* batch, void* cuda_stream);
+/* Per-scene state, host copies in the scene's creation order (as mpm_get_state). */
+MPM_API mpm_status mpm_batch_get_state(mpm_batch* batch, int32_t scene, mpm_state_host* state);
+MPM_API mpm_status mpm_batch_set_state(mpm_batch* batch, int32_t scene, const mpm_state_host* state);
+MPM_API mpm_status mpm_batch_get_positions(mpm_batch* batch, int32_t scene, float* out, size_t cap_floats);
+MPM_API mpm_status mpm_batch_get_status(mpm_batch* batch, int32_t scene, uint32_t* flags);
+/* Device timestamps (ns) of the last mpm_batch_step call: for each scene, its
+ * start and the end of each of its steps, [scene][nsteps + 1]; *nsteps gets the
+ * call's step count. Synchronises. */
+MPM_API mpm_status mpm_batch_step_times(mpm_batch* batch, uint64_t* out, size_t cap, int32_t* nsteps);
+MPM_API mpm_status mpm_batch_get_config(const mpm_batch* batch, mpm_batch_config* config);
+MPM_API mpm_status mpm_batch_set_config(mpm_batch* batch, const mpm_batch_config* config);
+/* Autotuner: times trial_steps steps of the batch under each candidate
+ * configuration (threads x particles per CTA), keeps the fastest, and restores
+ * the particle state, so the batch continues as if untuned. *best_ms gets the
+ * chosen configuration's time for the trial. Synchronises. */
+MPM_API mpm_status mpm_batch_tune(mpm_batch* batch, int32_t trial_steps, mpm_batch_config* chosen, double* best_ms);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

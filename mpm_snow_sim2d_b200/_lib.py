@@ -61,6 +61,11 @@ class MpmStateHost(C.Structure):
     ]
 
 
+class MpmBatchConfig(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("particles_per_cta", C.c_int32), ("max_cluster", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
 # Every symbol include/mpm/mpm.h declares, with its ctypes signature.
 _P = C.c_void_p
 SIGNATURES = {
@@ -100,6 +105,20 @@ SIGNATURES = {
     "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),
     "mpm_pair_log_read": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
+    "mpm_batch_create": (C.c_int, [C.POINTER(MpmParams), C.POINTER(MpmParticlesInit), C.c_int32, C.POINTER(_P)]),
+    "mpm_batch_destroy": (C.c_int, [_P]),
+    "mpm_batch_last_error": (C.c_char_p, [_P]),
+    "mpm_batch_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "mpm_batch_step": (C.c_int, [_P, C.c_int32]),
+    "mpm_batch_set_stream": (C.c_int, [_P, _P]),
+    "mpm_batch_get_state": (C.c_int, [_P, C.c_int32, C.POINTER(MpmStateHost)]),
+    "mpm_batch_set_state": (C.c_int, [_P, C.c_int32, C.POINTER(MpmStateHost)]),
+    "mpm_batch_get_positions": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_float), C.c_size_t]),
+    "mpm_batch_get_status": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_uint32)]),
+    "mpm_batch_step_times": (C.c_int, [_P, C.POINTER(C.c_uint64), C.c_size_t, C.POINTER(C.c_int32)]),
+    "mpm_batch_get_config": (C.c_int, [_P, C.POINTER(MpmBatchConfig)]),
+    "mpm_batch_set_config": (C.c_int, [_P, C.POINTER(MpmBatchConfig)]),
+    "mpm_batch_tune": (C.c_int, [_P, C.c_int32, C.POINTER(MpmBatchConfig), C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -16,6 +16,7 @@
 #include "mpm_kernels.cuh"
 #include "mpm_tiled.cuh"
 #include "mpm_mlp.cuh"
+#include "mpm_host.h"
 
 using namespace mpm;
 
@@ -435,57 +436,16 @@ mpm_status setup_tiled(mpm_solver* s) {
 // while |node velocity| <= v_cap = 16 cells per step (a blow-up long before
 // that point is flagged by the grid pass).
 void choose_scales(mpm_solver* s, double total_mass) {
-    const mpm_params& p = s->params;
-    const double v_cap = 16.0 / p.delta_time;
-    const double mt = total_mass > 0 ? total_mass * 1.125 : 1.0;
-    int lm = (int)std::floor(62.0 - std::log2(mt));
-    int lp = (int)std::floor(62.0 - std::log2(mt * v_cap));
-    lm = lm > 100 ? 100 : (lm < -100 ? -100 : lm);
-    lp = lp > 100 ? 100 : (lp < -100 ? -100 : lp);
-    if (p.fixed_point_log2_mass != 0) lm = p.fixed_point_log2_mass;
-    if (p.fixed_point_log2_momentum != 0) lp = p.fixed_point_log2_momentum;
-    s->log2_sm = lm;
-    s->log2_sp = lp;
-    s->log2_sf = lp + (int)std::floor(std::log2((double)p.delta_time));
-    s->C.sm = std::ldexp(1.0f, lm);
-    s->C.sp = std::ldexp(1.0f, lp);
-    s->C.sf = std::ldexp(1.0f, s->log2_sf);
-    s->C.inv_sm = std::ldexp(1.0f, -lm);
-    s->C.inv_sp = std::ldexp(1.0f, -lp);
-    s->C.inv_sf = std::ldexp(1.0f, -s->log2_sf);
-    s->C.v_cap = (float)v_cap;
+    int l2[3];
+    fixed_point_scales(s->params, total_mass, s->C, l2);
+    s->log2_sm = l2[0];
+    s->log2_sp = l2[1];
+    s->log2_sf = l2[2];
 }
 
-void fill_consts(mpm_solver* s) {
-    const mpm_params& p = s->params;
-    StepConsts& C = s->C;
-    C.W = p.width; C.H = p.height; C.Dp = s->dim == 3 ? p.depth : 0;
-    C.nx = p.width + 1; C.ny = p.height + 1; C.nz = s->dim == 3 ? p.depth + 1 : 1;
-    C.nodes = (long long)C.nx * C.ny * C.nz;
-    C.dt = p.delta_time; C.gravity = p.gravity; C.friction = p.friction;
-    C.theta_c = p.theta_c; C.theta_s = p.theta_s; C.xi = p.xi;
-    // Lame parameters as in src/shared/Parameters.h:82-84, evaluated in double.
-    const double E = p.youngs, nu = p.nu;
-    C.mu0 = (float)(E / (2.0 * (1.0 + nu)));
-    C.la0 = (float)((E * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu)));
-    C.margin = (float)p.border_margin;
-    C.boundary = p.boundary;
-}
+void fill_consts(mpm_solver* s) { s->C = step_consts(s->params, s->dim); }
 
-mpm_status validate(const mpm_params* p, std::string& why) {
-    if (!p) { why = "params is NULL"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->dim != 2 && p->dim != 3) { why = "dim must be 2 or 3"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->width < 1 || p->height < 1 || (p->dim == 3 && p->depth < 1)) { why = "grid extent must be >= 1 cell"; return MPM_ERR_INVALID_ARGUMENT; }
-    const double nodes = double(p->width + 1) * (p->height + 1) * (p->dim == 3 ? p->depth + 1 : 1);
-    if (nodes > 2.0e9) { why = "grid too large"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (!(p->delta_time > 0.f) || !std::isfinite(p->delta_time)) { why = "delta_time must be > 0"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->formulation != MPM_FORMULATION_MLS && p->formulation != MPM_FORMULATION_CLASSIC) { why = "unknown formulation"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->formulation == MPM_FORMULATION_CLASSIC && p->dim != 2) { why = "the CLASSIC (reference CPU) formulation is 2D only"; return MPM_ERR_UNSUPPORTED; }
-    if (p->boundary != MPM_BOUNDARY_FRICTION && p->boundary != MPM_BOUNDARY_STICKY) { why = "unknown boundary"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->border_margin < 0) { why = "border_margin must be >= 0"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (!(p->nu > -1.f && p->nu < 0.5f)) { why = "nu must be in (-1, 0.5)"; return MPM_ERR_INVALID_ARGUMENT; }
-    return MPM_OK;
-}
+mpm_status validate(const mpm_params* p, std::string& why) { return validate_params(p, why); }
 
 mpm_status ensure_staging(mpm_solver* s, size_t floats) {
     if (floats <= s->staging_floats) return MPM_OK;
@@ -1294,10 +1254,12 @@ mpm_status mpm_pair_log_read(mpm_solver* s, float* out, int64_t cap_pairs, int64
 
 // ---------------------------------------------------------------------------
 // Inference without allocation: fixed scratch in the device image.
-namespace {
 constexpr int kNoallocRows = MPM_MLP_NOALLOC_MAX_ROWS;
-// [rows][kMlpIn] staged inputs, then [rows][kMlpOut] outputs.
-__device__ __align__(256) float g_noalloc_scratch[(size_t)kNoallocRows * (kMlpIn + kMlpOut)];
+// [rows][kMlpIn] staged inputs, then [rows][kMlpOut] outputs. Host code sees
+// only a stand-in under this name; kernels get the device address that
+// cudaGetSymbolAddress returns.
+static __device__ __align__(256) float g_noalloc_scratch[(size_t)kNoallocRows * (kMlpIn + kMlpOut)];
+namespace {
 constexpr int kNoallocMaxDevices = 64;
 float* g_noalloc_ptr[kNoallocMaxDevices];
 cudaError_t g_noalloc_setup[kNoallocMaxDevices];

@@ -244,21 +244,15 @@ __device__ __forceinline__ void collide(const StepConsts& C, const float* loc, c
     }
 }
 
-// Grid update of one node (MLS: src/gpu/shaders/2d/grid_update.glsl:82-108,
-// 3D :88-117; CLASSIC: src/cpu/Grid.cpp:165-184). Reads and clears the
-// fixed-point accumulators (the reference's separate reset pass,
-// reset.glsl:13-23, is fused here) and writes the velocities G2P gathers.
+// Grid update of one node from its summed fixed-point accumulators q (MLS:
+// src/gpu/shaders/2d/grid_update.glsl:82-108, 3D :88-117; CLASSIC:
+// src/cpu/Grid.cpp:165-184): node velocity after gravity (vc, after the wall
+// planes; vf, after friction as well). Zero where the node mass is below 1e-6.
 template <int D, int FORM>
-__device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long long* __restrict__ acc,
-                                          float4* __restrict__ gv, unsigned* __restrict__ status, long long id) {
-    constexpr int NACC = Layout<D, FORM>::NACC;
-    long long q[NACC];
+__device__ __forceinline__ void grid_node_velocity(const StepConsts& C, const long long* q, long long ix, long long iy,
+                                                   long long iz, unsigned* __restrict__ status, float* vc, float* vf) {
 #pragma unroll
-    for (int c = 0; c < NACC; ++c) {
-        q[c] = (long long)acc[c * C.nodes + id];
-        if (q[c] != 0) acc[c * C.nodes + id] = 0ull;
-    }
-    float vc[3] = {0.f, 0.f, 0.f}, vf[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < 3; ++k) { vc[k] = 0.f; vf[k] = 0.f; }
     const float mass = __ll2float_rn(q[0]) * C.inv_sm;
     if (mass >= 1e-6f) {
         float vel[3] = {0.f, 0.f, 0.f};
@@ -278,7 +272,6 @@ __device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long lon
 #pragma unroll
         for (int k = 0; k < D; ++k) sp2 += vel[k] * vel[k];
         if (!(sp2 <= C.v_cap * C.v_cap)) raise_flag(status, (sp2 != sp2) ? 1u : 2u);
-        const long long ix = id % C.nx, iy = (id / C.nx) % C.ny, iz = id / ((long long)C.nx * C.ny);
         const float loc[3] = {float(ix), float(iy), float(iz)};
         if (C.boundary == kBoundarySticky) {
             const int mm = int(C.margin);
@@ -290,6 +283,24 @@ __device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long lon
             collide<D, FORM>(C, loc, vel, vc, vf);
         }
     }
+}
+
+// Grid update of one node of the global grid. Reads and clears the
+// fixed-point accumulators (the reference's separate reset pass,
+// reset.glsl:13-23, is fused here) and writes the velocities G2P gathers.
+template <int D, int FORM>
+__device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long long* __restrict__ acc,
+                                          float4* __restrict__ gv, unsigned* __restrict__ status, long long id) {
+    constexpr int NACC = Layout<D, FORM>::NACC;
+    long long q[NACC];
+#pragma unroll
+    for (int c = 0; c < NACC; ++c) {
+        q[c] = (long long)acc[c * C.nodes + id];
+        if (q[c] != 0) acc[c * C.nodes + id] = 0ull;
+    }
+    float vc[3], vf[3];
+    const long long ix = id % C.nx, iy = (id / C.nx) % C.ny, iz = id / ((long long)C.nx * C.ny);
+    grid_node_velocity<D, FORM>(C, q, ix, iy, iz, status, vc, vf);
     if (D == 2) {
         gv[id] = make_float4(vf[0], vf[1], vc[0], vc[1]);
     } else {
@@ -820,7 +831,7 @@ __global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, 
 // ---------------------------------------------------------------------------
 // Import / export between the caller's interleaved per-particle arrays (in
 // creation order) and the device SoA (in slot order; slot s holds particle id[s]).
-__global__ void k_export_soa(const float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
+static __global__ void k_export_soa(const float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
                              float* __restrict__ aos) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
@@ -828,7 +839,7 @@ __global__ void k_export_soa(const float* __restrict__ soa, int comps, int n, co
     for (int c = 0; c < comps; ++c) aos[(long long)p * comps + c] = soa[(long long)c * n + s];
 }
 
-__global__ void k_import_soa(float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
+static __global__ void k_import_soa(float* __restrict__ soa, int comps, int n, const int* __restrict__ id,
                              const float* __restrict__ aos) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;

@@ -193,6 +193,55 @@ def two_snowballs_3d(W: int = 256, ppc: int = 8, seed: int = 1005, steps: int = 
     return _scene(f"two_snowballs3d_{W}_ppc{ppc}", 3, W, dt, steps, pos, vel, ppc, dict(seed=seed))
 
 
+def batch_scene_2d(index: int, seed: int = 1004, steps: int = 500, side=(64, 256), count=(2000, 64000),
+                   fill_max: float = 0.35) -> Scene:
+    """Scene `index` of the batched workload: a square grid of side drawn
+    log-uniformly in [64, 256] cells, 1-4 non-overlapping snow blocks at 4-8
+    particles per cell holding a particle count drawn log-uniformly in
+    [2k, 64k] (capped at fill_max of the domain), E ~ U(1e5, 2e5),
+    nu ~ U(0.15, 0.3); dt scales with the cell size (1e-4 at 128 cells).
+    Seed: seed + index."""
+    rng = np.random.Generator(np.random.PCG64(seed + index))
+    W = int(round(np.exp(rng.uniform(np.log(side[0]), np.log(side[1])))))
+    dx = 1.0 / W
+    nblocks = int(rng.integers(1, 5))
+    ppc = int(rng.integers(4, 9))
+    youngs = float(rng.uniform(1e5, 2e5))
+    nu = float(rng.uniform(0.15, 0.3))
+    hi_count = min(count[1], fill_max * W * W * ppc)
+    target = float(np.exp(rng.uniform(np.log(count[0]), np.log(hi_count))))
+    area = target / (W * W * ppc)  # fraction of the unit square
+    shares = rng.dirichlet(np.ones(nblocks)) * area
+    lo_wall, hi_wall = (MARGIN + 2) * dx, 1.0 - (MARGIN + 2) * dx
+    boxes = []
+    for _ in range(1000):  # place every block, restarting the layout when one does not fit
+        boxes = []
+        for a in sorted(shares, reverse=True):
+            s_ = float(np.sqrt(a))
+            for _ in range(200):
+                c = rng.uniform(lo_wall + s_ / 2, hi_wall - s_ / 2, 2)
+                lo, hi = c - s_ / 2, c + s_ / 2
+                if all(np.any(hi <= b_lo) or np.any(lo >= b_hi) for b_lo, b_hi in boxes):
+                    boxes.append((lo, hi))
+                    break
+            else:
+                break
+        if len(boxes) == nblocks:
+            break
+    else:
+        raise RuntimeError("could not place the blocks without overlap")
+    pos = np.concatenate([_box(rng, lo, hi, ppc, dx) for lo, hi in boxes])
+    vel = np.array([0.0, -1.0]) + rng.uniform(-0.1, 0.1, pos.shape)
+    dt = 1e-4 * 128.0 / W
+    return _scene(f"batch2d_{index}_{W}_ppc{ppc}", 2, W, dt, steps, pos, vel, ppc,
+                  dict(seed=seed + index, blocks=nblocks), youngs=youngs, nu=nu)
+
+
+def batch_scenes_2d(nscenes: int = 256, seed: int = 1004, steps: int = 500) -> list:
+    """The batched workload: `nscenes` independent 2D scenes (batch_scene_2d)."""
+    return [batch_scene_2d(i, seed=seed, steps=steps) for i in range(nscenes)]
+
+
 def workload(name: str) -> Scene:
     """The named workloads: c1..c5 with the sizes stated for them."""
     if name == "c1":
