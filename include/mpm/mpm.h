@@ -289,7 +289,8 @@ typedef struct mpm_batch_config {
     int32_t particles_per_cta; /* spread a scene over more CTAs while it has more particles per CTA than this
                                   (0: only as many CTAs as its grid needs) */
     int32_t max_cluster;       /* largest cluster: 1, 2, 4 or 8 */
-    int32_t reserved[5];
+    int32_t sort_period;       /* steps between re-sorts of a multi-CTA scene's particles by row (0: 16) */
+    int32_t reserved[4];
 } mpm_batch_config;
 
 /* Scene s uses params[s] (each validated as by mpm_create) and init[s]. */

@@ -63,7 +63,7 @@ class MpmStateHost(C.Structure):
 
 class MpmBatchConfig(C.Structure):
     _fields_ = [("threads", C.c_int32), ("particles_per_cta", C.c_int32), ("max_cluster", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("sort_period", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 # Every symbol include/mpm/mpm.h declares, with its ctypes signature.

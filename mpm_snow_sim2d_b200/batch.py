@@ -105,9 +105,10 @@ class Batch:
     def config(self) -> dict:
         c = MpmBatchConfig()
         self._check(self._lib.mpm_batch_get_config(self._h, C.byref(c)))
-        return dict(threads=c.threads, particles_per_cta=c.particles_per_cta, max_cluster=c.max_cluster)
+        return dict(threads=c.threads, particles_per_cta=c.particles_per_cta, max_cluster=c.max_cluster,
+                    sort_period=c.sort_period)
 
-    def set_config(self, threads=None, particles_per_cta=None, max_cluster=None) -> None:
+    def set_config(self, threads=None, particles_per_cta=None, max_cluster=None, sort_period=None) -> None:
         c = MpmBatchConfig()
         self._check(self._lib.mpm_batch_get_config(self._h, C.byref(c)))
         if threads is not None:
@@ -116,6 +117,8 @@ class Batch:
             c.particles_per_cta = particles_per_cta
         if max_cluster is not None:
             c.max_cluster = max_cluster
+        if sort_period is not None:
+            c.sort_period = sort_period
         self._check(self._lib.mpm_batch_set_config(self._h, C.byref(c)))
 
     def tune(self, trial_steps: int = 4):
@@ -123,7 +126,8 @@ class Batch:
         c = MpmBatchConfig()
         ms = C.c_double()
         self._check(self._lib.mpm_batch_tune(self._h, int(trial_steps), C.byref(c), C.byref(ms)))
-        return dict(threads=c.threads, particles_per_cta=c.particles_per_cta, max_cluster=c.max_cluster), ms.value
+        return dict(threads=c.threads, particles_per_cta=c.particles_per_cta, max_cluster=c.max_cluster,
+                    sort_period=c.sort_period), ms.value
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -36,9 +36,9 @@ struct mpm_batch {
     std::vector<long long> p0;
     std::vector<int> counts;
     std::vector<BatchScene> scenes;  // host copy (cl, rows follow the configuration)
-    float *x = nullptr, *v = nullptr, *B = nullptr, *Fe = nullptr, *Jp = nullptr, *A = nullptr, *mass = nullptr,
-          *vol = nullptr;
+    BatchBuffers buf[2] = {};
     BatchScene* d_scenes = nullptr;
+    BatchSceneState* d_state = nullptr;
     int* d_order = nullptr;
     int* d_queue = nullptr;
     int* d_needs_affine = nullptr;
@@ -92,10 +92,14 @@ void drop_graph(mpm_batch* b) {
 
 void release(mpm_batch* b) {
     drop_graph(b);
-    float* fl[] = {b->x, b->v, b->B, b->Fe, b->Jp, b->A, b->mass, b->vol};
-    for (float* p : fl)
-        if (p) cudaFree(p);
+    for (BatchBuffers& f : b->buf) {
+        float* fl[] = {f.x, f.v, f.B, f.Fe, f.Jp, f.A, f.mass, f.vol};
+        for (float* p : fl)
+            if (p) cudaFree(p);
+        if (f.id) cudaFree(f.id);
+    }
     if (b->d_scenes) cudaFree(b->d_scenes);
+    if (b->d_state) cudaFree(b->d_state);
     if (b->d_order) cudaFree(b->d_order);
     if (b->d_queue) cudaFree(b->d_queue);
     if (b->d_needs_affine) cudaFree(b->d_needs_affine);
@@ -113,8 +117,26 @@ using BatchKernel = void (*)(BatchParticles, BatchRun);
 
 BatchKernel kernel_for(int threads) { return threads == 512 ? k_batch_run<512> : k_batch_run<256>; }
 
-BatchParticles particles(const mpm_batch* b) {
-    return BatchParticles{b->x, b->v, b->B, b->Fe, b->Jp, b->A, b->mass, b->vol, b->N};
+BatchParticles particles(const mpm_batch* b) { return BatchParticles{{b->buf[0], b->buf[1]}, b->N}; }
+
+// Where each scene's particles are now (buffer parity) and their slot order.
+mpm_status scene_states(mpm_batch* b, std::vector<BatchSceneState>& st) {
+    st.resize(b->nscenes);
+    BATCH_CUDA(b, cudaMemcpyAsync(st.data(), b->d_state, sizeof(BatchSceneState) * st.size(), cudaMemcpyDeviceToHost,
+                                  b->stream));
+    BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+    return MPM_OK;
+}
+
+// Forget every scene's bands (they belong to a cluster size): the next step
+// of each multi-CTA scene starts with a sort.
+mpm_status invalidate_bands(mpm_batch* b) {
+    std::vector<BatchSceneState> st;
+    mpm_status r = scene_states(b, st);
+    if (r != MPM_OK) return r;
+    for (auto& x : st) x.sorted = 0;
+    BATCH_CUDA(b, cudaMemcpy(b->d_state, st.data(), sizeof(BatchSceneState) * st.size(), cudaMemcpyHostToDevice));
+    return MPM_OK;
 }
 
 cudaLaunchConfig_t launch_config(const mpm_batch* b, const BatchClass& k, cudaLaunchAttribute* attr, int clusters) {
@@ -138,6 +160,7 @@ mpm_status configure(mpm_batch* b, const mpm_batch_config& cfg) {
     if (cfg.max_cluster != 1 && cfg.max_cluster != 2 && cfg.max_cluster != 4 && cfg.max_cluster != 8)
         return bfail(b, MPM_ERR_INVALID_ARGUMENT, "max_cluster must be 1, 2, 4 or 8");
     if (cfg.particles_per_cta < 0) return bfail(b, MPM_ERR_INVALID_ARGUMENT, "particles_per_cta must be >= 0");
+    if (cfg.sort_period < 0) return bfail(b, MPM_ERR_INVALID_ARGUMENT, "sort_period must be >= 0");
     std::vector<BatchScene> sc = b->scenes;
     std::vector<std::vector<int>> members(4);
     for (int s = 0; s < b->nscenes; ++s) {
@@ -157,7 +180,8 @@ mpm_status configure(mpm_batch* b, const mpm_batch_config& cfg) {
                    (long long)sc[s].n > (long long)cfg.particles_per_cta * kClusterSizes[ci])
                 ++ci;
         sc[s].cl = kClusterSizes[ci];
-        sc[s].rows = (ny + sc[s].cl - 1) / sc[s].cl;
+        // a multi-CTA scene may give any CTA up to its full capacity in rows
+        sc[s].rows = sc[s].cl == 1 ? ny : b->cap_max / nx;
         if (sc[s].n > 0) members[ci].push_back(s);
     }
     std::vector<int> order;
@@ -175,6 +199,7 @@ mpm_status configure(mpm_batch* b, const mpm_batch_config& cfg) {
             cls[c].cap = std::max(cls[c].cap, sc[s].rows * sc[s].C.nx);
             order.push_back(s);
         }
+        if (cls[c].cl > 1 && cls[c].count > 0) cls[c].cap = b->cap_max;
     }
     // Shared-memory opt-in and persistent cluster counts.
     b->cfg = cfg;
@@ -199,7 +224,8 @@ mpm_status configure(mpm_batch* b, const mpm_batch_config& cfg) {
     BATCH_CUDA(b, cudaMemcpy(b->d_scenes, sc.data(), sizeof(BatchScene) * sc.size(), cudaMemcpyHostToDevice));
     if (!order.empty())
         BATCH_CUDA(b, cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
-    return MPM_OK;
+    // bands of the old cluster sizes are void: each scene re-sorts on its next step
+    return invalidate_bands(b);
 }
 
 // Enqueue one call: zero the queues, then every class's persistent launch on
@@ -214,8 +240,9 @@ cudaError_t enqueue(mpm_batch* b, int nsteps) {
         const BatchClass& k = b->cls[c];
         if (k.count == 0) continue;
         if ((e = cudaStreamWaitEvent(b->aux[c], b->fork, 0)) != cudaSuccess) return e;
-        BatchRun R{b->d_scenes, b->d_order + k.first, k.count, k.cap, b->d_queue + c, b->d_needs_affine,
-                   b->d_status, b->d_stamps, nsteps};
+        BatchRun R{b->d_scenes, b->d_state, b->d_order + k.first, k.count, k.cap, b->d_queue + c,
+                   b->d_needs_affine, b->d_status, b->d_stamps, nsteps,
+                   b->cfg.sort_period > 0 ? b->cfg.sort_period : 16};
         cudaLaunchAttribute attr[1];
         cudaLaunchConfig_t lc = launch_config(b, k, attr, k.clusters);
         lc.stream = b->aux[c];
@@ -226,33 +253,33 @@ cudaError_t enqueue(mpm_batch* b, int nsteps) {
     return cudaSuccess;
 }
 
-mpm_status copy_slice_out(mpm_batch* b, const float* soa, int comps, int scene, float* host) {
+// Scene slice of one field in creation order (slots hold particles id[slot]).
+mpm_status copy_slice_out(mpm_batch* b, int field, int comps, int scene, float* host) {
     const int n = b->counts[scene];
     if (n == 0) return MPM_OK;
+    std::vector<BatchSceneState> st;
+    mpm_status r = scene_states(b, st);
+    if (r != MPM_OK) return r;
+    const BatchBuffers& F = b->buf[st[scene].parity & 1];
+    const float* soa[] = {F.x, F.v, F.B, F.Fe, F.Jp};
     std::vector<float> tmp((size_t)n * comps);
+    std::vector<int> id(n);
     for (int c = 0; c < comps; ++c)
-        BATCH_CUDA(b, cudaMemcpyAsync(tmp.data() + (size_t)c * n, soa + (size_t)c * b->N + b->p0[scene],
+        BATCH_CUDA(b, cudaMemcpyAsync(tmp.data() + (size_t)c * n, soa[field] + (size_t)c * b->N + b->p0[scene],
                                       sizeof(float) * n, cudaMemcpyDeviceToHost, b->stream));
+    BATCH_CUDA(b, cudaMemcpyAsync(id.data(), F.id + b->p0[scene], sizeof(int) * n, cudaMemcpyDeviceToHost, b->stream));
     BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
-    for (int i = 0; i < n; ++i)
-        for (int c = 0; c < comps; ++c) host[(size_t)i * comps + c] = tmp[(size_t)c * n + i];
-    return MPM_OK;
-}
-
-mpm_status copy_slice_in(mpm_batch* b, float* soa, int comps, int scene, const float* host) {
-    const int n = b->counts[scene];
-    if (n == 0 || !host) return MPM_OK;
-    std::vector<float> tmp((size_t)n * comps);
-    for (int i = 0; i < n; ++i)
-        for (int c = 0; c < comps; ++c) tmp[(size_t)c * n + i] = host[(size_t)i * comps + c];
-    for (int c = 0; c < comps; ++c)
-        BATCH_CUDA(b, cudaMemcpyAsync(soa + (size_t)c * b->N + b->p0[scene], tmp.data() + (size_t)c * n,
-                                      sizeof(float) * n, cudaMemcpyHostToDevice, b->stream));
-    BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+    for (int j = 0; j < n; ++j) {
+        const int i = id[j];
+        if (i < 0 || i >= n) return bfail(b, MPM_ERR_CUDA, "corrupt particle order");
+        for (int c = 0; c < comps; ++c) host[(size_t)i * comps + c] = tmp[(size_t)c * n + j];
+    }
     return MPM_OK;
 }
 
 bool valid_scene(const mpm_batch* b, int32_t s) { return b && s >= 0 && s < b->nscenes; }
+
+enum { kFieldX = 0, kFieldV = 1, kFieldB = 2, kFieldFe = 3, kFieldJp = 4 };
 
 }  // namespace
 
@@ -269,6 +296,7 @@ mpm_status mpm_batch_create(const mpm_params* params, const mpm_particles_init* 
         mpm_status st = validate_params(&params[s], why);
         if (st != MPM_OK) return st;
         if (params[s].dim != 2 || params[s].formulation != MPM_FORMULATION_MLS) return MPM_ERR_UNSUPPORTED;
+        if (params[s].height + 1 > kBatchMaxRows) return MPM_ERR_CAPACITY;
         if (init[s].count < 0 || init[s].count > 0x7fffffff) return MPM_ERR_INVALID_ARGUMENT;
         if (init[s].count > 0 && (!init[s].position || !init[s].volume)) return MPM_ERR_INVALID_ARGUMENT;
         N += init[s].count;
@@ -330,14 +358,20 @@ mpm_status mpm_batch_create(const mpm_params* params, const mpm_particles_init* 
             return bail(MPM_ERR_CUDA);
     if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return bail(MPM_ERR_CUDA);
     const size_t n = (size_t)N;
-    if (balloc(&b->x, n * 2) || balloc(&b->v, n * 2) || balloc(&b->B, n * 4) || balloc(&b->Fe, n * 4) ||
-        balloc(&b->Jp, n) || balloc(&b->A, n * 4) || balloc(&b->mass, n) || balloc(&b->vol, n) ||
-        balloc(&b->d_scenes, (size_t)nscenes) || balloc(&b->d_order, (size_t)nscenes) || balloc(&b->d_queue, 4) ||
+    bool alloc_ok = true;
+    for (BatchBuffers& f : b->buf)
+        alloc_ok = alloc_ok && !balloc(&f.x, n * 2) && !balloc(&f.v, n * 2) && !balloc(&f.B, n * 4) &&
+                   !balloc(&f.Fe, n * 4) && !balloc(&f.Jp, n) && !balloc(&f.A, n * 4) && !balloc(&f.mass, n) &&
+                   !balloc(&f.vol, n) && !balloc(&f.id, n);
+    if (!alloc_ok || balloc(&b->d_scenes, (size_t)nscenes) || balloc(&b->d_state, (size_t)nscenes) ||
+        balloc(&b->d_order, (size_t)nscenes) || balloc(&b->d_queue, 4) ||
         balloc(&b->d_needs_affine, (size_t)nscenes) || balloc(&b->d_status, (size_t)nscenes)) {
         cudaGetLastError();
         return bail(MPM_ERR_OUT_OF_MEMORY);
     }
-    // SoA upload: F_E = I, B = 0, J_p = 1 (Particle ctor, src/cpu/Particles.cpp:7-19).
+    // SoA upload into buffer 0: F_E = I, B = 0, J_p = 1 (Particle ctor,
+    // src/cpu/Particles.cpp:7-19); slot order = creation order.
+    const BatchBuffers& F = b->buf[0];
     std::vector<float> soa(n * 4, 0.f);
     bool ok = true;
     auto up = [&](float* dst, size_t count) {
@@ -346,21 +380,28 @@ mpm_status mpm_batch_create(const mpm_params* params, const mpm_particles_init* 
     for (int s = 0; s < nscenes; ++s)
         for (int i = 0; i < b->counts[s]; ++i)
             for (int k = 0; k < 2; ++k) soa[(size_t)k * n + b->p0[s] + i] = init[s].position[(size_t)i * 2 + k];
-    ok = ok && up(b->x, n * 2);
+    ok = ok && up(F.x, n * 2);
     for (int s = 0; s < nscenes; ++s)
         for (int i = 0; i < b->counts[s]; ++i)
             for (int k = 0; k < 2; ++k)
                 soa[(size_t)k * n + b->p0[s] + i] = init[s].velocity ? init[s].velocity[(size_t)i * 2 + k] : 0.f;
-    ok = ok && up(b->v, n * 2);
+    ok = ok && up(F.v, n * 2);
     std::fill(soa.begin(), soa.end(), 0.f);
-    ok = ok && up(b->B, n * 4) && up(b->A, n * 4);
+    ok = ok && up(F.B, n * 4) && up(F.A, n * 4);
     for (int k = 0; k < 4; ++k)
         for (size_t i = 0; i < n; ++i) soa[(size_t)k * n + i] = (k % 3 == 0) ? 1.f : 0.f;
-    ok = ok && up(b->Fe, n * 4);
+    ok = ok && up(F.Fe, n * 4);
     std::fill(soa.begin(), soa.begin() + n, 1.f);
-    ok = ok && up(b->Jp, n);
-    ok = ok && cudaMemcpy(b->mass, massv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
-    ok = ok && cudaMemcpy(b->vol, volv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && up(F.Jp, n);
+    ok = ok && cudaMemcpy(F.mass, massv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && cudaMemcpy(F.vol, volv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    std::vector<int> ids(n);
+    for (int s = 0; s < nscenes; ++s)
+        for (int i = 0; i < b->counts[s]; ++i) ids[b->p0[s] + i] = i;
+    ok = ok && cudaMemcpy(F.id, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    std::vector<BatchSceneState> st0(nscenes);
+    std::memset(st0.data(), 0, sizeof(BatchSceneState) * nscenes);
+    ok = ok && cudaMemcpy(b->d_state, st0.data(), sizeof(BatchSceneState) * nscenes, cudaMemcpyHostToDevice) == cudaSuccess;
     std::vector<int> ones(nscenes, 1);
     ok = ok && cudaMemcpy(b->d_needs_affine, ones.data(), sizeof(int) * nscenes, cudaMemcpyHostToDevice) == cudaSuccess;
     ok = ok && cudaMemset(b->d_status, 0, sizeof(unsigned) * nscenes) == cudaSuccess;
@@ -369,6 +410,7 @@ mpm_status mpm_batch_create(const mpm_params* params, const mpm_particles_init* 
     cfg.threads = 512;
     cfg.particles_per_cta = 8192;
     cfg.max_cluster = kBatchMaxCluster;
+    cfg.sort_period = 16;
     mpm_status st = configure(b, cfg);
     if (st != MPM_OK) return bail(st);
     *out = b;
@@ -442,14 +484,17 @@ mpm_status mpm_batch_set_stream(mpm_batch* b, void* stream) {
 mpm_status mpm_batch_get_state(mpm_batch* b, int32_t scene, mpm_state_host* st) {
     if (!valid_scene(b, scene) || !st || st->count != b->counts[scene]) return MPM_ERR_INVALID_ARGUMENT;
     mpm_status r = MPM_OK;
-    if (st->position && (r = copy_slice_out(b, b->x, 2, scene, st->position)) != MPM_OK) return r;
-    if (st->velocity && (r = copy_slice_out(b, b->v, 2, scene, st->velocity)) != MPM_OK) return r;
-    if (st->affine_b && (r = copy_slice_out(b, b->B, 4, scene, st->affine_b)) != MPM_OK) return r;
-    if (st->elastic_f && (r = copy_slice_out(b, b->Fe, 4, scene, st->elastic_f)) != MPM_OK) return r;
-    if (st->plastic_det && (r = copy_slice_out(b, b->Jp, 1, scene, st->plastic_det)) != MPM_OK) return r;
+    if (st->position && (r = copy_slice_out(b, kFieldX, 2, scene, st->position)) != MPM_OK) return r;
+    if (st->velocity && (r = copy_slice_out(b, kFieldV, 2, scene, st->velocity)) != MPM_OK) return r;
+    if (st->affine_b && (r = copy_slice_out(b, kFieldB, 4, scene, st->affine_b)) != MPM_OK) return r;
+    if (st->elastic_f && (r = copy_slice_out(b, kFieldFe, 4, scene, st->elastic_f)) != MPM_OK) return r;
+    if (st->plastic_det && (r = copy_slice_out(b, kFieldJp, 1, scene, st->plastic_det)) != MPM_OK) return r;
     return MPM_OK;
 }
 
+// Writes the scene back in creation order (ids reset), so it re-sorts on its
+// next step and re-derives its affine matrices. Fields left NULL keep their
+// values.
 mpm_status mpm_batch_set_state(mpm_batch* b, int32_t scene, const mpm_state_host* st) {
     if (!valid_scene(b, scene) || !st || st->count != b->counts[scene]) return MPM_ERR_INVALID_ARGUMENT;
     const int n = b->counts[scene];
@@ -463,12 +508,45 @@ mpm_status mpm_batch_set_state(mpm_batch* b, int32_t scene, const mpm_state_host
         !finite(st->affine_b, 4 * (size_t)n) || !finite(st->elastic_f, 4 * (size_t)n) ||
         !finite(st->plastic_det, (size_t)n))
         return bfail(b, MPM_ERR_INVALID_ARGUMENT, "state holds non-finite values");
-    mpm_status r = MPM_OK;
-    if ((r = copy_slice_in(b, b->x, 2, scene, st->position)) != MPM_OK) return r;
-    if ((r = copy_slice_in(b, b->v, 2, scene, st->velocity)) != MPM_OK) return r;
-    if ((r = copy_slice_in(b, b->B, 4, scene, st->affine_b)) != MPM_OK) return r;
-    if ((r = copy_slice_in(b, b->Fe, 4, scene, st->elastic_f)) != MPM_OK) return r;
-    if ((r = copy_slice_in(b, b->Jp, 1, scene, st->plastic_det)) != MPM_OK) return r;
+    if (n == 0) return MPM_OK;
+    std::vector<BatchSceneState> ss;
+    mpm_status r = scene_states(b, ss);
+    if (r != MPM_OK) return r;
+    const BatchBuffers& F = b->buf[ss[scene].parity & 1];
+    // current contents in creation order, overlaid with what the caller gives
+    const int comps[] = {2, 2, 4, 4, 1};
+    const float* given[] = {st->position, st->velocity, st->affine_b, st->elastic_f, st->plastic_det};
+    float* soa[] = {F.x, F.v, F.B, F.Fe, F.Jp};
+    std::vector<int> id(n);
+    BATCH_CUDA(b, cudaMemcpyAsync(id.data(), F.id + b->p0[scene], sizeof(int) * n, cudaMemcpyDeviceToHost, b->stream));
+    std::vector<float> mass(n), vol(n), ms(n), vs(n);
+    BATCH_CUDA(b, cudaMemcpyAsync(ms.data(), F.mass + b->p0[scene], sizeof(float) * n, cudaMemcpyDeviceToHost, b->stream));
+    BATCH_CUDA(b, cudaMemcpyAsync(vs.data(), F.vol + b->p0[scene], sizeof(float) * n, cudaMemcpyDeviceToHost, b->stream));
+    BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+    for (int j = 0; j < n; ++j) {
+        if (id[j] < 0 || id[j] >= n) return bfail(b, MPM_ERR_CUDA, "corrupt particle order");
+        mass[id[j]] = ms[j];
+        vol[id[j]] = vs[j];
+    }
+    for (int f = 0; f < 5; ++f) {
+        std::vector<float> host((size_t)n * comps[f]);
+        if (given[f]) std::memcpy(host.data(), given[f], sizeof(float) * host.size());
+        else if ((r = copy_slice_out(b, f, comps[f], scene, host.data())) != MPM_OK) return r;
+        std::vector<float> tmp(host.size());
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < comps[f]; ++c) tmp[(size_t)c * n + i] = host[(size_t)i * comps[f] + c];
+        for (int c = 0; c < comps[f]; ++c)
+            BATCH_CUDA(b, cudaMemcpyAsync(soa[f] + (size_t)c * b->N + b->p0[scene], tmp.data() + (size_t)c * n,
+                                          sizeof(float) * n, cudaMemcpyHostToDevice, b->stream));
+        BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+    }
+    for (int i = 0; i < n; ++i) id[i] = i;
+    BATCH_CUDA(b, cudaMemcpy(F.mass + b->p0[scene], mass.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    BATCH_CUDA(b, cudaMemcpy(F.vol + b->p0[scene], vol.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    BATCH_CUDA(b, cudaMemcpy(F.id + b->p0[scene], id.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    ss[scene].sorted = 0;
+    ss[scene].step = 0;
+    BATCH_CUDA(b, cudaMemcpy(b->d_state + scene, &ss[scene], sizeof(BatchSceneState), cudaMemcpyHostToDevice));
     const int one = 1;
     BATCH_CUDA(b, cudaMemcpy(b->d_needs_affine + scene, &one, sizeof(int), cudaMemcpyHostToDevice));
     return MPM_OK;
@@ -477,7 +555,7 @@ mpm_status mpm_batch_set_state(mpm_batch* b, int32_t scene, const mpm_state_host
 mpm_status mpm_batch_get_positions(mpm_batch* b, int32_t scene, float* out, size_t cap_floats) {
     if (!valid_scene(b, scene) || (!out && b->counts[scene] > 0)) return MPM_ERR_INVALID_ARGUMENT;
     if (cap_floats < (size_t)b->counts[scene] * 2) return bfail(b, MPM_ERR_CAPACITY, "output buffer too small");
-    return copy_slice_out(b, b->x, 2, scene, out);
+    return copy_slice_out(b, kFieldX, 2, scene, out);
 }
 
 mpm_status mpm_batch_get_status(mpm_batch* b, int32_t scene, uint32_t* flags) {
@@ -523,37 +601,37 @@ mpm_status mpm_batch_tune(mpm_batch* b, int32_t trial_steps, mpm_batch_config* c
     if (!b || trial_steps < 1) return MPM_ERR_INVALID_ARGUMENT;
     BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
     const size_t n = (size_t)b->N;
-    // Snapshot of everything a step changes.
-    float* fields[] = {b->x, b->v, b->B, b->Fe, b->Jp, b->A};
-    const size_t comps[] = {2, 2, 4, 4, 1, 4};
-    size_t total = 0;
-    for (size_t c : comps) total += c * n;
-    float* snap = nullptr;
-    int* snap_aff = nullptr;
-    unsigned* snap_status = nullptr;
-    BATCH_CUDA(b, balloc(&snap, total));
-    if (balloc(&snap_aff, (size_t)b->nscenes) != cudaSuccess || balloc(&snap_status, (size_t)b->nscenes) != cudaSuccess) {
-        cudaGetLastError();
-        cudaFree(snap);
-        if (snap_aff) cudaFree(snap_aff);
-        return bfail(b, MPM_ERR_OUT_OF_MEMORY, "tuner snapshot");
+    // Snapshot of everything a step changes: both particle buffers (a sort
+    // moves particles between them), per-scene state, flags.
+    struct Span { void* p; size_t bytes; };
+    std::vector<Span> spans;
+    for (BatchBuffers& f : b->buf) {
+        spans.push_back({f.x, sizeof(float) * 2 * n});
+        spans.push_back({f.v, sizeof(float) * 2 * n});
+        spans.push_back({f.B, sizeof(float) * 4 * n});
+        spans.push_back({f.Fe, sizeof(float) * 4 * n});
+        spans.push_back({f.Jp, sizeof(float) * n});
+        spans.push_back({f.A, sizeof(float) * 4 * n});
+        spans.push_back({f.mass, sizeof(float) * n});
+        spans.push_back({f.vol, sizeof(float) * n});
+        spans.push_back({f.id, sizeof(int) * n});
     }
+    spans.push_back({b->d_state, sizeof(BatchSceneState) * (size_t)b->nscenes});
+    spans.push_back({b->d_needs_affine, sizeof(int) * (size_t)b->nscenes});
+    spans.push_back({b->d_status, sizeof(unsigned) * (size_t)b->nscenes});
+    size_t total = 0;
+    for (const Span& sp : spans) total += (sp.bytes + 255) / 256 * 256;
+    unsigned char* snap = nullptr;
+    BATCH_CUDA(b, balloc(&snap, total));
     auto copy_all = [&](bool save) {
         size_t o = 0;
         cudaError_t e = cudaSuccess;
-        for (int f = 0; f < 6 && e == cudaSuccess; ++f) {
-            const size_t bytes = sizeof(float) * comps[f] * n;
-            e = save ? cudaMemcpyAsync(snap + o, fields[f], bytes, cudaMemcpyDeviceToDevice, b->stream)
-                     : cudaMemcpyAsync(fields[f], snap + o, bytes, cudaMemcpyDeviceToDevice, b->stream);
-            o += comps[f] * n;
+        for (const Span& sp : spans) {
+            if (e != cudaSuccess) break;
+            e = save ? cudaMemcpyAsync(snap + o, sp.p, sp.bytes, cudaMemcpyDeviceToDevice, b->stream)
+                     : cudaMemcpyAsync(sp.p, snap + o, sp.bytes, cudaMemcpyDeviceToDevice, b->stream);
+            o += (sp.bytes + 255) / 256 * 256;
         }
-        const size_t sb = sizeof(int) * (size_t)b->nscenes;
-        if (e == cudaSuccess)
-            e = save ? cudaMemcpyAsync(snap_aff, b->d_needs_affine, sb, cudaMemcpyDeviceToDevice, b->stream)
-                     : cudaMemcpyAsync(b->d_needs_affine, snap_aff, sb, cudaMemcpyDeviceToDevice, b->stream);
-        if (e == cudaSuccess)
-            e = save ? cudaMemcpyAsync(snap_status, b->d_status, sb, cudaMemcpyDeviceToDevice, b->stream)
-                     : cudaMemcpyAsync(b->d_status, snap_status, sb, cudaMemcpyDeviceToDevice, b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         return e;
     };
@@ -576,6 +654,7 @@ mpm_status mpm_batch_tune(mpm_batch* b, int32_t trial_steps, mpm_batch_config* c
             // one untimed call (graph capture, first-touch), then the timed one
             for (int rep = 0; rep < 2 && ce == cudaSuccess && st == MPM_OK; ++rep) {
                 if ((ce = copy_all(false)) != cudaSuccess) break;
+                if ((st = invalidate_bands(b)) != MPM_OK) break;
                 if ((ce = cudaEventRecord(e0, b->stream)) != cudaSuccess) break;
                 st = mpm_batch_step(b, trial_steps);
                 if (st != MPM_OK) break;
@@ -588,17 +667,23 @@ mpm_status mpm_batch_tune(mpm_batch* b, int32_t trial_steps, mpm_batch_config* c
                 best = cfg;
             }
         }
-    if (ce == cudaSuccess && st == MPM_OK) ce = copy_all(false);
+    // put the batch back as it was, whatever happened above
+    const cudaError_t ce_restore = copy_all(false);
+    if (ce == cudaSuccess) ce = ce_restore;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(snap);
-    cudaFree(snap_aff);
-    cudaFree(snap_status);
     if (ce != cudaSuccess) {
         cudaGetLastError();
+        configure(b, start);
         return bfail(b, MPM_ERR_CUDA, std::string("tuner: ") + cudaGetErrorString(ce));
     }
-    if (st != MPM_OK) return st;
+    if (st != MPM_OK) {
+        const std::string why = b->err;
+        configure(b, start);
+        b->err = why;
+        return st;
+    }
     st = configure(b, best);
     if (st != MPM_OK) return st;
     if (chosen) *chosen = best;

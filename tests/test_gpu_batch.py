@@ -3,6 +3,8 @@ mixed batch (grids of 64 to 256 cells, clusters of 1 to 8 CTAs) against the
 FP64 oracle and the single-scene solver; a scene's result independent of its
 cluster size and of the other scenes (bitwise); determinism; the autotuner;
 state round trips; errors."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -132,8 +134,9 @@ def test_step_times_and_errors(gpu_lib):
         with pytest.raises(MpmError) as e:
             b.set_config(threads=384)
         assert e.value.status == 1
-        with pytest.raises(MpmError):
-            b.get_state(3)
+        out = np.empty(8, np.float32)
+        assert b._lib.mpm_batch_get_positions(b._h, 3, out.ctypes.data_as(C.POINTER(C.c_float)), 8) == 1
+        assert b._lib.mpm_batch_get_positions(b._h, 0, out.ctypes.data_as(C.POINTER(C.c_float)), 8) == 11
     big = scenes.batch_scene_2d(0).with_(width=400, height=400)  # 401^2 nodes: beyond 8 CTAs
     with pytest.raises(MpmError) as e:
         Batch([big])
