@@ -212,6 +212,75 @@ def mlp_vs_plain(args, torch, stream):
     }
 
 
+def batched_scenes(args, torch):
+    """The batched workload: 256 independent 2D scenes (grid sides 64-256,
+    2k-64k particles each) advanced `batch_steps` steps in one call after the
+    autotuner picked the launch configuration. Scene-step latency from the
+    device timestamps each scene records at the end of each of its steps;
+    batch-step latency from CUDA events around single-step calls. For
+    comparison, the single-scene solver is timed on a sample of the same
+    scenes, one after another."""
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    from mpm_snow_sim2d_b200.batch import Batch
+    scs = scenes.batch_scenes_2d(args.batch_scenes, steps=args.batch_steps)
+    n = sum(s.count for s in scs)
+    stream = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    with Batch(scs) as b:
+        b.set_stream(stream.cuda_stream)
+        cfg, tune_ms = b.tune(4)
+        b.step(args.warmup)
+        torch.cuda.synchronize()
+        ms = timed(lambda: b.step(args.batch_steps))
+        t = b.step_times().astype(np.int64)
+        scene_step_us = np.diff(t, axis=1).ravel() / 1e3
+        flags = 0
+        for k in range(len(scs)):
+            flags |= b.status(k)
+        one = [timed(lambda: b.step(1)) for _ in range(args.batch_latency_calls)]
+    # the single-scene solver on every 16th scene, back to back
+    sample = scs[:: max(1, len(scs) // 16)]
+    seq_ms, seq_steps = 0.0, 100
+    for sc in sample:
+        with Solver.from_scene(sc) as s:
+            s.set_stream(stream.cuda_stream)
+            s.Step(5)
+            seq_ms += timed(lambda: s.Step(seq_steps))
+    seq_scene_step_ms = seq_ms / (len(sample) * seq_steps)
+    seq_total_s = seq_scene_step_ms * len(scs) * args.batch_steps / 1e3
+    p2g_b, g2p_b = bytes_per_particle(2)
+    peak, peak_src = load_peaks()
+    gbs = n * args.batch_steps * (p2g_b + g2p_b) / (ms / 1e3) / 1e9
+    return {
+        "workload": f"{len(scs)} independent 2D scenes, grid sides log-uniform 64-256, 1-4 blocks at 4-8 ppc, "
+                    f"2k-64k particles each, E ~ U(1e5, 2e5), nu ~ U(0.15, 0.3)",
+        "scenes": len(scs), "particles": n, "steps": args.batch_steps, "ms": ms,
+        "scenes_per_s": len(scs) / (ms / 1e3),
+        "scene_steps_per_s": len(scs) * args.batch_steps / (ms / 1e3),
+        "particle_updates_per_s": n * args.batch_steps / (ms / 1e3),
+        "scene_step_latency_us": {"p50": float(np.percentile(scene_step_us, 50)),
+                                  "p99": float(np.percentile(scene_step_us, 99))},
+        "batch_step_latency_ms": {"p50": float(np.percentile(one, 50)), "p99": float(np.percentile(one, 99)),
+                                  "calls": len(one)},
+        "config": cfg, "tuner_trial_ms": tune_ms,
+        "hbm": {"algorithmic_bytes_per_particle_step": p2g_b + g2p_b, "achieved_gbs": gbs, "peak": peak,
+                "frac": gbs / peak, "peak_source": peak_src},
+        "sequential_single_solver": {"sample_scenes": len(sample), "ms_per_scene_step": seq_scene_step_ms,
+                                     "estimated_total_s": seq_total_s,
+                                     "batch_speedup": seq_total_s / (ms / 1e3)},
+        "status_flags": flags,
+        "timing": "CUDA events on the batch's stream; one CUDA graph per call",
+    }
+
+
 def cpu_port_time(scene, target_s=12.0, max_steps=20):
     """FP32 OpenMP port of the reference MLS step on all host cores."""
     from oracle import oracle as O
@@ -290,6 +359,10 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=1000)
     ap.add_argument("--mlp-tolerance", type=float, default=1e-3)
     ap.add_argument("--no-mlp", action="store_true", help="skip the learned-plasticity comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes measurement")
+    ap.add_argument("--batch-scenes", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--batch-latency-calls", type=int, default=50)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -402,6 +475,13 @@ def main():
         except Exception as e:  # reported next to the headline, never required for it
             mlp = {"error": str(e)}
 
+    batch = None
+    if world == 1 and not args.no_batch:
+        try:
+            batch = batched_scenes(args, torch)
+        except Exception as e:  # reported next to the headline, never required for it
+            batch = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -427,6 +507,7 @@ def main():
             "status_flags": flags,
             "cpu_baseline": cpu,
             "mlp_vs_plain": mlp,
+            "batched": batch,
         }
         print(json.dumps(line), flush=True)
     solver.close()

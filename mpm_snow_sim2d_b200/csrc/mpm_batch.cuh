@@ -207,6 +207,13 @@ __device__ __forceinline__ void batch_g2p(const BatchBuffers& P, long long N, co
                                           unsigned* status) {
     for (long long i = lo + threadIdx.x; i < hi; i += THREADS) {
         const float x[2] = {P.x[i], P.x[N + i]};
+        // the rest of the particle's state, loaded before the gather so that
+        // its latency overlaps the stencil reads
+        float Fe[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Fe[k] = P.Fe[k * N + i];
+        float Jp = P.Jp[i];
+        const float mass = P.mass[i], vol = P.vol[i];
         const int ext[2] = {C.W, C.H};
         int base[2];
         float wk[2][4], off[2][4];
@@ -265,17 +272,13 @@ __device__ __forceinline__ void batch_g2p(const BatchBuffers& P, long long N, co
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) P.B[k * N + i] = nB[k];
-        float Fe[4], L[4], Fh[4];
+        float L[4], Fh[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            Fe[k] = P.Fe[k * N + i];
-            L[k] = ((k % 3) == 0 ? 1.f : 0.f) + C.dt * (3.f * nB[k]);
-        }
+        for (int k = 0; k < 4; ++k) L[k] = ((k % 3) == 0 ? 1.f : 0.f) + C.dt * (3.f * nB[k]);
         matmul<2>(L, Fe, Fh);
-        float Jp = P.Jp[i];
         plasticity<2, kMLS>(C, Fh, Fe, Jp, status);
         float Anext[4];
-        mls_affine<2>(C, nB, Fe, Jp, P.mass[i], P.vol[i], Anext);
+        mls_affine<2>(C, nB, Fe, Jp, mass, vol, Anext);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             P.Fe[k * N + i] = Fe[k];
