@@ -304,8 +304,25 @@ __device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long lon
     if (D == 2) {
         gv[id] = make_float4(vf[0], vf[1], vc[0], vc[1]);
     } else {
-        gv[2 * id] = make_float4(vf[0], vf[1], vf[2], 0.f);
-        gv[2 * id + 1] = make_float4(vc[0], vc[1], vc[2], 0.f);
+        // vc differs from vf only where a wall plane acted on the node: flag
+        // those in .w and store their vc in the second half of the array, so
+        // that the gather reads one float4 per node elsewhere.
+        const bool hit = vc[0] != vf[0] || vc[1] != vf[1] || vc[2] != vf[2];
+        gv[id] = make_float4(vf[0], vf[1], vf[2], hit ? 1.f : 0.f);
+        if (hit) gv[C.nodes + id] = make_float4(vc[0], vc[1], vc[2], 0.f);
+    }
+}
+
+// 3D node velocities as grid_node stores them: vf, and vc (= vf unless flagged).
+__device__ __forceinline__ void load_node3(const float4* __restrict__ gv, long long nodes, long long cid, float* vf,
+                                           float* vc) {
+    const float4 g = __ldg(&gv[cid]);
+    vf[0] = g.x; vf[1] = g.y; vf[2] = g.z;
+    if (g.w != 0.f) {
+        const float4 h = __ldg(&gv[nodes + cid]);
+        vc[0] = h.x; vc[1] = h.y; vc[2] = h.z;
+    } else {
+        vc[0] = g.x; vc[1] = g.y; vc[2] = g.z;
     }
 }
 
@@ -433,8 +450,7 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
                     const float4 g = gv[cid];
                     vf[0] = g.x; vf[1] = g.y; vc[0] = g.z; vc[1] = g.w;
                 } else {
-                    const float4 g0 = gv[2 * cid], g1 = gv[2 * cid + 1];
-                    vf[0] = g0.x; vf[1] = g0.y; vf[2] = g0.z; vc[0] = g1.x; vc[1] = g1.y; vc[2] = g1.z;
+                    load_node3(gv, C.nodes, cid, vf, vc);
                 }
 #pragma unroll
                 for (int r = 0; r < D; ++r) {
@@ -545,6 +561,7 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
     const long long sy = C.nx, sz = (long long)C.nx * C.ny;
     const long long c0 = (D == 3 ? base[2] * sz : 0) + base[1] * sy + base[0];
     float vc[D];
+    bool wall = false;
 #pragma unroll
     for (int r = 0; r < D; ++r) { nv[r] = 0.f; vc[r] = 0.f; }
 #pragma unroll
@@ -557,15 +574,17 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             if constexpr (D == 3) {
-                float Pv[3] = {0.f, 0.f, 0.f}, Pd[3] = {0.f, 0.f, 0.f}, Pc[3] = {0.f, 0.f, 0.f};
+                // vc = vf at every node the wall planes left alone (flag .w = 0):
+                // the vc sum is then the vf sum; flagged nodes are handled below.
+                float Pv[3] = {0.f, 0.f, 0.f}, Pd[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const long long cid = c0 + a + b * sy + c * sz;
-                    const float4 g0 = __ldg(&gv[2 * cid]), g1 = __ldg(&gv[2 * cid + 1]);
+                    const float4 g = __ldg(&gv[cid]);
+                    wall = wall || g.w != 0.f;
                     const float z = wk[2][c], zd = wd[2][c];
-                    Pv[0] += z * g0.x; Pv[1] += z * g0.y; Pv[2] += z * g0.z;
-                    Pd[0] += zd * g0.x; Pd[1] += zd * g0.y; Pd[2] += zd * g0.z;
-                    Pc[0] += z * g1.x; Pc[1] += z * g1.y; Pc[2] += z * g1.z;
+                    Pv[0] += z * g.x; Pv[1] += z * g.y; Pv[2] += z * g.z;
+                    Pd[0] += zd * g.x; Pd[1] += zd * g.y; Pd[2] += zd * g.z;
                 }
                 const float y = wk[1][b], yd = wd[1][b];
 #pragma unroll
@@ -573,7 +592,6 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
                     Q[r] += y * Pv[r];
                     Qy[r] += yd * Pv[r];
                     Qz[r] += y * Pd[r];
-                    Qc[r] += y * Pc[r];
                 }
             } else {
                 const long long cid = c0 + a + b * sy;
@@ -592,7 +610,37 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
             nB[r * D + 0] += xd * Q[r];
             nB[r * D + 1] += x * Qy[r];
             if (D == 3) nB[r * D + 2] += x * Qz[r];
-            vc[r] += x * Qc[r];
+            else vc[r] += x * Qc[r];
+        }
+    }
+    if constexpr (D == 3) {
+        if (!wall) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) vc[r] = nv[r];
+        } else {
+            // a stencil node was moved by a wall plane: the vc sum, in the same
+            // order as the vf sum above
+#pragma unroll 1
+            for (int a = 0; a < 4; ++a) {
+                float Qc[3] = {0.f, 0.f, 0.f};
+#pragma unroll 1
+                for (int b = 0; b < 4; ++b) {
+                    float Pc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        float f[3], g[3];
+                        load_node3(gv, C.nodes, c0 + a + b * sy + c * sz, f, g);
+                        const float z = wk[2][c];
+                        Pc[0] += z * g[0]; Pc[1] += z * g[1]; Pc[2] += z * g[2];
+                    }
+                    const float y = wk[1][b];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) Qc[r] += y * Pc[r];
+                }
+                const float x = wk[0][a];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) vc[r] += x * Qc[r];
+            }
         }
     }
     // sum w (x_i - x_p) per axis is separable: (sum wd_k) prod_{l != k} (sum w_l)
@@ -643,8 +691,7 @@ __device__ __forceinline__ float gather_clipped(const StepConsts& C, const float
                     const float4 g = __ldg(&gv[cid]);
                     vf[0] = g.x; vf[1] = g.y; vc[0] = g.z; vc[1] = g.w;
                 } else {
-                    const float4 g0 = __ldg(&gv[2 * cid]), g1 = __ldg(&gv[2 * cid + 1]);
-                    vf[0] = g0.x; vf[1] = g0.y; vf[2] = g0.z; vc[0] = g1.x; vc[1] = g1.y; vc[2] = g1.z;
+                    load_node3(gv, C.nodes, cid, vf, vc);
                 }
                 for (int r = 0; r < D; ++r) {
                     const float wv = w * vf[r];
