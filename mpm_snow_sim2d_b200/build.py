@@ -41,7 +41,7 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     """Compile the CUDA library if any source or header is newer than it."""
-    deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted((INCLUDE / "mpm").glob("*.h"))
+    deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted((INCLUDE / "mpm").glob("*.h"))
     if not force and not _stale(LIB, deps):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")

@@ -653,7 +653,15 @@ namespace mpm {
 //   3D (28): wx[4] | wy[4] | wz[4] | fx fy fz m | mv0 mv1 mv2 A00 | A01 A02 A10 A11 | A12 A20 A21 A22
 //   2D (20): wx[4] | wy[4] | fx fy m mv0 | mv1 A00 A01 A10 | A11 pad pad pad
 template <int D> struct WarpGeom;
-template <> struct WarpGeom<3> { static constexpr int CHUNK = 40, SPLIT = 4, PS = 28; };
+#ifndef MPM_P2G_CHUNK3
+#define MPM_P2G_CHUNK3 48
+#endif
+#ifndef MPM_P2G_SPLIT3
+#define MPM_P2G_SPLIT3 8
+#endif
+// 3D: SPLIT threads per run, each holding 16 * 4 / SPLIT nodes (x-offset a,
+// and 16 / SPLIT of the y-offsets) x 4 channels.
+template <> struct WarpGeom<3> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 28; };
 template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
 constexpr int kP2GWarps = 8;
 
@@ -746,13 +754,16 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                 kk /= (extk + 18);
             }
             if constexpr (D == 3) {
-                float am[16], a0[16], a1[16], a2[16];
+                constexpr int NB = 16 / W::SPLIT;  // y-offsets per thread
+                constexpr int NN = NB * 4;         // nodes per thread
+                const int ax = a % 4, by0 = (a / 4) * NB;
+                float am[NN], a0[NN], a1[NN], a2[NN];
 #pragma unroll
-                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
-                const float da = float(a - 1);
+                for (int k = 0; k < NN; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
+                const float da = float(ax - 1);
                 for (int j = j0; j < j1; ++j) {
                     const float4* pp = pay + j * (W::PS / 4);
-                    const float alpha = payf[j * W::PS + a];
+                    const float alpha = payf[j * W::PS + ax];
                     const float4 wy = pp[1], wz = pp[2], fm = pp[3], p4 = pp[4], p5 = pp[5], p6 = pp[6];
                     // A = (p4.w p5.x p5.y | p5.z p5.w p6.x | p6.y p6.z p6.w)
                     const float beta = alpha * (da - fm.x);
@@ -768,13 +779,15 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
 #pragma unroll
                     for (int cc = 0; cc < 4; ++cc) Zd[cc] = Z[cc] * (float(cc - 1) - fm.z);
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const float Y = Yv[b], Yd = Y * (float(b - 1) - fm.y);
+                    for (int bb = 0; bb < NB; ++bb) {
+                        const int b = by0 + bb;
+                        const float Y = NB == 4 ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
+                        const float Yd = Y * (float(b - 1) - fm.y);
                         const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
                         const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) {
-                            const int idx = b * 4 + cc;
+                            const int idx = bb * 4 + cc;
                             am[idx] += mY * Z[cc];
                             a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
                             a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
@@ -784,24 +797,24 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                 }
                 float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
-                for (int k = 0; k < 16; ++k) {
+                for (int k = 0; k < NN; ++k) {
                     mx_m = fmaxf(mx_m, fabsf(am[k]));
                     mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fmaxf(fabsf(a1[k]), fabsf(a2[k]))));
                 }
                 if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
                     raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
-                const int gx = cell[0] - 1 + a;
+                const int gx = cell[0] - 1 + ax;
                 const bool inside = gx >= 0 && gx <= C.W && cell[1] >= 1 && cell[1] + 2 <= C.H && cell[2] >= 1 &&
                                     cell[2] + 2 <= C.Dp;
                 if (inside) {
-                    const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1)) * C.nx + gx;
+                    const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1 + by0)) * C.nx + gx;
                     const long long sy = C.nx, sz = (long long)C.nx * C.ny;
 #pragma unroll
-                    for (int b = 0; b < 4; ++b)
+                    for (int bb = 0; bb < NB; ++bb)
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) {
-                            const int idx = b * 4 + cc;
-                            unsigned long long* p0 = acc + (g0 + b * sy + cc * sz);
+                            const int idx = bb * 4 + cc;
+                            unsigned long long* p0 = acc + (g0 + bb * sy + cc * sz);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
                             red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
@@ -809,11 +822,11 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                         }
                 } else {
                     bool outside = false;
-                    for (int b = 0; b < 4; ++b)
+                    for (int bb = 0; bb < NB; ++bb)
                         for (int cc = 0; cc < 4; ++cc) {
-                            const int gy = cell[1] - 1 + b, gz = cell[2] - 1 + cc;
+                            const int gy = cell[1] - 1 + by0 + bb, gz = cell[2] - 1 + cc;
                             if (gx < 0 || gx > C.W || gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
-                            const int idx = b * 4 + cc;
+                            const int idx = bb * 4 + cc;
                             unsigned long long* p0 = acc + (((long long)gz * C.ny + gy) * C.nx + gx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -823,8 +836,8 @@ __global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepCo
                     if (outside) raise_flag(status, 4u);
                 }
                 if (gx >= 0 && gx <= C.W) {
-                    // node blocks holding the unit's in-grid nodes (empty range: none)
-                    const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
+                    // node blocks holding the thread's in-grid nodes (empty range: none)
+                    const int y0 = max(0, cell[1] - 1 + by0), y1 = min(C.H, cell[1] - 2 + by0 + NB);
                     const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + 2);
                     if (y0 <= y1 && z0 <= z1)
                         for (int bz = z0 / T; bz <= z1 / T; ++bz)
