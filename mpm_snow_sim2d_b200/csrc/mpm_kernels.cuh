@@ -714,7 +714,10 @@ __device__ __forceinline__ int queue_slot(const SlowQueue& Q) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(256, 2) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+#ifndef MPM_G2P_MIN_BLOCKS
+#define MPM_G2P_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                        SlowQueue Q, unsigned* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;

@@ -682,7 +682,10 @@ __device__ __forceinline__ void red_fixed(unsigned long long* p, float v, float 
 }
 
 template <int D>
-__global__ void __launch_bounds__(kP2GWarps * 32) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
+#ifndef MPM_P2G_MIN_BLOCKS
+#define MPM_P2G_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kP2GWarps * 32, MPM_P2G_MIN_BLOCKS) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
                                                               unsigned long long* __restrict__ acc,
                                                               unsigned* __restrict__ status) {
     using W = WarpGeom<D>;
