@@ -1,16 +1,18 @@
 """Run a named workload for a number of steps through the C ABI.
 
     python -m mpm_snow_sim2d_b200.run c3 --steps 4
+    python -m mpm_snow_sim2d_b200.run impact64 --steps 100 --plasticity mlp
 
 Prints the particle count, the device status word and the wall time; used for
-profiling captures and quick checks. Workloads: see scenes.workload().
+profiling captures and quick checks. Workloads: see scenes.workload(); "impact64" is the training set-up of the
+learned return map (a 6 m/s snowball impact on a slab, 64^3).
 """
 from __future__ import annotations
 
 import argparse
 import time
 
-from . import Solver, scenes
+from . import Solver, _lib, scenes
 
 
 def main(argv=None) -> int:
@@ -18,15 +20,26 @@ def main(argv=None) -> int:
     ap.add_argument("workload")
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--sort-period", type=int, default=0)
+    ap.add_argument("--plasticity", choices=["exact", "mlp"], default="exact")
     args = ap.parse_args(argv)
-    scene = scenes.workload(args.workload)
+    if args.workload == "impact64":
+        from .mlp_train import impact_scene
+        scene = impact_scene(6.0, seed=777002, W=64, steps=args.steps)
+    else:
+        scene = scenes.workload(args.workload)
     with Solver.from_scene(scene, sort_period=args.sort_period) as s:
+        if args.plasticity == "mlp":
+            from .mlp import DEFAULT_WEIGHTS, Mlp
+            net = Mlp.load(DEFAULT_WEIGHTS)
+            s.set_plasticity(_lib.PLASTIC_MLP, net, 1e-3)
         t0 = time.perf_counter()
         s.Step(args.steps)
         pos = s.GetParticlePositions()  # synchronises
         dt = time.perf_counter() - t0
         print(f"{scene.name}: {scene.count} particles, {args.steps} steps, status {s.status()}, "
               f"{dt * 1e3:.1f} ms, first position {pos[0].tolist()}")
+        if args.plasticity == "mlp":
+            print("learned return map: accepted %d, fell back %d" % s.mlp_stats())
     return 0
 
 
