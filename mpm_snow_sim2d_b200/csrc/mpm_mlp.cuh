@@ -528,9 +528,12 @@ __global__ void __launch_bounds__(kMlpWarps * 32) k_return_map_mlp(Particles P, 
                                                                    MlpParams ML) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MlpWarpSmem& S = *reinterpret_cast<MlpWarpSmem*>(smem_raw);
+    const int m = *Q.count;
+    // CTAs past the queue's end leave before staging the weights (the grid is
+    // sized for the largest queue; most steps queue far fewer particles)
+    if ((long long)blockIdx.x * kMlpWarps * 32 >= m) return;
     mlp_stage_weights(S, ML.wbf, ML.wf32);
     __syncthreads();
-    const int m = *Q.count;
     const int n = P.n;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     __nv_bfloat16* X = S.x[wid];
@@ -542,12 +545,18 @@ __global__ void __launch_bounds__(kMlpWarps * 32) k_return_map_mlp(Particles P, 
         const int e = base + lane;
         const int entry = e < m ? Q.list[e] : -1;
         const bool valid = entry >= 0;
-        float Fh[9], Jp0 = 1.f;
+        float Fh[9], Jp0 = 1.f, B[9], mass = 0.f, vol = 0.f;
         float in[kMlpIn];
         if (valid) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) Fh[k] = Q.fh[k * Q.capacity + e];
             Jp0 = P.Jp[entry];
+            // the particle's B, mass and volume, loaded now so that their
+            // latency overlaps the network
+#pragma unroll
+            for (int k = 0; k < 9; ++k) B[k] = P.B[k * n + entry];
+            mass = P.mass ? P.mass[entry] : P.mass_u;
+            vol = P.vol ? P.vol[entry] : P.vol_u;
             mlp_features(Fh, Jp0, ML.norm, in);
         }
         uint32_t* xr = reinterpret_cast<uint32_t*>(X + lane * kMwIn);
@@ -578,11 +587,10 @@ __global__ void __launch_bounds__(kMlpWarps * 32) k_return_map_mlp(Particles P, 
             const float Jp = Jp0 * ratio;
             if (ok) ok = hardened_stress_series<3>(Fp, Jp, C.mu0, C.la0, C.xi, sig);
             if (ok) {
-                const float mass = P.mass ? P.mass[entry] : P.mass_u, vol = P.vol ? P.vol[entry] : P.vol_u;
 #pragma unroll
                 for (int k = 0; k < 9; ++k) {
                     P.Fe[k * n + entry] = Fp[k];
-                    P.A[k * n + entry] = 3.f * mass * P.B[k * n + entry] - 3.f * C.dt * vol * sig[k];
+                    P.A[k * n + entry] = 3.f * mass * B[k] - 3.f * C.dt * vol * sig[k];
                 }
                 P.Jp[entry] = Jp;
                 Q.list[e] = kQueueDone;
