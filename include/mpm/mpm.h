@@ -285,7 +285,7 @@ struct mpm_batch;
 typedef struct mpm_batch mpm_batch;
 
 typedef struct mpm_batch_config {
-    int32_t threads;           /* threads per CTA: 256 or 512 */
+    int32_t threads;           /* threads per CTA: 256, 512 or 1024 */
     int32_t particles_per_cta; /* spread a scene over more CTAs while it has more particles per CTA than this
                                   (0: only as many CTAs as its grid needs) */
     int32_t max_cluster;       /* largest cluster: 1, 2, 4 or 8 */
@@ -315,7 +315,8 @@ MPM_API mpm_status mpm_batch_step_times(mpm_batch* batch, uint64_t* out, size_t 
 MPM_API mpm_status mpm_batch_get_config(const mpm_batch* batch, mpm_batch_config* config);
 MPM_API mpm_status mpm_batch_set_config(mpm_batch* batch, const mpm_batch_config* config);
 /* Autotuner: times trial_steps steps of the batch under each candidate
- * configuration (threads x particles per CTA), keeps the fastest, and restores
+ * configuration (threads {256, 512, 1024} x particles per CTA {grid-limited,
+ * 16k, 8k, 4k}), keeps the fastest, and restores
  * the particle state, so the batch continues as if untuned. *best_ms gets the
  * chosen configuration's time for the trial. Synchronises. */
 MPM_API mpm_status mpm_batch_tune(mpm_batch* batch, int32_t trial_steps, mpm_batch_config* chosen, double* best_ms);

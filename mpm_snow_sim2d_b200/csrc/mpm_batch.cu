@@ -115,7 +115,9 @@ void release(mpm_batch* b) {
 
 using BatchKernel = void (*)(BatchParticles, BatchRun);
 
-BatchKernel kernel_for(int threads) { return threads == 512 ? k_batch_run<512> : k_batch_run<256>; }
+BatchKernel kernel_for(int threads) {
+    return threads == 1024 ? k_batch_run<1024> : threads == 512 ? k_batch_run<512> : k_batch_run<256>;
+}
 
 BatchParticles particles(const mpm_batch* b) { return BatchParticles{{b->buf[0], b->buf[1]}, b->N}; }
 
@@ -156,7 +158,8 @@ cudaLaunchConfig_t launch_config(const mpm_batch* b, const BatchClass& k, cudaLa
 // Cluster size and node band of every scene under b->cfg; scenes grouped by
 // cluster size, most particles per CTA first; persistent cluster counts.
 mpm_status configure(mpm_batch* b, const mpm_batch_config& cfg) {
-    if (cfg.threads != 256 && cfg.threads != 512) return bfail(b, MPM_ERR_INVALID_ARGUMENT, "threads must be 256 or 512");
+    if (cfg.threads != 256 && cfg.threads != 512 && cfg.threads != 1024)
+        return bfail(b, MPM_ERR_INVALID_ARGUMENT, "threads must be 256, 512 or 1024");
     if (cfg.max_cluster != 1 && cfg.max_cluster != 2 && cfg.max_cluster != 4 && cfg.max_cluster != 8)
         return bfail(b, MPM_ERR_INVALID_ARGUMENT, "max_cluster must be 1, 2, 4 or 8");
     if (cfg.particles_per_cta < 0) return bfail(b, MPM_ERR_INVALID_ARGUMENT, "particles_per_cta must be >= 0");
@@ -643,9 +646,9 @@ mpm_status mpm_batch_tune(mpm_batch* b, int32_t trial_steps, mpm_batch_config* c
     cudaError_t ce = copy_all(true);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
-    const int threads_c[2] = {256, 512};
+    const int threads_c[3] = {256, 512, 1024};
     const int ppc_c[4] = {0, 16384, 8192, 4096};
-    for (int ti = 0; ti < 2 && ce == cudaSuccess && st == MPM_OK; ++ti)
+    for (int ti = 0; ti < 3 && ce == cudaSuccess && st == MPM_OK; ++ti)
         for (int pi = 0; pi < 4 && ce == cudaSuccess && st == MPM_OK; ++pi) {
             mpm_batch_config cfg = start;
             cfg.threads = threads_c[ti];

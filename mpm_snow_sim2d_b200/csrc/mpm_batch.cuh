@@ -100,6 +100,8 @@ __device__ __forceinline__ uint32_t cluster_map(uint32_t addr, uint32_t rank) {
     return r;
 }
 
+// Each shared::cluster access carries a "memory" clobber so that the compiler
+// keeps it on its side of the cluster barriers (which order the phases).
 __device__ __forceinline__ void cluster_red_add(uint32_t addr, long long v) {
     if (v != 0)
         asm volatile("red.relaxed.cluster.shared::cluster.add.u64 [%0], %1;" ::"r"(addr), "l"((unsigned long long)v)

@@ -69,31 +69,45 @@ def test_batch_scenes_match_oracle_and_single_solver(gpu_lib, oracle_mod):
 
 
 def test_scene_result_independent_of_cluster_and_partners(gpu_lib):
+    """Bitwise, for each kernel width: the int64 sums are exact and every
+    particle's arithmetic is its own, so neither the cluster size, nor the
+    particle order, nor the other scenes change a scene's result. (Kernels of
+    different widths are compiled under different register limits and may
+    contract multiply-adds differently: equal within FP32 rounding.)"""
     from mpm_snow_sim2d_b200.batch import Batch
     scs = _mixed_scenes(k=6, steps=40)
-    with Batch(scs) as b:
-        b.set_config(particles_per_cta=0, threads=256)
-        b.step(40)
-        base = _states(b, len(scs))
-    with Batch(scs) as b:
-        b.set_config(particles_per_cta=1024, threads=512)  # every scene on more CTAs
-        b.step(25)
-        b.step(15)
-        spread = _states(b, len(scs))
+    per_width = {}
+    for threads in (512, 1024):
+        with Batch(scs) as b:
+            b.set_config(particles_per_cta=0, threads=threads)
+            b.step(40)
+            base = _states(b, len(scs))
+        with Batch(scs) as b:
+            b.set_config(particles_per_cta=1024, threads=threads)  # every scene on more CTAs
+            b.step(25)
+            b.step(15)
+            spread = _states(b, len(scs))
+        for s in range(len(scs)):
+            assert _equal(base[s], spread[s]), f"scene {s} changed with its cluster size ({threads} threads)"
+        with Batch([scs[-1]]) as b:  # the largest scene alone
+            b.set_config(threads=threads)
+            b.step(40)
+            alone = b.get_state(0)
+        assert _equal(alone, base[-1])
+        per_width[threads] = base
     for s in range(len(scs)):
-        assert _equal(base[s], spread[s]), f"scene {s} changed with its cluster size"
-    with Batch([scs[-1]]) as b:  # the largest scene alone
-        b.step(40)
-        alone = b.get_state(0)
-    assert _equal(alone, base[-1])
+        errs = state_errors(per_width[1024][s], _as_ref(per_width[512][s]), 2)
+        _check(errs, dict(x=1e-6, v=1e-5, B=1e-5, F=1e-6, Jp=1e-6), f"scene {s}, 1024 vs 512 threads")
 
 
-def test_batch_determinism_and_state_roundtrip(gpu_lib):
+@pytest.mark.parametrize("threads", [512, 1024])
+def test_batch_determinism_and_state_roundtrip(gpu_lib, threads):
     from mpm_snow_sim2d_b200.batch import Batch
     scs = _mixed_scenes(k=4, steps=30)
     runs = []
     for rt in range(2):
         with Batch(scs) as b:
+            b.set_config(threads=threads)
             b.step(10)
             if rt:
                 for s in range(len(scs)):  # upload what was read: continues unchanged
@@ -109,14 +123,19 @@ def test_autotuner_keeps_the_state(gpu_lib):
     from mpm_snow_sim2d_b200.batch import Batch
     scs = _mixed_scenes(k=6, steps=20)
     with Batch(scs) as b:
-        b.step(20)
-        ref = _states(b, len(scs))
-    with Batch(scs) as b:
+        before = _states(b, len(scs))
         cfg, ms = b.tune(3)
-        assert cfg["threads"] in (256, 512) and ms > 0
+        assert cfg["threads"] in (256, 512, 1024) and ms > 0
         assert b.config == cfg
+        after = _states(b, len(scs))
         b.step(20)
         got = _states(b, len(scs))
+    for s in range(len(scs)):
+        assert _equal(before[s], after[s]), f"scene {s}: the tuner left its trial steps behind"
+    with Batch(scs) as b:  # the chosen configuration from the start: same run, bitwise
+        b.set_config(**cfg)
+        b.step(20)
+        ref = _states(b, len(scs))
     for s in range(len(scs)):
         assert _equal(ref[s], got[s]), f"scene {s}"
 
