@@ -233,7 +233,7 @@ template <int D> __device__ __forceinline__ void mark_stencil_blocks(const TileI
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        lo[k] = max(0, base[k]) / T;
+        lo[k] = min(max(0, base[k]) / T, TI.nblk[k] - 1);
         hi[k] = min(TI.nblk[k] * T - 1, max(0, base[k] + 3)) / T;
     }
     for (int bz = lo[2]; bz <= hi[2]; ++bz)
@@ -685,7 +685,7 @@ template <int D>
 #ifndef MPM_P2G_MIN_BLOCKS
 #define MPM_P2G_MIN_BLOCKS 3
 #endif
-__global__ void __launch_bounds__(kP2GWarps * 32, MPM_P2G_MIN_BLOCKS) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
+__global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 2) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
                                                               unsigned long long* __restrict__ acc,
                                                               unsigned* __restrict__ status) {
     using W = WarpGeom<D>;
