@@ -2,10 +2,12 @@
 
     python -m mpm_snow_sim2d_b200.run c3 --steps 4
     python -m mpm_snow_sim2d_b200.run impact64 --steps 100 --plasticity mlp
+    python -m mpm_snow_sim2d_b200.run c4 --scenes 64 --steps 10 --batch-threads 1024
 
 Prints the particle count, the device status word and the wall time; used for
 profiling captures and quick checks. Workloads: see scenes.workload(); "impact64" is the training set-up of the
-learned return map (a 6 m/s snowball impact on a slab, 64^3).
+learned return map (a 6 m/s snowball impact on a slab, 64^3); "c4" the first
+`--scenes` scenes of the batched workload, run as one batch.
 """
 from __future__ import annotations
 
@@ -21,7 +23,23 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--sort-period", type=int, default=0)
     ap.add_argument("--plasticity", choices=["exact", "mlp"], default="exact")
+    ap.add_argument("--scenes", type=int, default=256, help="c4: scenes in the batch")
+    ap.add_argument("--batch-threads", type=int, default=1024, help="c4: threads per CTA")
     args = ap.parse_args(argv)
+    if args.workload == "c4":
+        from .batch import Batch
+        scs = scenes.batch_scenes_2d(args.scenes)
+        with Batch(scs) as b:
+            b.set_config(threads=args.batch_threads, particles_per_cta=16384)
+            t0 = time.perf_counter()
+            b.step(args.steps)
+            flags = 0
+            for k in range(len(scs)):
+                flags |= b.status(k)  # synchronises
+            dt = time.perf_counter() - t0
+            print(f"c4: {len(scs)} scenes, {b.total_particles} particles, {args.steps} steps, status {flags}, "
+                  f"{dt * 1e3:.1f} ms, config {b.config}")
+        return 0
     if args.workload == "impact64":
         from .mlp_train import impact_scene
         scene = impact_scene(6.0, seed=777002, W=64, steps=args.steps)
