@@ -44,6 +44,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "particle-updates/s (P2G+grid+G2P), plain vs MLP-plasticity, 1 B200, % HBM peak"
 UNIT = "particle-updates/s"
 DEFAULT_SORT_PERIOD = 16  # the solver's re-sort interval when mpm_params.sort_period is 0
+# DRAM bytes (read + write) per launch of the dominant kernels, from one full
+# ncu capture of the same scene (dram__bytes_read.sum + dram__bytes_write.sum).
+NCU_TRAFFIC = {("c3", "p2g"): 113.1e6, ("c3", "g2p"): 254.4e6}
 
 # Algorithmic bytes (minimal FP32 SoA state, uniform mass/volume).
 # Per particle-step: P2G reads x, v, B, F_E, J_p; G2P reads x, F_E, J_p and
@@ -463,7 +466,7 @@ def main():
     step_bytes = sum(alg.values())
     step_ms = ms / args.steps
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                "frac": achieved / peak, "traffic": NCU_TRAFFIC.get((args.workload, dom)), "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg[dom],
                 "step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
                          "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
