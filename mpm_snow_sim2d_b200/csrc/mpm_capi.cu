@@ -64,11 +64,8 @@ struct mpm_solver {
     bool needs_sort = true;
     int sort_period = 8;
     int sms = 148;
-    int p2g_grid = 0;
     TileInfo ti{};
     SortBuffers alt{};
-    bool p2g_direct = false;  // P2G flush per unit to global (else via a shared tile)
-    int p2g_mode = 2;         // 2: warp chunks (default); else tile items
     int p2g_warp_grid = 0;
     // CUDA graphs of one sort period (sort + sort_period steps), one per
     // buffer parity (the sort swaps the particle buffers).
@@ -141,13 +138,11 @@ void release(mpm_solver* s) {
     for (float* p : al)
         if (p) cudaFree(p);
     if (s->alt.id) cudaFree(s->alt.id);
-    int* ti[] = {s->ti.key, s->ti.tile_count, s->ti.tile_cursor, s->ti.tile_start, s->ti.n_items, s->ti.mark,
-                 s->ti.mark_list, s->ti.n_marked, s->ti.n_orphans, s->ti.perm, s->ti.tile_list, s->ti.n_tile_list,
-                 s->ti.sval};
+    int* ti[] = {s->ti.key,      s->ti.tile_count, s->ti.tile_cursor, s->ti.tile_start, s->ti.mark, s->ti.mark_list,
+                 s->ti.n_marked, s->ti.perm,       s->ti.tile_list,   s->ti.n_tile_list, s->ti.sval};
     if (s->ti.skey) cudaFree(s->ti.skey);
     for (int* p : ti)
         if (p) cudaFree(p);
-    if (s->ti.items) cudaFree(s->ti.items);
     for (auto& g : s->period_graph)
         if (g) cudaGraphExecDestroy(g);
     if (s->mlp_counters) cudaFree(s->mlp_counters);
@@ -213,7 +208,7 @@ void invalidate_graphs(mpm_solver* s) {
 }
 
 template <int D> cudaError_t launch_sort(mpm_solver* s) {
-    if (s->n == 0) { s->needs_sort = false; return cudaMemsetAsync(s->ti.n_items, 0, sizeof(int), s->stream); }
+    if (s->n == 0) { s->needs_sort = false; return cudaSuccess; }
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
     k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
     k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
@@ -227,17 +222,8 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
 }
 
 template <int D> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
-    if (s->p2g_mode == 2) {
-        k_p2g_warp<D><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D>), s->stream>>>(particle_view(s), s->C,
-                                                                                              s->ti, s->acc, s->status);
-        return cudaGetLastError();
-    }
-    if (s->p2g_direct)
-        k_p2g_tiled<D, true><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D, true>), s->stream>>>(
-            particle_view(s), s->C, s->ti, s->acc, s->status);
-    else
-        k_p2g_tiled<D, false><<<s->p2g_grid, kTileThreads, sizeof(P2GSmem<D, false>), s->stream>>>(
-            particle_view(s), s->C, s->ti, s->acc, s->status);
+    k_p2g_warp<D><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D>), s->stream>>>(particle_view(s), s->C,
+                                                                                          s->ti, s->acc, s->status);
     return cudaGetLastError();
 }
 
@@ -345,21 +331,8 @@ cudaError_t clear_after_p2g(mpm_solver* s) {
     return cudaMemsetAsync(s->acc, 0, sizeof(unsigned long long) * nacc(s->dim, s->form) * s->nodes, s->stream);
 }
 
-template <int D> cudaError_t p2g_occupancy(bool direct, int* per_sm) {
-    cudaError_t e;
-    if (direct) {
-        const size_t smem = sizeof(P2GSmem<D, true>);
-        e = cudaFuncSetAttribute(k_p2g_tiled<D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_p2g_tiled<D, true>, kTileThreads, smem);
-    } else {
-        const size_t smem = sizeof(P2GSmem<D, false>);
-        e = cudaFuncSetAttribute(k_p2g_tiled<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_p2g_tiled<D, false>, kTileThreads, smem);
-    }
-    return e;
-}
 
-// Tiles, work items, node-block marks and the sort's alternate buffers.
+// Tiles, node-block marks and the sort's alternate buffers.
 mpm_status setup_tiled(mpm_solver* s) {
     const int D = s->dim, n = s->n;
     const int T = D == 3 ? TileGeom<3>::T : TileGeom<2>::T;
@@ -374,11 +347,10 @@ mpm_status setup_tiled(mpm_solver* s) {
         ti.n_tiles *= ti.tiles[k];
         ti.n_blocks *= ti.nblk[k];
     }
-    const size_t max_items = (size_t)n / kItem + ti.n_tiles + 1;
     if (dalloc(&ti.key, (size_t)n) || dalloc(&ti.tile_count, (size_t)ti.n_tiles) ||
         dalloc(&ti.tile_cursor, (size_t)ti.n_tiles) || dalloc(&ti.tile_start, (size_t)ti.n_tiles) ||
-        dalloc(&ti.items, max_items) || dalloc(&ti.n_items, 1) || dalloc(&ti.mark, (size_t)ti.n_blocks) ||
-        dalloc(&ti.mark_list, (size_t)ti.n_blocks) || dalloc(&ti.n_marked, 1) || dalloc(&ti.n_orphans, 1) ||
+        dalloc(&ti.mark, (size_t)ti.n_blocks) || dalloc(&ti.mark_list, (size_t)ti.n_blocks) ||
+        dalloc(&ti.n_marked, 1) ||
         dalloc(&ti.perm, (size_t)n) || dalloc(&ti.tile_list, (size_t)ti.n_tiles) || dalloc(&ti.n_tile_list, 1) ||
         dalloc(&ti.skey, (size_t)n) || dalloc(&ti.sval, (size_t)n) ||
         dalloc(&s->alt.x, (size_t)n * D) || dalloc(&s->alt.v, (size_t)n * D) || dalloc(&s->alt.B, (size_t)n * D * D) ||
@@ -391,19 +363,13 @@ mpm_status setup_tiled(mpm_solver* s) {
     if (s->vol && dalloc(&s->alt.vol, (size_t)n)) return MPM_ERR_OUT_OF_MEMORY;
     bool ok = cudaMemset(ti.tile_count, 0, sizeof(int) * ti.n_tiles) == cudaSuccess &&
               cudaMemset(ti.tile_cursor, 0, sizeof(int) * ti.n_tiles) == cudaSuccess &&
-              cudaMemset(ti.n_items, 0, sizeof(int)) == cudaSuccess &&
               cudaMemset(ti.mark, 0, sizeof(int) * ti.n_blocks) == cudaSuccess &&
-              cudaMemset(ti.n_marked, 0, sizeof(int)) == cudaSuccess &&
-              cudaMemset(ti.n_orphans, 0, sizeof(int)) == cudaSuccess;
+              cudaMemset(ti.n_marked, 0, sizeof(int)) == cudaSuccess;
     if (!ok) return MPM_ERR_CUDA;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     s->sms = sms > 0 ? sms : 148;
-    const char* env = std::getenv("MPM_P2G_DIRECT");
-    s->p2g_direct = env && env[0] == '1';
-    const char* envm = std::getenv("MPM_P2G_MODE");
-    s->p2g_mode = envm ? std::atoi(envm) : 2;
     {
         const size_t wsm = D == 3 ? sizeof(P2GWarpSmem<3>) : sizeof(P2GWarpSmem<2>);
         cudaError_t ew = D == 3 ? cudaFuncSetAttribute(k_p2g_warp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm)
@@ -415,12 +381,6 @@ mpm_status setup_tiled(mpm_solver* s) {
         if (ew != cudaSuccess || per < 1) return MPM_ERR_CUDA;
         s->p2g_warp_grid = s->sms * per;
     }
-    int per_sm = 0;
-    cudaError_t e = cudaSuccess;
-    if (D == 3) e = p2g_occupancy<3>(s->p2g_direct, &per_sm);
-    else e = p2g_occupancy<2>(s->p2g_direct, &per_sm);
-    if (e != cudaSuccess || per_sm < 1) return MPM_ERR_CUDA;
-    s->p2g_grid = s->sms * per_sm;
     s->q.capacity = n > 0 ? n : 1;
     if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 1) ||
         dalloc(&s->q.fh, (size_t)s->q.capacity * D * D)) {
@@ -872,10 +832,10 @@ mpm_status mpm_get_fixed_point(const mpm_solver* s, int32_t* lm, int32_t* lp) {
 
 // Checkpoint: "MPMS" | u32 version=2 | i32 dim | i64 count | i32 W, H, D |
 // u64 params hash | i64 step | f32 x[n*d] v[n*d] B[n*d*d] Fe[n*d*d] Jp[n]
-// (creation order) | u32 has_order | [i32 slot_id[n] | i32 n_items |
-// i32x4 items[n_items]]. The slot order and work items of the tiled path are
-// saved so that a resumed run groups particles exactly as the original did and
-// continues bit-identically.
+// (creation order) | u32 has_order | [i32 slot_id[n] | i32 n_extra |
+// i32x4 extra[n_extra]]. The slot order of the tiled path is saved so that a
+// resumed run groups particles exactly as the original did and continues
+// bit-identically. `extra` is reserved (written empty, skipped on load).
 mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
     const int D = s->dim;
@@ -886,16 +846,11 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (r != MPM_OK) return r;
     const uint32_t has_order = (s->tiled && !s->needs_sort) ? 1u : 0u;
     std::vector<int> ids;
-    std::vector<int4> items;
-    int n_items = 0;
+    const int32_t n_extra = 0;
     if (has_order) {
         ids.resize(n);
         MPM_CUDA(s, cudaMemcpyAsync(ids.data(), s->id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
-        MPM_CUDA(s, cudaMemcpyAsync(&n_items, s->ti.n_items, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
         MPM_CUDA(s, cudaStreamSynchronize(s->stream));
-        items.resize(n_items);
-        if (n_items > 0)
-            MPM_CUDA(s, cudaMemcpy(items.data(), s->ti.items, sizeof(int4) * n_items, cudaMemcpyDeviceToHost));
     }
     FILE* f = std::fopen(path, "wb");
     if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
@@ -910,8 +865,7 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
         ok = ok && std::fwrite(vec->data(), sizeof(float), vec->size(), f) == vec->size();
     ok = ok && std::fwrite(&has_order, 4, 1, f) == 1;
     if (has_order) {
-        ok = ok && std::fwrite(ids.data(), sizeof(int), n, f) == n && std::fwrite(&n_items, 4, 1, f) == 1 &&
-             std::fwrite(items.data(), sizeof(int4), items.size(), f) == items.size();
+        ok = ok && std::fwrite(ids.data(), sizeof(int), n, f) == n && std::fwrite(&n_extra, 4, 1, f) == 1;
     }
     ok = (std::fclose(f) == 0) && ok;
     return ok ? MPM_OK : fail(s, MPM_ERR_IO, "short write");
@@ -941,27 +895,23 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     for (auto* vec : {&x, &v, &B, &Fe, &Jp}) ok = ok && std::fread(vec->data(), sizeof(float), vec->size(), f) == vec->size();
     uint32_t has_order = 0;
     std::vector<int> ids;
-    std::vector<int4> items;
-    int n_items = 0;
+    int n_extra = 0;
     if (ok && ver == 2) {
         ok = std::fread(&has_order, 4, 1, f) == 1;
         if (ok && has_order) {
             ids.resize(n);
-            ok = std::fread(ids.data(), sizeof(int), n, f) == n && std::fread(&n_items, 4, 1, f) == 1 && n_items >= 0 &&
-                 (size_t)n_items <= n / kItem + (size_t)s->ti.n_tiles + 1;
+            ok = std::fread(ids.data(), sizeof(int), n, f) == n && std::fread(&n_extra, 4, 1, f) == 1 && n_extra >= 0 &&
+                 (size_t)n_extra <= n + (size_t)s->ti.n_tiles + 1;
             if (ok) {
-                items.resize(n_items);
-                ok = std::fread(items.data(), sizeof(int4), items.size(), f) == items.size();
+                std::vector<int4> extra(n_extra);
+                ok = std::fread(extra.data(), sizeof(int4), extra.size(), f) == extra.size();
             }
-            // every slot must name a distinct particle and every item a slot range
+            // every slot must name a distinct particle
             std::vector<char> seen(ok ? n : 0, 0);
             for (size_t i = 0; ok && i < n; ++i) {
                 ok = ids[i] >= 0 && (size_t)ids[i] < n && !seen[ids[i]];
                 if (ok) seen[ids[i]] = 1;
             }
-            for (int i = 0; ok && i < n_items; ++i)
-                ok = items[i].x >= 0 && items[i].x < s->ti.n_tiles && items[i].y >= 0 && items[i].z > 0 &&
-                     items[i].z <= kItem && (size_t)items[i].y + items[i].z <= n;
         }
     }
     std::fclose(f);
@@ -973,8 +923,6 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     mpm_status r = mpm_set_state(s, &st);
     if (r != MPM_OK) return r;
     if (restore_order) {
-        if (n_items > 0) MPM_CUDA(s, cudaMemcpy(s->ti.items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice));
-        MPM_CUDA(s, cudaMemcpy(s->ti.n_items, &n_items, sizeof(int), cudaMemcpyHostToDevice));
         s->needs_sort = false;
     }
     s->step = step;

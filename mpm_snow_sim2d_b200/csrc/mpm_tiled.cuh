@@ -1,18 +1,16 @@
-// Tiled MLS step for B200: particles binned by cell tile, P2G accumulated per
-// cell in registers and per tile in shared memory, and a grid update that only
-// visits node blocks P2G touched.
+// Tiled MLS step for B200: particles binned by cell tile, P2G accumulated by
+// warps over runs of same-cell particles, and a grid update that only visits
+// the node blocks P2G touched.
 //
 // Tiles are T^D cells (3D: 4^3, 2D: 8^2). Every `sort_period` steps (counted
 // in absolute steps) a sort moves the particle state into the order
 // (tile, cell in tile, particle id), which depends on the state alone
-// (k_sort_count, k_sort_scan, k_sort_bucket, k_tile_sort). Between sorts a
-// particle may drift M = 1 cell out of its tile and is still handled by its
-// tile's CTA; farther drifters ("orphans") take a per-particle path with global
-// atomics. Determinism: work items are fixed slices of that order; inside a
-// CTA the particles of one cell are accumulated in particle-id order in FP32;
-// every cross-cell / cross-CTA sum is an int64 fixed-point atomic. Grid sums
-// are therefore bit-identical run to run, and a checkpoint that carries the
-// slot order resumes bit-identically.
+// (k_sort_count, k_sort_scan, k_sort_bucket, k_tile_sort). P2G (k_p2g_warp)
+// groups consecutive slots whose particles share their current cell; inside
+// a group the contributions are summed in FP32 in slot order, and every
+// cross-group sum is an int64 fixed-point atomic. Grid sums are therefore
+// bit-identical run to run, and a checkpoint that carries the slot order
+// resumes bit-identically.
 #pragma once
 
 #include "mpm_kernels.cuh"
@@ -20,17 +18,9 @@
 namespace mpm {
 
 template <int D> struct TileGeom;
-template <> struct TileGeom<3> {
-    static constexpr int T = 4, M = 1, R = T + 2 * M, NR = R + 3;
-    static constexpr int RC = R * R * R, NN = NR * NR * NR, SPLIT = 4, PS = 29, BN = T * T * T;
-};
-template <> struct TileGeom<2> {
-    static constexpr int T = 8, M = 1, R = T + 2 * M, NR = R + 3;
-    static constexpr int RC = R * R, NN = NR * NR, SPLIT = 1, PS = 17, BN = T * T;
-};
-
-constexpr int kItem = 512;     // particles per work item (one CTA pass)
-constexpr int kTileThreads = 256;
+// T: cells per tile edge (also nodes per node-block edge); BN: nodes per block.
+template <> struct TileGeom<3> { static constexpr int T = 4, BN = T * T * T; };
+template <> struct TileGeom<2> { static constexpr int T = 8, BN = T * T; };
 
 struct TileInfo {
     int tiles[3];      // cell tiles per axis
@@ -41,12 +31,9 @@ struct TileInfo {
     int* tile_count;   // per tile
     int* tile_cursor;  // per tile
     int* tile_start;   // per tile (exclusive scan of tile_count)
-    int4* items;       // (tile, first slot, count, 0)
-    int* n_items;      // device scalar
     int* mark;         // per node block: touched by this step's P2G
     int* mark_list;    // touched node blocks
     int* n_marked;     // device scalar
-    int* n_orphans;    // device scalar, diagnostics (accumulates)
     int* perm;         // sort scratch: slot order by tile (source slots)
     int* tile_list;    // non-empty tiles of the last sort
     int* n_tile_list;  // device scalar
@@ -84,48 +71,40 @@ __global__ void __launch_bounds__(256) k_sort_count(Particles P, StepConsts C, T
     if (lane == __ffs(peers) - 1) atomicAdd(&TI.tile_count[t], __popc(peers));
 }
 
-// Single-CTA exclusive scans of the tile counts and of the work items per tile
-// (a tile with n particles is ceil(n / kItem) items); writes the item list,
-// clears count/cursor for the next sort.
+// Single-CTA exclusive scans of the tile counts and of the non-empty tiles;
+// writes each tile's first slot and the list of non-empty tiles, and clears
+// the cursors for the bucket pass.
 __global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
-    __shared__ int s_cnt[1024], s_itm[1024], s_ne[1024];
+    __shared__ int s_cnt[1024], s_ne[1024];
     const int nt = TI.n_tiles, tid = threadIdx.x;
     const int chunk = (nt + 1023) / 1024;
     const int lo = min(nt, tid * chunk), hi = min(nt, lo + chunk);
-    int c = 0, it = 0, ne = 0;
+    int c = 0, ne = 0;
     for (int t = lo; t < hi; ++t) {
         const int n = TI.tile_count[t];
         c += n;
-        it += (n + kItem - 1) / kItem;
         ne += n > 0;
     }
     s_cnt[tid] = c;
-    s_itm[tid] = it;
     s_ne[tid] = ne;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scans
         const int a = tid >= off ? s_cnt[tid - off] : 0;
-        const int b = tid >= off ? s_itm[tid - off] : 0;
         const int d = tid >= off ? s_ne[tid - off] : 0;
         __syncthreads();
         s_cnt[tid] += a;
-        s_itm[tid] += b;
         s_ne[tid] += d;
         __syncthreads();
     }
-    int base = s_cnt[tid] - c, ibase = s_itm[tid] - it, lbase = s_ne[tid] - ne;
+    int base = s_cnt[tid] - c, lbase = s_ne[tid] - ne;
     for (int t = lo; t < hi; ++t) {
         const int n = TI.tile_count[t];
         TI.tile_start[t] = base;
         TI.tile_cursor[t] = 0;
-        for (int j = 0; j < n; j += kItem) TI.items[ibase++] = make_int4(t, base + j, min(kItem, n - j), 0);
         if (n > 0) TI.tile_list[lbase++] = t;  // non-empty tiles in tile order
         base += n;
     }
-    if (tid == 1023) {
-        *TI.n_items = s_itm[1023];
-        *TI.n_tile_list = s_ne[1023];
-    }
+    if (tid == 1023) *TI.n_tile_list = s_ne[1023];
 }
 
 struct SortBuffers {
@@ -228,386 +207,6 @@ __device__ __forceinline__ void mark_block(const TileInfo& TI, int b) {
     if (atomicExch(&TI.mark[b], 1) == 0) TI.mark_list[atomicAdd(TI.n_marked, 1)] = b;
 }
 
-template <int D> __device__ __forceinline__ void mark_stencil_blocks(const TileInfo& TI, const int* base) {
-    constexpr int T = TileGeom<D>::T;
-    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-        lo[k] = min(max(0, base[k]) / T, TI.nblk[k] - 1);
-        hi[k] = min(TI.nblk[k] * T - 1, max(0, base[k] + 3)) / T;
-    }
-    for (int bz = lo[2]; bz <= hi[2]; ++bz)
-        for (int by = lo[1]; by <= hi[1]; ++by)
-            for (int bx = lo[0]; bx <= hi[0]; ++bx) mark_block(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
-}
-
-// ---------------------------------------------------------------------------
-// Tiled P2G (MLS).
-template <int D, bool DIRECT> struct P2GSmem {
-    using G = TileGeom<D>;
-    float pay[kItem * G::PS];
-    int lcell[kItem];
-    int order[kItem];
-    int cnt[G::RC];
-    int start[G::RC];
-    int cur[G::RC];
-    int ne[G::RC];
-    int n_ne;
-    unsigned blockmask;
-    unsigned long long tile[DIRECT ? 1 : (1 + D) * G::NN];
-};
-
-// Payload layout (floats) per particle:
-//   3D: wx[4] wy[4] wz[4] | f[3] | mv[3] | A[9] | m
-//   2D: wx[4] wy[4] | f[2] | mv[2] | A[4] | m
-// with f = x - cell (cell = int(x)), A = 3 m B - 3 dt V sigma, mv = m v.
-template <int D> struct PayOff {
-    static constexpr int F = 4 * D, MV = F + D, A = MV + D, M = A + D * D;
-};
-
-template <int D>
-__device__ __forceinline__ void scatter_orphan(const StepConsts& C, const TileInfo& TI, const int* base,
-                                               const float (*wk)[4], const float* f, const float* mv, const float* A,
-                                               float m, unsigned long long* acc, unsigned* status) {
-    const int lim[3] = {C.W, C.H, C.Dp};
-    bool outside = false;
-    const int nzs = (D == 3) ? 4 : 1;
-    for (int a = 0; a < 4; ++a) {
-        const int ix = base[0] + a;
-        if (ix < 0 || ix > lim[0]) { outside = true; continue; }
-        for (int b = 0; b < 4; ++b) {
-            const int iy = base[1] + b;
-            if (iy < 0 || iy > lim[1]) { outside = true; continue; }
-            for (int c = 0; c < nzs; ++c) {
-                const int iz = (D == 3) ? base[2] + c : 0;
-                if (D == 3 && (iz < 0 || iz > lim[2])) { outside = true; continue; }
-                const long long cid = ((long long)iz * C.ny + iy) * C.nx + ix;
-                const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
-                const float d[3] = {float(a - 1) - f[0], float(b - 1) - f[1], D == 3 ? float(c - 1) - f[2] : 0.f};
-                red_add(&acc[cid], to_fixed(w * m, C.sm, status));
-#pragma unroll
-                for (int r = 0; r < D; ++r) {
-                    float s = mv[r];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) s += A[r * D + k] * d[k];
-                    red_add(&acc[(1 + r) * C.nodes + cid], to_fixed(w * s, C.sp, status));
-                }
-            }
-        }
-    }
-    if (outside) raise_flag(status, 4u);
-    mark_stencil_blocks<D>(TI, base);
-}
-
-// Node blocks (of T^D nodes, numbered relative to tile tc - 1 per axis) that
-// hold the in-grid nodes of a unit: x in [lx, lx + wx), y and z 4 nodes from
-// ly, lz (region-local node coordinates; region node 0 is cell rlo - 1).
-template <int D>
-__device__ __forceinline__ void unit_blocks(const int* rlo, int lx, int ly, int lz, int wx, const int* ext,
-                                            const int* tc, unsigned* mask) {
-    constexpr int T = TileGeom<D>::T;
-    const int l[3] = {lx, ly, lz}, wd[3] = {wx, 4, 4};
-    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-        const int g0 = max(0, rlo[k] - 1 + l[k]), g1 = min(ext[k], rlo[k] - 1 + l[k] + wd[k] - 1);
-        if (g0 > g1) return;
-        lo[k] = g0 / T - (tc[k] - 1);
-        hi[k] = g1 / T - (tc[k] - 1);
-    }
-    unsigned bits = 0u;
-    for (int z = lo[2]; z <= (D == 3 ? hi[2] : 0); ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-            for (int x = lo[0]; x <= hi[0]; ++x) bits |= 1u << (x + 3 * y + 9 * z);
-    atomicOr(mask, bits);
-}
-
-// DIRECT: each (cell, x-offset) unit adds its 16 (2D: 16) node partial sums
-// straight to the global int64 sums; otherwise they are gathered in a shared
-// int64 tile first and flushed once per work item.
-template <int D, bool DIRECT>
-__global__ void __launch_bounds__(kTileThreads) k_p2g_tiled(Particles P, StepConsts C, TileInfo TI,
-                                                            unsigned long long* __restrict__ acc,
-                                                            unsigned* __restrict__ status) {
-    using G = TileGeom<D>;
-    using O = PayOff<D>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    P2GSmem<D, DIRECT>& S = *reinterpret_cast<P2GSmem<D, DIRECT>*>(smem_raw);
-    const int tid = threadIdx.x;
-    const int n = P.n;
-    const int ext[3] = {C.W, C.H, C.Dp};
-    if (!DIRECT)
-        for (int e = tid; e < (1 + D) * G::NN; e += blockDim.x) S.tile[e] = 0ull;
-
-    const int n_items = *TI.n_items;
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const int4 it = TI.items[item];
-        int tc[3] = {0, 0, 0};
-        {
-            int t = it.x;
-#pragma unroll
-            for (int k = 0; k < D; ++k) { tc[k] = t % TI.tiles[k]; t /= TI.tiles[k]; }
-        }
-        int rlo[3] = {0, 0, 0};
-#pragma unroll
-        for (int k = 0; k < D; ++k) rlo[k] = tc[k] * G::T - G::M;
-        for (int c = tid; c < G::RC; c += blockDim.x) { S.cnt[c] = 0; S.cur[c] = 0; }
-        if (tid == 0) { S.n_ne = 0; S.blockmask = 0u; }
-        __syncthreads();
-
-        // Phase A: per-particle payload: weights, m v and the affine matrix A
-        // that the previous G2P (or k_prepare_affine) computed.
-        for (int j = tid; j < it.z; j += blockDim.x) {
-            const int i = it.y + j;
-            float x[D], A[D * D], mv[D], f[D], wk[3][4];
-            const float mass = P.mass ? P.mass[i] : P.mass_u;
-            const float vol = P.vol ? P.vol[i] : P.vol_u;
-            S.lcell[j] = -1;
-            if (vol == 0.f) continue;  // p2g.glsl:42
-#pragma unroll
-            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; mv[k] = mass * P.v[k * n + i]; }
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
-            int base[3] = {0, 0, 0}, lc = 0;
-            bool inreg = true;
-#pragma unroll
-            for (int k = D - 1; k >= 0; --k) {
-                const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-                const int rlok = k == 0 ? rlo[0] : (k == 1 ? rlo[1] : rlo[2]);
-                base[k] = stencil_base(x[k], extk);
-                const int cell = base[k] + 1;
-                f[k] = x[k] - float(cell);
-#pragma unroll
-                for (int o = 0; o < 4; ++o) wk[k][o] = bspline_n(x[k] - float(base[k] + o));
-                const int l = cell - rlok;
-                inreg = inreg && l >= 0 && l < G::R;
-                lc = lc * G::R + l;
-            }
-            if (inreg) {
-                float* q = S.pay + j * G::PS;
-#pragma unroll
-                for (int k = 0; k < D; ++k) {
-#pragma unroll
-                    for (int o = 0; o < 4; ++o) q[4 * k + o] = wk[k][o];
-                    q[O::F + k] = f[k];
-                    q[O::MV + k] = mv[k];
-                }
-#pragma unroll
-                for (int k = 0; k < D * D; ++k) q[O::A + k] = A[k];
-                q[O::M] = mass;
-                S.lcell[j] = lc;
-                atomicAdd(&S.cnt[lc], 1);
-            } else {
-                scatter_orphan<D>(C, TI, base, wk, f, mv, A, mass, acc, status);
-                atomicAdd(TI.n_orphans, 1);
-            }
-        }
-        __syncthreads();
-
-        // Phase B (warp 0): exclusive scan of the cell counts, list of non-empty
-        // cells, and a stable placement of the particles into per-cell lists in
-        // slot order (deterministic: the slot order is the last sort's order).
-        if (tid < 32) {
-            int carry = 0;
-            for (int c0 = 0; c0 < G::RC; c0 += 32) {
-                const int c = c0 + tid;
-                const int v = c < G::RC ? S.cnt[c] : 0;
-                int incl = v;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (tid >= o) incl += y;
-                }
-                if (c < G::RC) S.start[c] = carry + incl - v;
-                const unsigned nz = __ballot_sync(0xffffffffu, v > 0);
-                if (v > 0) S.ne[S.n_ne + __popc(nz & ((1u << tid) - 1))] = c;
-                __syncwarp();
-                if (tid == 0) S.n_ne += __popc(nz);
-                __syncwarp();
-                carry += __shfl_sync(0xffffffffu, incl, 31);
-            }
-            for (int j0 = 0; j0 < it.z; j0 += 32) {
-                const int j = j0 + tid;
-                const int lc = j < it.z ? S.lcell[j] : -1;
-                const unsigned peers = __match_any_sync(0xffffffffu, lc);
-                const int rank = __popc(peers & ((1u << tid) - 1));
-                if (lc >= 0) S.order[S.start[lc] + S.cur[lc] + rank] = j;
-                __syncwarp();
-                if (lc >= 0 && rank == 0) S.cur[lc] += __popc(peers);
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-
-        // Phase C: one thread per (cell, x-offset): registers over the cell's
-        // particles, then int64 fixed point into the shared tile.
-        const int units = S.n_ne * G::SPLIT;
-        for (int u = tid; u < units; u += blockDim.x) {
-            const int c = S.ne[u / G::SPLIT];
-            const int a = u % G::SPLIT;
-            const int s0 = S.start[c], s1 = s0 + S.cnt[c];
-            if constexpr (D == 3) {
-                const int cx = c % G::R, cy = (c / G::R) % G::R, cz = c / (G::R * G::R);
-                float am[16], a0[16], a1[16], a2[16];
-#pragma unroll
-                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
-                for (int q = s0; q < s1; ++q) {
-                    const float* pp = S.pay + S.order[q] * G::PS;
-                    const float alpha = pp[a];
-                    const float beta = alpha * (float(a - 1) - pp[O::F + 0]);
-                    const float fy = pp[O::F + 1], fz = pp[O::F + 2];
-                    const float* Am = pp + O::A;
-                    const float e0 = alpha * pp[O::MV + 0] + beta * Am[0];
-                    const float e1 = alpha * pp[O::MV + 1] + beta * Am[3];
-                    const float e2 = alpha * pp[O::MV + 2] + beta * Am[6];
-                    const float f0 = alpha * Am[1], f1 = alpha * Am[4], f2 = alpha * Am[7];
-                    const float g0 = alpha * Am[2], g1 = alpha * Am[5], g2 = alpha * Am[8];
-                    const float ma = pp[O::M] * alpha;
-                    float Z[4], Zd[4];
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) { Z[cc] = pp[8 + cc]; Zd[cc] = Z[cc] * (float(cc - 1) - fz); }
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const float Y = pp[4 + b], Yd = Y * (float(b - 1) - fy);
-                        const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
-                        const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
-#pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const int idx = b * 4 + cc;
-                            am[idx] += mY * Z[cc];
-                            a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
-                            a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
-                            a2[idx] += h2 * Z[cc] + k2 * Zd[cc];
-                        }
-                    }
-                }
-                if (DIRECT) unit_blocks<D>(rlo, cx + a, cy, cz, 1, ext, tc, &S.blockmask);
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const int idx = b * 4 + cc;
-                        const long long q0 = to_fixed(am[idx], C.sm, status);
-                        const long long q1 = to_fixed(a0[idx], C.sp, status);
-                        const long long q2 = to_fixed(a1[idx], C.sp, status);
-                        const long long q3 = to_fixed(a2[idx], C.sp, status);
-                        if (DIRECT) {
-                            const int gx = rlo[0] - 1 + cx + a, gy = rlo[1] - 1 + cy + b, gz = rlo[2] - 1 + cz + cc;
-                            if (gx < 0 || gx > ext[0] || gy < 0 || gy > ext[1] || gz < 0 || gz > ext[2]) {
-                                if (q0 | q1 | q2 | q3) raise_flag(status, 4u);
-                                continue;
-                            }
-                            const long long gid = ((long long)gz * C.ny + gy) * C.nx + gx;
-                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
-                            if (q1) atomicAdd(&acc[1 * C.nodes + gid], (unsigned long long)q1);
-                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
-                            if (q3) atomicAdd(&acc[3 * C.nodes + gid], (unsigned long long)q3);
-                        } else {
-                            const int nd = (cx + a) + G::NR * ((cy + b) + G::NR * (cz + cc));
-                            if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
-                            if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
-                            if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
-                            if (q3) atomicAdd(&S.tile[3 * G::NN + nd], (unsigned long long)q3);
-                        }
-                    }
-            } else {
-                const int cx = c % G::R, cy = c / G::R;
-                float am[16], a0[16], a1[16];
-#pragma unroll
-                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
-                for (int q = s0; q < s1; ++q) {
-                    const float* pp = S.pay + S.order[q] * G::PS;
-                    const float fx = pp[O::F + 0], fy = pp[O::F + 1];
-                    const float* Am = pp + O::A;
-                    const float mv0 = pp[O::MV + 0], mv1 = pp[O::MV + 1], m = pp[O::M];
-                    float Y[4], Yd[4];
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) { Y[b] = pp[4 + b]; Yd[b] = Y[b] * (float(b - 1) - fy); }
-#pragma unroll
-                    for (int aa = 0; aa < 4; ++aa) {
-                        const float X = pp[aa], Xd = X * (float(aa - 1) - fx);
-                        const float e0 = mv0 * X + Am[0] * Xd, e1 = mv1 * X + Am[2] * Xd;
-                        const float f0 = Am[1] * X, f1 = Am[3] * X, mX = m * X;
-#pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            const int idx = aa * 4 + b;
-                            am[idx] += mX * Y[b];
-                            a0[idx] += e0 * Y[b] + f0 * Yd[b];
-                            a1[idx] += e1 * Y[b] + f1 * Yd[b];
-                        }
-                    }
-                }
-                if (DIRECT) unit_blocks<D>(rlo, cx, cy, 0, 4, ext, tc, &S.blockmask);
-#pragma unroll
-                for (int aa = 0; aa < 4; ++aa)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int idx = aa * 4 + b;
-                        const long long q0 = to_fixed(am[idx], C.sm, status);
-                        const long long q1 = to_fixed(a0[idx], C.sp, status);
-                        const long long q2 = to_fixed(a1[idx], C.sp, status);
-                        if (DIRECT) {
-                            const int gx = rlo[0] - 1 + cx + aa, gy = rlo[1] - 1 + cy + b;
-                            if (gx < 0 || gx > ext[0] || gy < 0 || gy > ext[1]) {
-                                if (q0 | q1 | q2) raise_flag(status, 4u);
-                                continue;
-                            }
-                            const long long gid = (long long)gy * C.nx + gx;
-                            if (q0) atomicAdd(&acc[gid], (unsigned long long)q0);
-                            if (q1) atomicAdd(&acc[1 * C.nodes + gid], (unsigned long long)q1);
-                            if (q2) atomicAdd(&acc[2 * C.nodes + gid], (unsigned long long)q2);
-                        } else {
-                            const int nd = (cx + aa) + G::NR * (cy + b);
-                            if (q0) atomicAdd(&S.tile[0 * G::NN + nd], (unsigned long long)q0);
-                            if (q1) atomicAdd(&S.tile[1 * G::NN + nd], (unsigned long long)q1);
-                            if (q2) atomicAdd(&S.tile[2 * G::NN + nd], (unsigned long long)q2);
-                        }
-                    }
-            }
-        }
-        __syncthreads();
-
-        // Phase D: shared tile -> global int64 sums (nodes outside the grid are
-        // dropped, as the reference skips them), clear, mark node blocks.
-        int nlo[3] = {0, 0, 0};
-#pragma unroll
-        for (int k = 0; k < D; ++k) nlo[k] = rlo[k] - 1;
-        bool outside = false;
-        for (int e = tid; !DIRECT && e < (1 + D) * G::NN; e += blockDim.x) {
-            const unsigned long long v = S.tile[e];
-            if (v == 0ull) continue;
-            S.tile[e] = 0ull;
-            const int ch = e / G::NN, nd = e % G::NN;
-            int g[3] = {0, 0, 0}, rem = nd;
-            bool in = true;
-            int bb = 0, mul = 1;
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                g[k] = nlo[k] + rem % G::NR;
-                rem /= G::NR;
-                in = in && g[k] >= 0 && g[k] <= ext[k];
-                bb += mul * (g[k] / G::T - (tc[k] - 1));
-                mul *= 3;
-            }
-            if (!in) { outside = true; continue; }
-            const long long gid = ((long long)g[2] * C.ny + g[1]) * C.nx + g[0];
-            atomicAdd(&acc[ch * C.nodes + gid], v);
-            if (ch == 0) atomicOr(&S.blockmask, 1u << bb);
-        }
-        if (outside) raise_flag(status, 4u);
-        __syncthreads();
-        if (tid < (D == 3 ? 27 : 9) && (S.blockmask >> tid) & 1u) {
-            int b[3] = {0, 0, 0}, rem = tid, gb = 0;
-#pragma unroll
-            for (int k = 0; k < D; ++k) { b[k] = tc[k] - 1 + rem % 3; rem /= 3; }
-#pragma unroll
-            for (int k = D - 1; k >= 0; --k) gb = gb * TI.nblk[k] + b[k];
-            mark_block(TI, gb);
-        }
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Grid update over the node blocks P2G marked (reads and clears the int64 sums).
 template <int D, int FORM>
@@ -629,8 +228,6 @@ __global__ void __launch_bounds__(256) k_grid_marked(StepConsts C, TileInfo TI, 
         grid_node<D, FORM>(C, acc, gv, status, ((long long)gz * C.ny + gy) * C.nx + gx);
     }
 }
-
-__global__ void k_reset_marks(TileInfo TI) { *TI.n_marked = 0; }
 
 }  // namespace mpm
 
