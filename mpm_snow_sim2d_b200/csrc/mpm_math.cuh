@@ -16,10 +16,13 @@ enum : int { kBoundaryFriction = 0, kBoundarySticky = 1 };
 // Cubic B-spline N(x) and dN/dx with support |x| < 2:
 // src/gpu/shaders/2d/common.glsl:43-69 (src/cpu/Grid.h:86-116). pow(a, 3.0)
 // is evaluated as a product.
+// Cubic B-spline weight. The outer piece multiplies by the rounded 1/6
+// instead of dividing (within 1 ulp of t^3 / 6; an IEEE division per weight
+// would cost a subroutine call in every stencil).
 template <typename R> __device__ __forceinline__ R bspline_n(R x) {
     R a = fabs(x);
     if (a < R(1)) return R(0.5) * a * a * a - a * a + R(2) / R(3);
-    if (a < R(2)) { R t = R(2) - a; return t * t * t / R(6); }
+    if (a < R(2)) { R t = R(2) - a; return t * t * t * (R(1) / R(6)); }
     return R(0);
 }
 template <typename R> __device__ __forceinline__ R bspline_dn(R x) {

@@ -247,7 +247,9 @@ namespace mpm {
 //
 // Payload per particle (float4-aligned, conflict-free for 8 distinct
 // particles per load):
-//   3D (28): wx[4] | wy[4] | wz[4] | fx fy fz m | mv0 mv1 mv2 A00 | A01 A02 A10 A11 | A12 A20 A21 A22
+//   3D (36): wx[4] | wy[4] | wz[4] | yd[4] | zd[4] | m s0 s1 s2 | A00 A10 A20 A01 | A11 A21 A02 A12 | A22 pad pad pad
+//            with yd[b] = wy[b] (b - 1 - fy), zd[c] = wz[c] (c - 1 - fz) and
+//            s_r = m v_r - fx A_r0 (f = x - cell: the particle's offset in its cell)
 //   2D (20): wx[4] | wy[4] | fx fy m mv0 | mv1 A00 A01 A10 | A11 pad pad pad
 template <int D> struct WarpGeom;
 #ifndef MPM_P2G_CHUNK3
@@ -258,7 +260,7 @@ template <int D> struct WarpGeom;
 #endif
 // 3D: SPLIT threads per run, each holding 16 * 4 / SPLIT nodes (x-offset a,
 // and 16 / SPLIT of the y-offsets) x 4 channels.
-template <> struct WarpGeom<3> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 28; };
+template <> struct WarpGeom<3> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 36; };
 template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
 constexpr int kP2GWarps = 8;
 
@@ -319,10 +321,19 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 k3 = k3 * (extk + 18) + (base + 9);  // cell key: base + 9 >= 0
             }
             if constexpr (D == 3) {
-                reinterpret_cast<float4*>(q)[3] = make_float4(f[0], f[1], f[2], mass);
-                reinterpret_cast<float4*>(q)[4] = make_float4(mv[0], mv[1], mv[2], P.A[i]);
-                reinterpret_cast<float4*>(q)[5] = make_float4(P.A[n + i], P.A[2 * n + i], P.A[3 * n + i], P.A[4 * n + i]);
-                reinterpret_cast<float4*>(q)[6] = make_float4(P.A[5 * n + i], P.A[6 * n + i], P.A[7 * n + i], P.A[8 * n + i]);
+                float A[9];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) A[k] = P.A[k * n + i];
+#pragma unroll
+                for (int o = 0; o < 4; ++o) {
+                    q[12 + o] = q[4 + o] * (float(o - 1) - f[1]);
+                    q[16 + o] = q[8 + o] * (float(o - 1) - f[2]);
+                }
+                reinterpret_cast<float4*>(q)[5] =
+                    make_float4(mass, mv[0] - f[0] * A[0], mv[1] - f[0] * A[3], mv[2] - f[0] * A[6]);
+                reinterpret_cast<float4*>(q)[6] = make_float4(A[0], A[3], A[6], A[1]);
+                reinterpret_cast<float4*>(q)[7] = make_float4(A[4], A[7], A[2], A[5]);
+                reinterpret_cast<float4*>(q)[8] = make_float4(A[8], 0.f, 0.f, 0.f);
             } else {
                 reinterpret_cast<float4*>(q)[2] = make_float4(f[0], f[1], mass, mv[0]);
                 reinterpret_cast<float4*>(q)[3] = make_float4(mv[1], P.A[i], P.A[n + i], P.A[2 * n + i]);
@@ -364,25 +375,25 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 for (int j = j0; j < j1; ++j) {
                     const float4* pp = pay + j * (W::PS / 4);
                     const float alpha = payf[j * W::PS + ax];
-                    const float4 wy = pp[1], wz = pp[2], fm = pp[3], p4 = pp[4], p5 = pp[5], p6 = pp[6];
-                    // A = (p4.w p5.x p5.y | p5.z p5.w p6.x | p6.y p6.z p6.w)
-                    const float beta = alpha * (da - fm.x);
-                    const float e0 = alpha * p4.x + beta * p4.w;
-                    const float e1 = alpha * p4.y + beta * p5.z;
-                    const float e2 = alpha * p4.z + beta * p6.y;
-                    const float f0 = alpha * p5.x, f1 = alpha * p5.w, f2 = alpha * p6.z;
-                    const float g0 = alpha * p5.y, g1 = alpha * p6.x, g2 = alpha * p6.w;
-                    const float ma = fm.w * alpha;
+                    const float4 wy = pp[1], wz = pp[2], yd = pp[3], zd = pp[4], ms = pp[5], q6 = pp[6], q7 = pp[7];
+                    const float a22 = payf[j * W::PS + 32];
+                    // A = (q6.x q6.w q7.z | q6.y q7.x q7.w | q6.z q7.y a22)
+                    const float ad = alpha * da;
+                    const float e0 = alpha * ms.y + ad * q6.x;
+                    const float e1 = alpha * ms.z + ad * q6.y;
+                    const float e2 = alpha * ms.w + ad * q6.z;
+                    const float f0 = alpha * q6.w, f1 = alpha * q7.x, f2 = alpha * q7.y;
+                    const float g0 = alpha * q7.z, g1 = alpha * q7.w, g2 = alpha * a22;
+                    const float ma = ms.x * alpha;
                     const float Z[4] = {wz.x, wz.y, wz.z, wz.w};
+                    const float Zd[4] = {zd.x, zd.y, zd.z, zd.w};
                     const float Yv[4] = {wy.x, wy.y, wy.z, wy.w};
-                    float Zd[4];
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) Zd[cc] = Z[cc] * (float(cc - 1) - fm.z);
+                    const float Ydv[4] = {yd.x, yd.y, yd.z, yd.w};
 #pragma unroll
                     for (int bb = 0; bb < NB; ++bb) {
                         const int b = by0 + bb;
                         const float Y = NB == 4 ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
-                        const float Yd = Y * (float(b - 1) - fm.y);
+                        const float Yd = NB == 4 ? Ydv[bb] : (b == 0 ? yd.x : b == 1 ? yd.y : b == 2 ? yd.z : yd.w);
                         const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
                         const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
 #pragma unroll
