@@ -139,6 +139,24 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(value: float) -> float:
+    """The largest of every rank's value (the job's time is its slowest rank's);
+    the value itself when not distributed. NCCL reduces on the GPU, gloo on the CPU."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return world * units_per_rank * steps / seconds
+
+
 def make_scene(name):
     from mpm_snow_sim2d_b200 import scenes
     return scenes.workload(name)
@@ -415,13 +433,9 @@ def main():
         e1.record(stream)
         e1.synchronize()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1))
     flags = solver.status()
-    value = world * scene.count * args.steps / (ms / 1e3)
+    value = job_rate(world, scene.count, args.steps, ms / 1e3)
 
     # ---- per-stage device time (events between kernels), for the roofline ----
     stages = solver.step_profiled(args.steps)
@@ -449,12 +463,8 @@ def main():
         check(lib.mpm_set_state(solver._h, C.byref(hin)), solver._h)
         check(lib.mpm_step(solver._h, 1), solver._h)
         check(lib.mpm_get_state(solver._h, C.byref(hout)), solver._h)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * n * ke / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = job_rate(world, n, ke, e2e_s)
 
     # ---- roofline of the dominant kernel ----
     peak, peak_src = load_peaks()
