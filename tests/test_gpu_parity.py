@@ -38,6 +38,7 @@ def _gpu_run(scene, steps, **kw):
 
 
 def _check(errs, tol, label):
+    print(f"{label}: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     for k, v in errs.items():
         assert v <= tol[k], f"{label}: {k} rel-L2 {v:.3e} > {tol[k]:.1e} (all: { {a: f'{b:.2e}' for a, b in errs.items()} })"
 
