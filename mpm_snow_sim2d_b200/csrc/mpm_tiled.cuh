@@ -149,17 +149,27 @@ __device__ void bitonic_sort_padded(K* key, V* val, int m) {
     }
 }
 
-constexpr int kSortSmem = 4096;  // particles per tile sorted in shared memory
+constexpr int kSortSmem = 4032;  // particles per tile sorted in shared memory (12 B each, within 48 KB)
+constexpr int kTileCells = 64;   // cells per tile: 4^3 in 3D, 8^2 in 2D
+constexpr int kCountSortMax = kSortSmem / 2;  // tiles up to this size: counting sort (two halves)
+constexpr int kCellSortMax = 64;              // ... when no cell holds more particles than this
 
 // One CTA per non-empty tile: order the tile's particles by (cell in tile,
 // particle id) -- a function of the state alone -- and gather their state into
-// the destination buffers in that order.
+// the destination buffers in that order. Tiles of up to kCountSortMax
+// particles whose cells hold at most kCellSortMax each take a counting sort by
+// cell and an insertion sort by id inside each cell (one thread per cell);
+// larger tiles a bitonic network (in shared memory up to kSortSmem, else in
+// global scratch). The result is the same order either way.
 template <int D>
 __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __restrict__ id_src, SortBuffers dst,
                                                    StepConsts C, TileInfo TI) {
+    static_assert(TileGeom<D>::BN == kTileCells, "a tile has 64 cells");
     constexpr int T = TileGeom<D>::T;
     __shared__ unsigned long long s_key[kSortSmem];
     __shared__ int s_val[kSortSmem];
+    __shared__ int s_cnt[kTileCells], s_off[kTileCells];
+    __shared__ int s_big;
     const int n = P.n, ext[3] = {C.W, C.H, C.Dp};
     const int ntl = *TI.n_tile_list;
     for (int e = blockIdx.x; e < ntl; e += gridDim.x) {
@@ -167,8 +177,12 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
         const int start = TI.tile_start[t];
         const int m = TI.tile_count[t];
         const bool in_smem = m <= kSortSmem;
+        const bool counting = m <= kCountSortMax;
         unsigned long long* key = in_smem ? s_key : TI.skey + start;
         int* val = in_smem ? s_val : TI.sval + start;
+        if (threadIdx.x < kTileCells) s_cnt[threadIdx.x] = 0;
+        if (threadIdx.x == 0) s_big = 0;
+        __syncthreads();
         for (int j = threadIdx.x; j < m; j += blockDim.x) {
             const int src = TI.perm[start + j];
             int cl = 0;
@@ -176,9 +190,54 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
             for (int k = D - 1; k >= 0; --k) cl = cl * T + cell_clamped<D>(P.x[k * n + src], ext[k]) % T;
             key[j] = ((unsigned long long)cl << 32) | (unsigned)id_src[src];
             val[j] = src;
+            if (counting) atomicAdd(&s_cnt[cl], 1);
         }
         __syncthreads();
-        bitonic_sort_padded(key, val, m);
+        if (counting) {
+            // exclusive scan of the 64 cell counts (one warp, two cells per lane)
+            if (threadIdx.x < 32) {
+                const int c0 = s_cnt[2 * threadIdx.x], c1 = s_cnt[2 * threadIdx.x + 1];
+                int incl = c0 + c1;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((int)threadIdx.x >= o) incl += u;
+                }
+                const int ex = incl - c0 - c1;
+                s_off[2 * threadIdx.x] = ex;
+                s_off[2 * threadIdx.x + 1] = ex + c0;
+                if (max(c0, c1) > kCellSortMax) s_big = 1;
+            }
+            __syncthreads();
+        }
+        if (counting && !s_big) {
+            // scatter by cell into the second half, then order each cell by id
+            unsigned long long* key2 = s_key + kCountSortMax;
+            int* val2 = s_val + kCountSortMax;
+            if (threadIdx.x < kTileCells) s_cnt[threadIdx.x] = s_off[threadIdx.x];  // cursors
+            __syncthreads();
+            for (int j = threadIdx.x; j < m; j += blockDim.x) {
+                const int p = atomicAdd(&s_cnt[(int)(key[j] >> 32)], 1);
+                key2[p] = key[j];
+                val2[p] = val[j];
+            }
+            __syncthreads();
+            if (threadIdx.x < kTileCells) {
+                const int lo = s_off[threadIdx.x], hi = s_cnt[threadIdx.x];
+                for (int a = lo + 1; a < hi; ++a) {
+                    const unsigned long long k = key2[a];
+                    const int v = val2[a];
+                    int b = a - 1;
+                    while (b >= lo && key2[b] > k) { key2[b + 1] = key2[b]; val2[b + 1] = val2[b]; --b; }
+                    key2[b + 1] = k;
+                    val2[b + 1] = v;
+                }
+            }
+            __syncthreads();
+            val = val2;
+        } else {
+            bitonic_sort_padded(key, val, m);
+        }
         for (int j = threadIdx.x; j < m; j += blockDim.x) {
             const int src = val[j], s = start + j;
 #pragma unroll
