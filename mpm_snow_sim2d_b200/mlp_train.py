@@ -1,6 +1,7 @@
 """Train the learned plasticity surrogate on pairs logged by the plain solver.
 
     python -m mpm_snow_sim2d_b200.mlp_train [--pairs 50000000] [--steps 60000] [--batch 16384] [--lr 4e-3] [--out PATH]
+        [--save-pairs DIR | --load-pairs DIR]
 
 Data: seeded snowball-on-slab impacts (the 3D workload's set-up, 64^3 grid so
 that contact starts at once) with impact speeds drawn from U(1, 8) m/s, 1000 steps
@@ -75,6 +76,44 @@ def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 1000, p
     return np.concatenate(chunks)[:n_pairs]
 
 
+PAIR_LAYOUT = "F_hat[9] J_p F_E'[9] J_p'"  # one row of the pair log (float32)
+
+
+def save_pair_shards(pairs: np.ndarray, directory, shard_rows: int = 1_000_000) -> list:
+    """Write logged pairs as .npy shards of at most `shard_rows` rows (float32,
+    (rows, 20)) plus index.json (row count, shard names, layout)."""
+    import json
+    from pathlib import Path
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    pairs = np.ascontiguousarray(pairs, np.float32)
+    if pairs.ndim != 2 or pairs.shape[1] != 20:
+        raise ValueError("pairs must be (n, 20)")
+    names = []
+    for k, lo in enumerate(range(0, pairs.shape[0], shard_rows)):
+        name = f"pairs_{k:05d}.npy"
+        np.save(d / name, pairs[lo:lo + shard_rows])
+        names.append(name)
+    (d / "index.json").write_text(json.dumps({"rows": int(pairs.shape[0]), "shards": names, "layout": PAIR_LAYOUT,
+                                              "dtype": "float32"}, indent=1))
+    return names
+
+
+def load_pair_shards(directory) -> np.ndarray:
+    """All rows of a shard directory written by save_pair_shards, in order."""
+    import json
+    from pathlib import Path
+    d = Path(directory)
+    idx = json.loads((d / "index.json").read_text())
+    if idx.get("layout") != PAIR_LAYOUT:
+        raise ValueError(f"unknown pair layout {idx.get('layout')!r}")
+    parts = [np.load(d / name, mmap_mode="r") for name in idx["shards"]]
+    out = np.concatenate(parts) if parts else np.empty((0, 20), np.float32)
+    if out.shape[0] != idx["rows"] or (out.ndim == 2 and out.shape[1] != 20):
+        raise ValueError("pair shards do not match their index")
+    return np.ascontiguousarray(out, np.float32)
+
+
 def evaluate(mlp: Mlp, pairs: np.ndarray):
     """Relative error of the predicted F_E' against the exact one, per pair."""
     pred = mlp.predict(pairs)
@@ -112,11 +151,19 @@ def main(argv=None) -> int:
     ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
+    ap.add_argument("--save-pairs", default=None, help="also write the collected pairs as shards to this directory")
+    ap.add_argument("--load-pairs", default=None, help="train on the shards in this directory instead of collecting")
     args = ap.parse_args(argv)
     _lib.load()
     t0 = time.perf_counter()
-    pairs = collect_pairs(args.pairs, seed=args.seed)
-    print(f"collected {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
+    if args.load_pairs:
+        pairs = load_pair_shards(args.load_pairs)
+        print(f"loaded {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
+    else:
+        pairs = collect_pairs(args.pairs, seed=args.seed)
+        print(f"collected {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
+        if args.save_pairs:
+            save_pair_shards(pairs, args.save_pairs)
     mlp, info = train(pairs, steps=args.steps, batch=args.batch, lr=args.lr, seed=args.seed)
     print({k: v for k, v in info.items() if k != "loss"}, "loss first/last", float(info["loss"][0]),
           float(info["loss"][-1]))
