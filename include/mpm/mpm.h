@@ -273,6 +273,27 @@ MPM_API mpm_status mpm_get_mlp_stats(mpm_solver* solver, uint64_t* accepted, uin
 MPM_API mpm_status mpm_pair_log_enable(mpm_solver* solver, int64_t capacity);
 MPM_API mpm_status mpm_pair_log_read(mpm_solver* solver, float* out, int64_t cap_pairs, int64_t* n_pairs);
 
+/* ---- Headless frames ----------------------------------------------------
+ * Visualize + saveFrame (src/main.cpp:51-205) without a window: particles as
+ * white smoothed points of point_size pixels, the border at BORDER_MARGIN as
+ * 2-pixel gray lines (2D rectangle; 3D wireframe box seen by the reference's
+ * orbit camera: 45 deg perspective, angle / elevation / distance around the
+ * grid centre), black background, nearest fragment wins. RGB8, rows top first
+ * (what saveFrame writes to its PNG). */
+typedef struct mpm_render_params {
+    int32_t width, height; /* WINDOW_WIDTH, WINDOW_HEIGHT (1200 x 600) */
+    float point_size;      /* PARTICLE_SIZE (1), pixels */
+    float camera_angle;    /* 3D: degrees around y (0) */
+    float camera_elevation;/* 3D: degrees (30) */
+    float camera_distance; /* 3D: grid units from the grid centre (300) */
+    float fov_degrees;     /* 3D: vertical field of view (45) */
+    int32_t reserved[5];
+} mpm_render_params;
+
+MPM_API void mpm_render_params_default(mpm_render_params* params);
+/* Writes width * height * 3 bytes into rgb (cap_bytes at least that). Synchronises. */
+MPM_API mpm_status mpm_render(mpm_solver* solver, const mpm_render_params* params, uint8_t* rgb, size_t cap_bytes);
+
 /* ---- Batched scenes (2D MLS) -------------------------------------------
  * Many independent scenes, each a full solver in the sense of mpm_create
  * (the reference constructs one Solver per process, src/main.cpp:164-174),

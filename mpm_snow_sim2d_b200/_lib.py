@@ -61,6 +61,12 @@ class MpmStateHost(C.Structure):
     ]
 
 
+class MpmRenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("point_size", C.c_float), ("camera_angle", C.c_float),
+                ("camera_elevation", C.c_float), ("camera_distance", C.c_float), ("fov_degrees", C.c_float),
+                ("reserved", C.c_int32 * 5)]
+
+
 class MpmBatchConfig(C.Structure):
     _fields_ = [("threads", C.c_int32), ("particles_per_cta", C.c_int32), ("max_cluster", C.c_int32),
                 ("sort_period", C.c_int32), ("reserved", C.c_int32 * 4)]
@@ -105,6 +111,8 @@ SIGNATURES = {
     "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),
     "mpm_pair_log_read": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
+    "mpm_render_params_default": (None, [C.POINTER(MpmRenderParams)]),
+    "mpm_render": (C.c_int, [_P, C.POINTER(MpmRenderParams), C.POINTER(C.c_uint8), C.c_size_t]),
     "mpm_batch_create": (C.c_int, [C.POINTER(MpmParams), C.POINTER(MpmParticlesInit), C.c_int32, C.POINTER(_P)]),
     "mpm_batch_destroy": (C.c_int, [_P]),
     "mpm_batch_last_error": (C.c_char_p, [_P]),

@@ -16,6 +16,7 @@
 #include "mpm_kernels.cuh"
 #include "mpm_tiled.cuh"
 #include "mpm_mlp.cuh"
+#include "mpm_render.cuh"
 #include "mpm_host.h"
 
 using namespace mpm;
@@ -55,6 +56,9 @@ struct mpm_solver {
     unsigned* status = nullptr;
     float* staging = nullptr;
     size_t staging_floats = 0;
+    unsigned long long* render_fb = nullptr;  // per-pixel (depth, intensity) words
+    unsigned char* render_rgb = nullptr;
+    long long render_pixels = 0;
     int log2_sm = 0, log2_sp = 0, log2_sf = 0;
     long long step = 0;
     StepConsts C{};
@@ -410,6 +414,8 @@ mpm_status validate(const mpm_params* p, std::string& why) { return validate_par
 mpm_status ensure_staging(mpm_solver* s, size_t floats) {
     if (floats <= s->staging_floats) return MPM_OK;
     if (s->staging) cudaFree(s->staging);
+    if (s->render_fb) cudaFree(s->render_fb);
+    if (s->render_rgb) cudaFree(s->render_rgb);
     s->staging = nullptr;
     s->staging_floats = 0;
     MPM_CUDA(s, dalloc(&s->staging, floats));
@@ -1199,6 +1205,144 @@ mpm_status mpm_pair_log_read(mpm_solver* s, float* out, int64_t cap_pairs, int64
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Headless frames (Visualize + saveFrame, src/main.cpp:51-205).
+namespace {
+
+void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+void normalise3(double* v) {
+    const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l > 0) for (int k = 0; k < 3; ++k) v[k] /= l;
+}
+
+// Host copy of render_project (for the line sample counts).
+bool host_project(const RenderView& V, const float* p, double& px, double& py) {
+    if (V.dim == 2) {
+        px = p[0] * V.sx;
+        py = V.height - p[1] * V.sy;
+        return true;
+    }
+    double d[3], xv = 0, yv = 0, w = 0;
+    for (int k = 0; k < 3; ++k) d[k] = p[k] - V.eye[k];
+    for (int k = 0; k < 3; ++k) { xv += V.s[k] * d[k]; yv += V.u[k] * d[k]; w += V.f[k] * d[k]; }
+    if (!(w >= V.znear && w <= V.zfar)) return false;
+    px = (V.px_scale * xv / w + 1.0) * 0.5 * V.width;
+    py = V.height - (V.py_scale * yv / w + 1.0) * 0.5 * V.height;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mpm_render_params_default(mpm_render_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->width = 1200;   // WINDOW_WIDTH (Parameters.h:64)
+    p->height = 600;   // WINDOW_HEIGHT (Parameters.h:65)
+    p->point_size = 1.f;           // PARTICLE_SIZE (Parameters.h:73)
+    p->camera_angle = 0.f;         // main.cpp:51-53
+    p->camera_elevation = 30.f;
+    p->camera_distance = 300.f;
+    p->fov_degrees = 45.f;         // main.cpp:61
+}
+
+mpm_status mpm_render(mpm_solver* s, const mpm_render_params* p, uint8_t* rgb, size_t cap_bytes) {
+    if (!s || !p || !rgb) return MPM_ERR_INVALID_ARGUMENT;
+    if (p->width < 1 || p->height < 1 || p->width > 16384 || p->height > 16384 || !(p->point_size > 0.f) ||
+        !(p->point_size <= 64.f) || !(p->fov_degrees > 0.f && p->fov_degrees < 180.f) || !(p->camera_distance > 0.f))
+        return fail(s, MPM_ERR_INVALID_ARGUMENT, "bad render parameters");
+    const long long pixels = (long long)p->width * p->height;
+    if (cap_bytes < (size_t)pixels * 3) return fail(s, MPM_ERR_CAPACITY, "image buffer smaller than width * height * 3");
+    if (pixels > s->render_pixels) {
+        if (s->render_fb) cudaFree(s->render_fb);
+        if (s->render_rgb) cudaFree(s->render_rgb);
+        s->render_fb = nullptr;
+        s->render_rgb = nullptr;
+        s->render_pixels = 0;
+        MPM_CUDA(s, dalloc(&s->render_fb, (size_t)pixels));
+        MPM_CUDA(s, dalloc(&s->render_rgb, (size_t)pixels * 3));
+        s->render_pixels = pixels;
+    }
+    RenderView V{};
+    V.dim = s->dim;
+    V.width = p->width;
+    V.height = p->height;
+    V.radius = 0.5f * p->point_size;
+    const float m = (float)s->params.border_margin, W = (float)s->params.width, H = (float)s->params.height,
+                Dp = s->dim == 3 ? (float)s->params.depth : 0.f;
+    RenderLines L{};
+    if (s->dim == 2) {  // glOrtho(0, WIDTH, 0, HEIGHT) onto the window (main.cpp:260-261)
+        V.sx = (float)p->width / W;
+        V.sy = (float)p->height / H;
+        const float c[4][3] = {{m, m, 0}, {W - m, m, 0}, {W - m, H - m, 0}, {m, H - m, 0}};
+        for (int k = 0; k < 4; ++k)
+            for (int c3 = 0; c3 < 3; ++c3) { L.a[k][c3] = c[k][c3]; L.b[k][c3] = c[(k + 1) % 4][c3]; }
+        L.count = 4;
+    } else {  // SetupCamera (main.cpp:56-80)
+        const double center[3] = {0.5 * W, 0.5 * H, 0.5 * Dp};
+        const double rad = p->camera_angle * M_PI / 180.0, elev = p->camera_elevation * M_PI / 180.0;
+        const double eye[3] = {center[0] + p->camera_distance * std::cos(elev) * std::sin(rad),
+                               center[1] + p->camera_distance * std::sin(elev),
+                               center[2] + p->camera_distance * std::cos(elev) * std::cos(rad)};
+        double f[3] = {center[0] - eye[0], center[1] - eye[1], center[2] - eye[2]};
+        normalise3(f);
+        const double up[3] = {0, 1, 0};
+        double sv[3], u[3];
+        cross3(f, up, sv);
+        normalise3(sv);
+        cross3(sv, f, u);
+        const double t = std::tan(0.5 * p->fov_degrees * M_PI / 180.0), aspect = (double)p->width / p->height;
+        for (int k = 0; k < 3; ++k) {
+            V.eye[k] = (float)eye[k];
+            V.f[k] = (float)f[k];
+            V.s[k] = (float)sv[k];
+            V.u[k] = (float)u[k];
+        }
+        V.px_scale = (float)(1.0 / (aspect * t));
+        V.py_scale = (float)(1.0 / t);
+        V.znear = 1.f;
+        V.zfar = 1000.f;
+        // wireframe box (main.cpp:85-111): bottom, top, pillars
+        const float x0 = m, y0 = m, z0 = m, x1 = W - m, y1 = H - m, z1 = Dp - m;
+        const float e[12][6] = {{x0, y0, z0, x1, y0, z0}, {x1, y0, z0, x1, y0, z1}, {x1, y0, z1, x0, y0, z1},
+                                {x0, y0, z1, x0, y0, z0}, {x0, y1, z0, x1, y1, z0}, {x1, y1, z0, x1, y1, z1},
+                                {x1, y1, z1, x0, y1, z1}, {x0, y1, z1, x0, y1, z0}, {x0, y0, z0, x0, y1, z0},
+                                {x1, y0, z0, x1, y1, z0}, {x1, y0, z1, x1, y1, z1}, {x0, y0, z1, x0, y1, z1}};
+        for (int k = 0; k < 12; ++k)
+            for (int c3 = 0; c3 < 3; ++c3) { L.a[k][c3] = e[k][c3]; L.b[k][c3] = e[k][3 + c3]; }
+        L.count = 12;
+    }
+    for (int k = 0; k < L.count; ++k) {
+        double ax, ay, bx, by;
+        if (host_project(V, L.a[k], ax, ay) && host_project(V, L.b[k], bx, by)) {
+            const double len = std::sqrt((bx - ax) * (bx - ax) + (by - ay) * (by - ay));
+            L.samples[k] = (int)std::min(65536.0, std::ceil(2.0 * len) + 1.0);
+        } else {
+            L.samples[k] = 4096;
+        }
+    }
+    const int threads = 256;
+    const unsigned pblocks = (unsigned)((pixels + threads - 1) / threads);
+    k_render_clear<<<pblocks, threads, 0, s->stream>>>(s->render_fb, pixels);
+    k_render_lines<<<L.count, threads, 0, s->stream>>>(V, L, s->render_fb);
+    if (s->n > 0)
+        k_render_points<<<(s->n + threads - 1) / threads, threads, 0, s->stream>>>(V, s->x, s->n, s->render_fb);
+    k_render_pack<<<pblocks, threads, 0, s->stream>>>(s->render_fb, pixels, s->render_rgb);
+    MPM_CUDA(s, cudaGetLastError());
+    MPM_CUDA(s, cudaMemcpyAsync(rgb, s->render_rgb, (size_t)pixels * 3, cudaMemcpyDeviceToHost, s->stream));
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+}  // extern "C"
+
 
 // ---------------------------------------------------------------------------
 // Inference without allocation: fixed scratch in the device image.

@@ -3,6 +3,7 @@
     python -m mpm_snow_sim2d_b200.run c3 --steps 4
     python -m mpm_snow_sim2d_b200.run impact64 --steps 100 --plasticity mlp
     python -m mpm_snow_sim2d_b200.run c4 --scenes 64 --steps 10 --batch-threads 1024
+    python -m mpm_snow_sim2d_b200.run c1 --steps 1000 --frames frames/
 
 Prints the particle count, the device status word and the wall time; used for
 profiling captures and quick checks. Workloads: see scenes.workload(); "impact64" is the training set-up of the
@@ -23,6 +24,9 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--sort-period", type=int, default=0)
     ap.add_argument("--plasticity", choices=["exact", "mlp"], default="exact")
+    ap.add_argument("--frames", default=None, help="write a PNG frame every --frame-steps steps to this directory")
+    ap.add_argument("--frame-steps", type=int, default=0,
+                    help="steps per frame (0: 1 / (SAVE_FPS dt), SAVE_FPS = 30 as in Parameters.h:69)")
     ap.add_argument("--scenes", type=int, default=256, help="c4: scenes in the batch")
     ap.add_argument("--batch-threads", type=int, default=1024, help="c4: threads per CTA")
     args = ap.parse_args(argv)
@@ -51,7 +55,22 @@ def main(argv=None) -> int:
             net = Mlp.load(DEFAULT_WEIGHTS)
             s.set_plasticity(_lib.PLASTIC_MLP, net, 1e-3)
         t0 = time.perf_counter()
-        s.Step(args.steps)
+        if args.frames:
+            # Simulate + Visualize + saveFrame (src/main.cpp:163-205) without a window
+            from pathlib import Path
+            from .image import write_png
+            out = Path(args.frames)
+            out.mkdir(parents=True, exist_ok=True)
+            per = args.frame_steps or max(1, round(1.0 / (30.0 * scene.delta_time)))
+            done, frame = 0, 0
+            while done < args.steps:
+                k = min(per, args.steps - done)
+                s.Step(k)
+                done += k
+                write_png(out / f"frame_{frame}.png", s.render())
+                frame += 1
+        else:
+            s.Step(args.steps)
         pos = s.GetParticlePositions()  # synchronises
         dt = time.perf_counter() - t0
         print(f"{scene.name}: {scene.count} particles, {args.steps} steps, status {s.status()}, "

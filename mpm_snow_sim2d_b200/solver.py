@@ -156,6 +156,20 @@ class Solver:
         check(self._lib.mpm_step_profiled(self._h, int(nsteps), ms, n), self._h)
         return {self._lib.mpm_stage_name(self._h, k).decode(): float(ms[k]) for k in range(n)}
 
+    # -- headless frames (Visualize + saveFrame) -------------------------------
+    def render(self, **kw) -> np.ndarray:
+        """(height, width, 3) uint8 frame of the current state; keywords
+        override mpm_render_params_default (width, height, point_size,
+        camera_angle, camera_elevation, camera_distance, fov_degrees)."""
+        p = _lib.MpmRenderParams()
+        self._lib.mpm_render_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        out = np.empty((p.height, p.width, 3), np.uint8)
+        check(self._lib.mpm_render(self._h, C.byref(p), out.ctypes.data_as(C.POINTER(C.c_uint8)), out.nbytes),
+              self._h)
+        return out
+
     # -- learned plasticity ---------------------------------------------------
     def set_plasticity(self, mode: int, mlp=None, tolerance: float = 1e-3) -> None:
         """_lib.PLASTIC_EXACT, or _lib.PLASTIC_MLP with an Mlp (kept alive by the caller)."""
