@@ -29,7 +29,7 @@ def test_render_2d_matches_oracle(gpu_lib):
     _compare(img, ref)
     assert img.shape == (600, 1200, 3)
     assert np.array_equal(img[..., 0], img[..., 1]) and np.array_equal(img[..., 0], img[..., 2])
-    assert img.max() == 255 and (img == 128).any()  # particles white, border gray
+    assert img.max() > 200 and (img == 128).any()  # particles (smoothed) white, border gray
 
 
 def test_render_3d_matches_oracle(gpu_lib):

@@ -14,10 +14,10 @@ def test_png_round_trip(tmp_path):
 def test_reference_renderer_geometry():
     from oracle import render_ref
     # one particle at the centre of a 2D 100 x 50 domain on a 200 x 100 image
-    img = render_ref.render(np.array([[50.0, 25.0]]), 2, 100, 50, 0, 3, 200, 100, point_size=1.0)
+    img = render_ref.render(np.array([[50.0, 25.0]]), 2, 100, 50, 0, 3, 200, 100, point_size=3.0)
     # x = 50 -> pixel column 100, y = 25 -> row 100 - 50 = 50 (rows top first)
     lit = np.argwhere(img[..., 0] == img[..., 0].max())
-    assert img[..., 0].max() > 200
+    assert img[..., 0].max() == 255
     assert abs(lit[:, 0].mean() - 49.5) <= 0.5 and abs(lit[:, 1].mean() - 99.5) <= 0.5
     assert (img == 128).any()  # the border
     # 3D: a particle at the grid centre projects to the image centre
