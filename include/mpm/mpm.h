@@ -273,6 +273,32 @@ MPM_API mpm_status mpm_get_mlp_stats(mpm_solver* solver, uint64_t* accepted, uin
 MPM_API mpm_status mpm_pair_log_enable(mpm_solver* solver, int64_t capacity);
 MPM_API mpm_status mpm_pair_log_read(mpm_solver* solver, float* out, int64_t cap_pairs, int64_t* n_pairs);
 
+/* ---- Seeded shape sampling ---------------------------------------------
+ * The reference fills each snow shape with Bridson's Poisson-disk sampling
+ * seeded from std::random_device (PoissonDiskCircle / PoissonDiskSphere,
+ * src/shared/Shapes.h:17-117,143-234): no two particles closer than min_dist,
+ * not reproducible. mpm_sample_shapes does the same on the device in parallel
+ * (grid-phase dart throwing, `rounds` candidates per background cell) and
+ * deterministically for a given seed. Output: `count` positions (count * dim
+ * floats, in background-cell order) and, if shape_of is not NULL, the first
+ * shape containing each. With capacity too small it returns MPM_ERR_CAPACITY
+ * and sets count to the number needed (call again with that capacity). */
+typedef enum mpm_shape_kind {
+    MPM_SHAPE_BALL = 0, /* SNOWBALL (Shapes.h:10-13): circle in 2D, sphere in 3D */
+    MPM_SHAPE_BOX = 1   /* axis-aligned box (center +- half) */
+} mpm_shape_kind;
+
+typedef struct mpm_shape {
+    int32_t kind;      /* mpm_shape_kind */
+    float center[3];   /* grid units (z ignored in 2D) */
+    float radius;      /* MPM_SHAPE_BALL */
+    float half[3];     /* MPM_SHAPE_BOX half extents */
+} mpm_shape;
+
+MPM_API mpm_status mpm_sample_shapes(int32_t dim, const mpm_shape* shapes, int32_t nshapes, float min_dist,
+                                     uint64_t seed, int32_t rounds, float* positions, int32_t* shape_of,
+                                     int64_t capacity, int64_t* count);
+
 /* ---- Headless frames ----------------------------------------------------
  * Visualize + saveFrame (src/main.cpp:51-205) without a window: particles as
  * white smoothed points of point_size pixels, the border at BORDER_MARGIN as

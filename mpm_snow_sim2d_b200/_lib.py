@@ -61,6 +61,14 @@ class MpmStateHost(C.Structure):
     ]
 
 
+class MpmShape(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("center", C.c_float * 3), ("radius", C.c_float), ("half", C.c_float * 3)]
+
+
+SHAPE_BALL = 0
+SHAPE_BOX = 1
+
+
 class MpmRenderParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("point_size", C.c_float), ("camera_angle", C.c_float),
                 ("camera_elevation", C.c_float), ("camera_distance", C.c_float), ("fov_degrees", C.c_float),
@@ -111,6 +119,8 @@ SIGNATURES = {
     "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),
     "mpm_pair_log_read": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
+    "mpm_sample_shapes": (C.c_int, [C.c_int32, C.POINTER(MpmShape), C.c_int32, C.c_float, C.c_uint64, C.c_int32,
+                                     C.POINTER(C.c_float), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
     "mpm_render_params_default": (None, [C.POINTER(MpmRenderParams)]),
     "mpm_render": (C.c_int, [_P, C.POINTER(MpmRenderParams), C.POINTER(C.c_uint8), C.c_size_t]),
     "mpm_batch_create": (C.c_int, [C.POINTER(MpmParams), C.POINTER(MpmParticlesInit), C.c_int32, C.POINTER(_P)]),

@@ -257,3 +257,49 @@ def workload(name: str) -> Scene:
     if name == "c5":
         return two_snowballs_3d()
     raise KeyError(name)
+
+
+# The reference's default scene, in its own units (src/shared/Parameters.h:30-80):
+# a 200 x 100 (x 100) grid, border margin 2, two snowballs of radius 15 at
+# (50, 45[, 50]) and (150, 55[, 50]) thrown at each other at 40 cells/s,
+# dt 1e-3, gravity -9.81, friction 0.3, theta_c 2e-2, theta_s 6e-3, xi 10,
+# nu 0.2, E 1.4e5, RHO 400; NUM_PARTICLES 3000 sets min_dist.
+REFERENCE_DEFAULT = dict(width=200, height=100, depth=100, margin=2, radius=15.0, num_particles=3000,
+                         centers=((50.0, 45.0, 50.0), (150.0, 55.0, 50.0)), velocities=((40.0, 0.0, 0.0), (-40.0, 0.0, 0.0)),
+                         delta_time=1e-3, gravity=-9.81, friction=0.3, theta_c=2.0e-2, theta_s=6.0e-3, xi=10.0,
+                         nu=0.2, youngs=1.4e5, rho=400.0)
+
+
+def reference_snowballs(dim: int = 2, seed: int = 1, steps: int = 6600, rounds: int = 30) -> Scene:
+    """The reference's two-snowball scene with particles from the device
+    Poisson-disk sampler (needs a GPU). Per snowball, as
+    src/gpu/GPUSolver.cpp:99-155: min_dist = radius / NUM_PARTICLES^(1/dim),
+    vol = (2 pi r^2 in 2D | 4/3 pi r^3 in 3D) / samples, mass = vol RHO / 100.
+    The default 6600 steps are the reference's 200 frames at 30 frames/s.
+    """
+    from .sampling import ball, sample_shapes
+
+    R = REFERENCE_DEFAULT
+    r = R["radius"]
+    n_ref = float(R["num_particles"])
+    md = np.float32(r) / (np.sqrt(np.float32(n_ref)) if dim == 2 else np.cbrt(np.float32(n_ref)))
+    pos, vel, vol, mass, counts = [], [], [], [], []
+    for k, (c, v) in enumerate(zip(R["centers"], R["velocities"])):
+        p, _ = sample_shapes(dim, [ball(c[:dim], r)], float(md), seed + 7919 * k, rounds)
+        n = p.shape[0]
+        f, pi, rf = np.float32, np.float32(3.1415926), np.float32(r)  # Shapes.h:8 PI, float arithmetic
+        v_p = (f(2) * pi * rf * rf if dim == 2 else (f(4) / f(3)) * pi * rf * rf * rf) / f(n)
+        pos.append(p)
+        vel.append(np.tile(np.asarray(v[:dim], np.float32), (n, 1)))
+        vol.append(np.full(n, v_p, np.float32))
+        mass.append(np.full(n, v_p * np.float32(R["rho"]) / np.float32(100.0), np.float32))
+        counts.append(n)
+    return Scene(
+        name=f"reference_snowballs{dim}d", dim=dim, width=R["width"], height=R["height"],
+        depth=R["depth"] if dim == 3 else 0, border_margin=R["margin"], delta_time=R["delta_time"],
+        gravity=R["gravity"], friction=R["friction"], theta_c=R["theta_c"], theta_s=R["theta_s"], xi=R["xi"],
+        nu=R["nu"], youngs=R["youngs"], rho=R["rho"], steps=steps,
+        position=np.ascontiguousarray(np.concatenate(pos)), velocity=np.ascontiguousarray(np.concatenate(vel)),
+        volume=np.concatenate(vol), mass=np.concatenate(mass),
+        info=dict(seed=seed, min_dist=float(md), per_ball=counts, sampler="device poisson-disk"),
+    )

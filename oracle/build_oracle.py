@@ -2,6 +2,8 @@
 
 * ``oracle/liboracle_mpm.so`` — the project's CPU restatement (mpm_oracle.cpp),
   FP64 oracle + FP32/OpenMP CPU baseline.
+* ``oracle/_ref/poisson{2,3}d`` — the reference's Poisson-disk samplers
+  (src/shared/Shapes.h, included where it lies) behind a small driver.
 * ``oracle/_ref/refcpu_driver`` — the reference's own CPU path: src/cpu/Grid.cpp
   and src/cpu/Particles.cpp compiled unmodified, where they lie in the reference
   tree, with g++ against the shadow headers in oracle/refcpu/shadow (runtime
@@ -22,6 +24,7 @@ REF_ROOT = Path(os.environ.get("MPM_REFERENCE_ROOT", "/root/reference"))
 ORACLE_LIB = HERE / "liboracle_mpm.so"
 REF_DIR = HERE / "_ref"
 REFCPU = REF_DIR / "refcpu_driver"
+POISSON = {2: REF_DIR / "poisson2d", 3: REF_DIR / "poisson3d"}
 
 
 def _stale(target: Path, deps) -> bool:
@@ -73,9 +76,28 @@ def build_refcpu(force: bool = False) -> Path | None:
     return REFCPU
 
 
+def build_poisson(force: bool = False) -> dict:
+    """The reference's Poisson-disk samplers (src/shared/Shapes.h) behind a
+    small driver; {dim: path}, empty when the reference tree is absent."""
+    if not reference_available():
+        return {d: p for d, p in POISSON.items() if p.exists()}
+    driver = HERE / "refcpu" / "poisson_driver.cpp"
+    shapes = REF_ROOT / "src" / "shared" / "Shapes.h"
+    for dim, out in POISSON.items():
+        if force or _stale(out, [driver, shapes]):
+            REF_DIR.mkdir(exist_ok=True)
+            tmp = out.with_suffix(".tmp")
+            _run(["g++", "-O2", "-std=c++17", "-w", *(["-DSIM_3D"] if dim == 3 else []),
+                  "-I", str(REF_ROOT / "src" / "shared"), "-I", str(REF_ROOT / "external" / "glm-0.9.7.1"),
+                  str(driver), "-o", str(tmp)])
+            os.replace(tmp, out)
+    return dict(POISSON)
+
+
 def build_all(force: bool = False) -> None:
     build_oracle(force)
     build_refcpu(force)
+    build_poisson(force)
 
 
 if __name__ == "__main__":
