@@ -68,8 +68,11 @@ enum {
 };
 
 typedef enum mpm_formulation {
-    MPM_FORMULATION_MLS = 0,    /* the reference GPU shaders (src/gpu/shaders/{2d,3d}) */
-    MPM_FORMULATION_CLASSIC = 1 /* the reference CPU path (src/cpu), 2D only */
+    MPM_FORMULATION_MLS = 0,           /* the reference GPU shaders (src/gpu/shaders/{2d,3d}) */
+    MPM_FORMULATION_CLASSIC = 1,       /* the reference CPU path (src/cpu), 2D only */
+    MPM_FORMULATION_MLS_QUADRATIC = 2  /* the MLS step on the quadratic B-spline stencil (3 nodes per
+                                          axis, D^-1 = 4); no counterpart in the reference, which is cubic
+                                          (src/gpu/shaders/2d/common.glsl:43-82) */
 } mpm_formulation;
 
 typedef enum mpm_boundary {

@@ -25,6 +25,7 @@ FLAG_TIMEOUT = 1 << 4
 
 FORMULATION_MLS = 0
 FORMULATION_CLASSIC = 1
+FORMULATION_MLS_QUADRATIC = 2
 BOUNDARY_FRICTION = 0
 BOUNDARY_STICKY = 1
 PLASTIC_EXACT = 0

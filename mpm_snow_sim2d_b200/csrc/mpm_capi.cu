@@ -40,6 +40,7 @@ struct mpm_mlp {
 struct mpm_solver {
     mpm_params params{};
     int dim = 2, form = kMLS;
+    int stencil = 4;  // nodes per axis: 4 cubic (MLS, CLASSIC), 3 quadratic (QUAD)
     int n = 0;
     long long nodes = 0;
     int device = 0;
@@ -211,13 +212,13 @@ void invalidate_graphs(mpm_solver* s) {
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
-template <int D> cudaError_t launch_sort(mpm_solver* s) {
+template <int D, int S> cudaError_t launch_sort(mpm_solver* s) {
     if (s->n == 0) { s->needs_sort = false; return cudaSuccess; }
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
-    k_sort_count<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
+    k_sort_count<D, S><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
     k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
     k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
-    k_tile_sort<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
+    k_tile_sort<D, S><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     swap_buffers(s);
@@ -225,20 +226,20 @@ template <int D> cudaError_t launch_sort(mpm_solver* s) {
     return cudaSuccess;
 }
 
-template <int D> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
-    k_p2g_warp<D><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D>), s->stream>>>(particle_view(s), s->C,
-                                                                                          s->ti, s->acc, s->status);
+template <int D, int S> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
+    k_p2g_warp<D, S><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D, S>), s->stream>>>(
+        particle_view(s), s->C, s->ti, s->acc, s->status);
     return cudaGetLastError();
 }
 
 // G2P of the tiled MLS path: gather + in-band return map (stage "g2p"), then
 // the queued particles' full return map (stage "return_map").
-template <int D> cudaError_t launch_g2p_gather(mpm_solver* s) {
+template <int D, int S> cudaError_t launch_g2p_gather(mpm_solver* s) {
     if (s->n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
-    k_g2p_gather<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
+    k_g2p_gather<D, S><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, s->status);
     return cudaGetLastError();
 }
 
@@ -251,41 +252,41 @@ cudaError_t mlp_kernel_attrs() {
     return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpWarpSmem));
 }
 
-template <int D> cudaError_t launch_return_map(mpm_solver* s) {
+template <int D, int S> cudaError_t launch_return_map(mpm_solver* s) {
     if (s->n == 0) return cudaSuccess;
     PairLog L{s->log_data, s->log_n, s->log_cap};
-    if (D == 3 && s->plasticity == MPM_PLASTIC_MLP && s->mlp) {
+    if (D == 3 && S == 4 && s->plasticity == MPM_PLASTIC_MLP && s->mlp) {
         MlpParams ML{s->mlp->wbf, s->mlp->w, s->mlp->norm, s->mlp_tol, s->mlp_counters};
         k_return_map_mlp<<<s->sms * 2, kMlpWarps * 32, sizeof(MlpWarpSmem), s->stream>>>(particle_view(s), s->C, s->q,
                                                                                        ML);
         L = PairLog{nullptr, nullptr, 0};
     }
-    k_g2p_plastic<D><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, L, s->status);
+    k_g2p_plastic<D, S><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->gv, s->q, L, s->status);
     return cudaGetLastError();
 }
 
-template <int D> cudaError_t launch_g2p_split(mpm_solver* s) {
-    cudaError_t e = launch_g2p_gather<D>(s);
+template <int D, int S> cudaError_t launch_g2p_split(mpm_solver* s) {
+    cudaError_t e = launch_g2p_gather<D, S>(s);
     if (e != cudaSuccess) return e;
-    return launch_return_map<D>(s);
+    return launch_return_map<D, S>(s);
 }
 
-template <int D> cudaError_t prepare_affine(mpm_solver* s) {
+template <int D, int S> cudaError_t prepare_affine(mpm_solver* s) {
     if (!s->needs_affine || s->n == 0) { s->needs_affine = false; return cudaSuccess; }
     const int threads = 256, blocks = (s->n + threads - 1) / threads;
-    k_prepare_affine<D><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C);
+    k_prepare_affine<D, S><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C);
     s->needs_affine = false;
     return cudaGetLastError();
 }
 
-template <int D> cudaError_t launch_p2g_tiled(mpm_solver* s) {
-    cudaError_t e0 = prepare_affine<D>(s);
+template <int D, int S> cudaError_t launch_p2g_tiled(mpm_solver* s) {
+    cudaError_t e0 = prepare_affine<D, S>(s);
     if (e0 != cudaSuccess) return e0;
     if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) {
-        cudaError_t e = launch_sort<D>(s);
+        cudaError_t e = launch_sort<D, S>(s);
         if (e != cudaSuccess) return e;
     }
-    return launch_p2g_tiled_kernel<D>(s);
+    return launch_p2g_tiled_kernel<D, S>(s);
 }
 
 template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
@@ -295,14 +296,14 @@ template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
     return cudaSuccess;
 }
 
-template <int D> cudaError_t step_tiled(mpm_solver* s) {
-    cudaError_t e = launch_p2g_tiled<D>(s);
+template <int D, int S> cudaError_t step_tiled(mpm_solver* s) {
+    cudaError_t e = launch_p2g_tiled<D, S>(s);
     if (e != cudaSuccess) return e;
     e = launch_grid_marked<D>(s);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
-    return launch_g2p_split<D>(s);
+    return launch_g2p_split<D, S>(s);
 }
 
 template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
@@ -314,13 +315,19 @@ template <int D, int FORM> cudaError_t step_once(mpm_solver* s) {
 }
 
 cudaError_t dispatch_step(mpm_solver* s) {
-    if (s->tiled) return s->dim == 2 ? step_tiled<2>(s) : step_tiled<3>(s);
+    if (s->tiled) {
+        if (s->stencil == 3) return s->dim == 2 ? step_tiled<2, 3>(s) : step_tiled<3, 3>(s);
+        return s->dim == 2 ? step_tiled<2, 4>(s) : step_tiled<3, 4>(s);
+    }
     if (s->dim == 2) return s->form == kClassic ? step_once<2, kClassic>(s) : step_once<2, kMLS>(s);
     return step_once<3, kMLS>(s);
 }
 
 cudaError_t dispatch_p2g(mpm_solver* s) {
-    if (s->tiled) return s->dim == 2 ? launch_p2g_tiled<2>(s) : launch_p2g_tiled<3>(s);
+    if (s->tiled) {
+        if (s->stencil == 3) return s->dim == 2 ? launch_p2g_tiled<2, 3>(s) : launch_p2g_tiled<3, 3>(s);
+        return s->dim == 2 ? launch_p2g_tiled<2, 4>(s) : launch_p2g_tiled<3, 4>(s);
+    }
     if (s->dim == 2) return s->form == kClassic ? launch_p2g<2, kClassic>(s) : launch_p2g<2, kMLS>(s);
     return launch_p2g<3, kMLS>(s);
 }
@@ -375,13 +382,18 @@ mpm_status setup_tiled(mpm_solver* s) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     s->sms = sms > 0 ? sms : 148;
     {
-        const size_t wsm = D == 3 ? sizeof(P2GWarpSmem<3>) : sizeof(P2GWarpSmem<2>);
-        cudaError_t ew = D == 3 ? cudaFuncSetAttribute(k_p2g_warp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm)
-                                : cudaFuncSetAttribute(k_p2g_warp<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+        const void* kfn;
+        size_t wsm;
+        if (s->stencil == 3) {
+            kfn = D == 3 ? (const void*)k_p2g_warp<3, 3> : (const void*)k_p2g_warp<2, 3>;
+            wsm = D == 3 ? sizeof(P2GWarpSmem<3, 3>) : sizeof(P2GWarpSmem<2, 3>);
+        } else {
+            kfn = D == 3 ? (const void*)k_p2g_warp<3, 4> : (const void*)k_p2g_warp<2, 4>;
+            wsm = D == 3 ? sizeof(P2GWarpSmem<3, 4>) : sizeof(P2GWarpSmem<2, 4>);
+        }
+        cudaError_t ew = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
         int per = 0;
-        if (ew == cudaSuccess)
-            ew = D == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g_warp<3>, kP2GWarps * 32, wsm)
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g_warp<2>, kP2GWarps * 32, wsm);
+        if (ew == cudaSuccess) ew = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kP2GWarps * 32, wsm);
         if (ew != cudaSuccess || per < 1) return MPM_ERR_CUDA;
         s->p2g_warp_grid = s->sms * per;
     }
@@ -469,24 +481,27 @@ template <int D, int FORM> cudaError_t stage(mpm_solver* s, int k) {
     if (k == 3) return launch_g2p<D, FORM>(s);
     return cudaSuccess;  // the untiled G2P includes its return map
 }
-template <int D> cudaError_t stage_tiled(mpm_solver* s, int k) {
+template <int D, int S> cudaError_t stage_tiled(mpm_solver* s, int k) {
     if (k == 0) {
-        cudaError_t e = prepare_affine<D>(s);
+        cudaError_t e = prepare_affine<D, S>(s);
         if (e != cudaSuccess) return e;
-        if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) return launch_sort<D>(s);
+        if (s->needs_sort || (s->sort_period > 0 && s->step % s->sort_period == 0)) return launch_sort<D, S>(s);
         return cudaSuccess;
     }
-    if (k == 1) return launch_p2g_tiled_kernel<D>(s);
+    if (k == 1) return launch_p2g_tiled_kernel<D, S>(s);
     if (k == 2) {
         cudaError_t e = launch_grid_marked<D>(s);
         if (e != cudaSuccess) return e;
         return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
     }
-    if (k == 3) return launch_g2p_gather<D>(s);
-    return launch_return_map<D>(s);
+    if (k == 3) return launch_g2p_gather<D, S>(s);
+    return launch_return_map<D, S>(s);
 }
 cudaError_t dispatch_stage(mpm_solver* s, int k) {
-    if (s->tiled) return s->dim == 2 ? stage_tiled<2>(s, k) : stage_tiled<3>(s, k);
+    if (s->tiled) {
+        if (s->stencil == 3) return s->dim == 2 ? stage_tiled<2, 3>(s, k) : stage_tiled<3, 3>(s, k);
+        return s->dim == 2 ? stage_tiled<2, 4>(s, k) : stage_tiled<3, 4>(s, k);
+    }
     if (s->dim == 2) return s->form == kClassic ? stage<2, kClassic>(s, k) : stage<2, kMLS>(s, k);
     return stage<3, kMLS>(s, k);
 }
@@ -597,6 +612,7 @@ mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, 
     s->params = *params;
     s->dim = params->dim;
     s->form = params->formulation;
+    s->stencil = stencil_of(s->form);
     s->device = dev;
     s->n = (int)init->count;
     fill_consts(s);
@@ -669,7 +685,7 @@ mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, 
     ok = ok && cudaMemset(s->status, 0, sizeof(unsigned)) == cudaSuccess;
     ok = ok && cudaDeviceSynchronize() == cudaSuccess;
     if (!ok) { cudaGetLastError(); return bail(MPM_ERR_CUDA); }
-    s->tiled = (s->form == kMLS);
+    s->tiled = (s->form != kClassic);  // MLS and QUAD
     if (s->tiled) {
         mpm_status ts = setup_tiled(s);
         if (ts != MPM_OK) return bail(ts);
@@ -1146,7 +1162,8 @@ mpm_status mpm_set_plasticity(mpm_solver* s, int32_t mode, mpm_mlp* mlp, float t
     if (mode != MPM_PLASTIC_EXACT && mode != MPM_PLASTIC_MLP) return fail(s, MPM_ERR_INVALID_ARGUMENT, "unknown plasticity mode");
     if (mode == MPM_PLASTIC_MLP) {
         if (!mlp) return fail(s, MPM_ERR_INVALID_ARGUMENT, "MLP plasticity needs a network");
-        if (s->dim != 3 || !s->tiled) return fail(s, MPM_ERR_UNSUPPORTED, "the learned return map is 3D MLS only");
+        if (s->dim != 3 || !s->tiled || s->stencil != 4)
+            return fail(s, MPM_ERR_UNSUPPORTED, "the learned return map is 3D MLS (cubic stencil) only");
         if (!(tolerance > 0.f)) return fail(s, MPM_ERR_INVALID_ARGUMENT, "tolerance must be > 0");
         MPM_CUDA(s, mlp_kernel_attrs());
         if (!s->mlp_counters) {

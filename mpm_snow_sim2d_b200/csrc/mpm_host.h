@@ -17,7 +17,8 @@ inline mpm_status validate_params(const mpm_params* p, std::string& why) {
     const double nodes = double(p->width + 1) * (p->height + 1) * (p->dim == 3 ? p->depth + 1 : 1);
     if (nodes > 2.0e9) { why = "grid too large"; return MPM_ERR_INVALID_ARGUMENT; }
     if (!(p->delta_time > 0.f) || !std::isfinite(p->delta_time)) { why = "delta_time must be > 0"; return MPM_ERR_INVALID_ARGUMENT; }
-    if (p->formulation != MPM_FORMULATION_MLS && p->formulation != MPM_FORMULATION_CLASSIC) { why = "unknown formulation"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->formulation != MPM_FORMULATION_MLS && p->formulation != MPM_FORMULATION_CLASSIC &&
+        p->formulation != MPM_FORMULATION_MLS_QUADRATIC) { why = "unknown formulation"; return MPM_ERR_INVALID_ARGUMENT; }
     if (p->formulation == MPM_FORMULATION_CLASSIC && p->dim != 2) { why = "the CLASSIC (reference CPU) formulation is 2D only"; return MPM_ERR_UNSUPPORTED; }
     if (p->boundary != MPM_BOUNDARY_FRICTION && p->boundary != MPM_BOUNDARY_STICKY) { why = "unknown boundary"; return MPM_ERR_INVALID_ARGUMENT; }
     if (p->border_margin < 0) { why = "border_margin must be >= 0"; return MPM_ERR_INVALID_ARGUMENT; }

@@ -74,6 +74,23 @@ __device__ __forceinline__ int stencil_base(float x, int extent) {
     return int(fminf(fmaxf(x, -8.f), float(extent) + 8.f)) - 1;
 }
 
+// A stencil of S nodes per axis: first node base(x), weight w(x - x_i), the
+// MLS factor D^-1, and the shift that makes floor(x + SHIFT) = base + 1 (the
+// particle's cell for the cubic stencil, its nearest node for the quadratic).
+template <int S> struct Stencil;
+template <> struct Stencil<4> {  // cubic, the reference's: nodes int(x) - 1 .. int(x) + 2
+    static constexpr float DINV = 3.f, SHIFT = 0.f;
+    __device__ static __forceinline__ int base(float x, int ext) { return stencil_base(x, ext); }
+    __device__ static __forceinline__ float w(float d) { return bspline_n(d); }
+};
+template <> struct Stencil<3> {  // quadratic: nodes floor(x - 1/2) .. floor(x - 1/2) + 2
+    static constexpr float DINV = 4.f, SHIFT = 0.5f;
+    __device__ static __forceinline__ int base(float x, int ext) {
+        return int(floorf(fminf(fmaxf(x, -8.f), float(ext) + 8.f) - 0.5f));
+    }
+    __device__ static __forceinline__ float w(float d) { return quad_n(d); }
+};
+
 // ---------------------------------------------------------------------------
 // P2G, one thread per particle.
 // MLS (src/gpu/shaders/2d/p2g.glsl:29-92, 3d/p2g.glsl:31-96): per node
@@ -82,6 +99,7 @@ __device__ __forceinline__ int stencil_base(float x, int extent) {
 // which is the shader's  m (v + 3 B (-dist)) + w V sigma dist 3 dt  regrouped.
 // CLASSIC (src/cpu/Grid.cpp:118-163): p_i += w m_p (v_p + 3 B_p (x_i - x_p)),
 //   f_i += A_p^T grad w (A_p = V_p sigma_p, glm row-vector product).
+// QUAD: the MLS sums on the quadratic stencil, A_p = 4 m_p B_p - 4 dt V_p sigma_p.
 // Sums are int64 fixed point (exact, order independent).
 template <int D, int FORM>
 __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, unsigned long long* __restrict__ acc,
@@ -97,10 +115,13 @@ __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, u
     const float Jp = P.Jp[i];
     const float mass = P.mass ? P.mass[i] : P.mass_u;
     const float vol = P.vol ? P.vol[i] : P.vol_u;
-    if (FORM == kMLS && vol == 0.f) return;
+    constexpr bool MLS = FORM != kClassic;
+    constexpr int S = stencil_of(FORM);
+    using St = Stencil<S>;
+    if (MLS && vol == 0.f) return;
 
     float sig[D * D];
-    if (vol != 0.f) hardened_stress_polar<D, FORM>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
+    if (vol != 0.f) hardened_stress_polar<D, math_form(FORM)>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
     else {
 #pragma unroll
         for (int k = 0; k < D * D; ++k) sig[k] = 0.f;
@@ -111,21 +132,21 @@ __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, u
         mv[r] = mass * v[r];
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            if (FORM == kMLS) A[r * D + c] = 3.f * mass * B[r * D + c] - 3.f * C.dt * vol * sig[r * D + c];
+            if (MLS) A[r * D + c] = St::DINV * mass * B[r * D + c] - St::DINV * C.dt * vol * sig[r * D + c];
             else A[r * D + c] = vol * sig[r * D + c];
         }
     }
 
     const int ext[3] = {C.W, C.H, C.Dp};
     int base[3] = {0, 0, 0};
-    float wk[3][4], dwk[3][4], off[3][4];  // off = x_i - x_p per axis
+    float wk[3][S], dwk[3][S], off[3][S];  // off = x_i - x_p per axis
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        base[k] = stencil_base(x[k], ext[k]);
+        base[k] = St::base(x[k], ext[k]);
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
+        for (int o = 0; o < S; ++o) {
             const float dist = x[k] - float(base[k] + o);
-            wk[k][o] = bspline_n(dist);
+            wk[k][o] = St::w(dist);
             dwk[k][o] = (FORM == kClassic) ? bspline_dn(dist) : 0.f;
             off[k][o] = -dist;
         }
@@ -133,13 +154,13 @@ __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, u
     const int lim[3] = {C.W, C.H, C.Dp};
     bool outside = false;
     constexpr int NACC = Layout<D, FORM>::NACC;
-    const int nzs = (D == 3) ? 4 : 1;
+    const int nzs = (D == 3) ? S : 1;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < S; ++a) {
         const int ix = base[0] + a;
         if (ix < 0 || ix > lim[0]) { outside = true; continue; }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < S; ++b) {
             const int iy = base[1] + b;
             if (iy < 0 || iy > lim[1]) { outside = true; continue; }
 #pragma unroll
@@ -150,7 +171,7 @@ __global__ void __launch_bounds__(256) k_p2g_simple(Particles P, StepConsts C, u
                 const float w = (D == 3) ? wk[0][a] * wk[1][b] * wk[2][c] : wk[0][a] * wk[1][b];
                 const float d[3] = {off[0][a], off[1][b], D == 3 ? off[2][c] : 0.f};
                 red_add(&acc[cid], to_fixed(w * mass, C.sm, status));
-                if (FORM == kMLS) {
+                if (MLS) {
 #pragma unroll
                     for (int r = 0; r < D; ++r) {
                         float s = mv[r];
@@ -256,7 +277,7 @@ __device__ __forceinline__ void grid_node_velocity(const StepConsts& C, const lo
     const float mass = __ll2float_rn(q[0]) * C.inv_sm;
     if (mass >= 1e-6f) {
         float vel[3] = {0.f, 0.f, 0.f};
-        if (FORM == kMLS) {
+        if (FORM != kClassic) {
 #pragma unroll
             for (int k = 0; k < D; ++k) vel[k] = (__ll2float_rn(q[1 + k]) * C.inv_sp) / mass;
             vel[1] += C.gravity * C.dt;
@@ -390,7 +411,8 @@ __device__ __forceinline__ void plasticity(const StepConsts& C, const float* Fh,
 }
 
 // G2P + APIC + plasticity, one thread per particle (MLS: src/gpu/shaders/2d/
-// g2p.glsl:21-93, 3d/g2p.glsl:22-104; CLASSIC: src/cpu/Particles.cpp:133-216).
+// g2p.glsl:21-93, 3d/g2p.glsl:22-104; CLASSIC: src/cpu/Particles.cpp:133-216;
+// QUAD: the MLS update on the quadratic stencil, F_hat = (I + 4 dt B) F_E).
 // The new position  sum w (x_i + dt v_col)  is evaluated as
 // x_p * sum(w) + sum w ((x_i - x_p) + dt v_col), with sum(w) taken as exactly 1
 // when the whole stencil lies inside the grid (partition of unity): the same
@@ -403,19 +425,21 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     const int n = P.n;
+    constexpr int S = stencil_of(FORM);
+    using St = Stencil<S>;
     float x[D];
 #pragma unroll
     for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
     const int ext[3] = {C.W, C.H, C.Dp};
     int base[3] = {0, 0, 0};
-    float wk[3][4], dwk[3][4], off[3][4];
+    float wk[3][S], dwk[3][S], off[3][S];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        base[k] = stencil_base(x[k], ext[k]);
+        base[k] = St::base(x[k], ext[k]);
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
+        for (int o = 0; o < S; ++o) {
             const float dist = x[k] - float(base[k] + o);
-            wk[k][o] = bspline_n(dist);
+            wk[k][o] = St::w(dist);
             dwk[k][o] = (FORM == kClassic) ? bspline_dn(dist) : 0.f;
             off[k][o] = -dist;
         }
@@ -426,15 +450,15 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 #pragma unroll
     for (int k = 0; k < D * D; ++k) { nB[k] = 0.f; gvel[k] = 0.f; }
     const int lim[3] = {C.W, C.H, C.Dp};
-    const int nzs = (D == 3) ? 4 : 1;
+    const int nzs = (D == 3) ? S : 1;
     float wsum = 0.f;
     bool clipped = false;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < S; ++a) {
         const int ix = base[0] + a;
         if (ix < 0 || ix > lim[0]) { clipped = true; continue; }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < S; ++b) {
             const int iy = base[1] + b;
             if (iy < 0 || iy > lim[1]) { clipped = true; continue; }
 #pragma unroll
@@ -487,12 +511,12 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 #pragma unroll
     for (int k = 0; k < D * D; ++k) {
         Fe[k] = P.Fe[k * n + i];
-        const float L = (FORM == kMLS) ? 3.f * nB[k] : gvel[k];
+        const float L = (FORM != kClassic) ? St::DINV * nB[k] : gvel[k];
         A[k] = ((k % (D + 1)) == 0 ? 1.f : 0.f) + C.dt * L;
     }
     matmul<D>(A, Fe, Fh);
     float Jp = P.Jp[i];
-    plasticity<D, FORM>(C, Fh, Fe, Jp, status);
+    plasticity<D, math_form(FORM)>(C, Fh, Fe, Jp, status);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
     P.Jp[i] = Jp;
@@ -504,17 +528,19 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 // scatter (src/gpu/shaders/2d/p2g.glsl:44-90): A = 3 m B - 3 dt V sigma(F_E, J_p),
 // so that a node receives w (m v + A (x_i - x_p)). Computed by G2P for the next
 // step (and by k_prepare_affine after any state upload), always with this one
-// function, so the value depends on (B, F_E, J_p, m, V) alone.
-template <int D>
+// function, so the value depends on (B, F_E, J_p, m, V) alone. On the
+// quadratic stencil (S = 3) the factor is D^-1 = 4 instead of 3.
+template <int D, int S = 4>
 __device__ __forceinline__ void mls_affine(const StepConsts& C, const float* B, const float* Fe, float Jp, float mass,
                                            float vol, float* A) {
+    constexpr float K = Stencil<S>::DINV;
     float sig[D * D];
     hardened_stress_fast<D, kMLS>(Fe, Jp, C.mu0, C.la0, C.xi, sig);
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) A[k] = 3.f * mass * B[k] - 3.f * C.dt * vol * sig[k];
+    for (int k = 0; k < D * D; ++k) A[k] = K * mass * B[k] - K * C.dt * vol * sig[k];
 }
 
-template <int D>
+template <int D, int S = 4>
 __global__ void __launch_bounds__(256) k_prepare_affine(Particles P, StepConsts C) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
@@ -522,7 +548,7 @@ __global__ void __launch_bounds__(256) k_prepare_affine(Particles P, StepConsts 
     float B[D * D], Fe[D * D], A[D * D];
 #pragma unroll
     for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
-    mls_affine<D>(C, B, Fe, P.Jp[i], P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+    mls_affine<D, S>(C, B, Fe, P.Jp[i], P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
 }
@@ -546,18 +572,31 @@ struct SlowQueue {
     int capacity;
 };
 
+// Element a of an S-vector held in registers, for a loop index the compiler
+// does not unroll.
+template <int S> __device__ __forceinline__ float pick(const float* v, int a) {
+    if constexpr (S == 4) return a == 0 ? v[0] : a == 1 ? v[1] : a == 2 ? v[2] : v[3];
+    else return a == 0 ? v[0] : a == 1 ? v[1] : v[2];
+}
+
+// Sum of an S-vector, pairwise for S = 4.
+template <int S> __device__ __forceinline__ float sum_s(const float* v) {
+    if constexpr (S == 4) return (v[0] + v[1]) + (v[2] + v[3]);
+    else return (v[0] + v[1]) + v[2];
+}
+
 // Interior gather: every stencil node inside the grid. The sums
 //   v = sum w vf,  B = sum w vf (x_i - x_p)^T,  x' = x + sum w (x_i - x_p) + dt sum w vc
 // are contracted axis by axis (z, then y, then x) with the separable weights.
-template <int D>
+template <int D, int S = 4>
 __device__ __forceinline__ void gather_interior(const StepConsts& C, const float4* __restrict__ gv, const int* base,
-                                                const float (*wk)[4], const float (*off)[4], float* nv, float* nB,
+                                                const float (*wk)[S], const float (*off)[S], float* nv, float* nB,
                                                 float* nx) {
-    float wd[3][4];
+    float wd[3][S];
 #pragma unroll
     for (int k = 0; k < D; ++k)
 #pragma unroll
-        for (int o = 0; o < 4; ++o) wd[k][o] = wk[k][o] * off[k][o];
+        for (int o = 0; o < S; ++o) wd[k][o] = wk[k][o] * off[k][o];
     const long long sy = C.nx, sz = (long long)C.nx * C.ny;
     const long long c0 = (D == 3 ? base[2] * sz : 0) + base[1] * sy + base[0];
     float vc[D];
@@ -567,18 +606,18 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
 #pragma unroll
     for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
 #pragma unroll 1
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < S; ++a) {
         float Q[D], Qy[D], Qz[D], Qc[D];
 #pragma unroll
         for (int r = 0; r < D; ++r) { Q[r] = 0.f; Qy[r] = 0.f; Qz[r] = 0.f; Qc[r] = 0.f; }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < S; ++b) {
             if constexpr (D == 3) {
                 // vc = vf at every node the wall planes left alone (flag .w = 0):
                 // the vc sum is then the vf sum; flagged nodes are handled below.
                 float Pv[3] = {0.f, 0.f, 0.f}, Pd[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
+                for (int c = 0; c < S; ++c) {
                     const long long cid = c0 + a + b * sy + c * sz;
                     const float4 g = __ldg(&gv[cid]);
                     wall = wall || g.w != 0.f;
@@ -602,8 +641,8 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
                 Qc[0] += y * g.z; Qc[1] += y * g.w;
             }
         }
-        const float x = a == 0 ? wk[0][0] : a == 1 ? wk[0][1] : a == 2 ? wk[0][2] : wk[0][3];
-        const float xd = a == 0 ? wd[0][0] : a == 1 ? wd[0][1] : a == 2 ? wd[0][2] : wd[0][3];
+        const float x = pick<S>(wk[0], a);
+        const float xd = pick<S>(wd[0], a);
 #pragma unroll
         for (int r = 0; r < D; ++r) {
             nv[r] += x * Q[r];
@@ -621,13 +660,13 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
             // a stencil node was moved by a wall plane: the vc sum, in the same
             // order as the vf sum above
 #pragma unroll 1
-            for (int a = 0; a < 4; ++a) {
+            for (int a = 0; a < S; ++a) {
                 float Qc[3] = {0.f, 0.f, 0.f};
 #pragma unroll 1
-                for (int b = 0; b < 4; ++b) {
+                for (int b = 0; b < S; ++b) {
                     float Pc[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
+                    for (int c = 0; c < S; ++c) {
                         float f[3], g[3];
                         load_node3(gv, C.nodes, c0 + a + b * sy + c * sz, f, g);
                         const float z = wk[2][c];
@@ -647,8 +686,8 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
     float sw[3], swd[3];
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        sw[k] = (wk[k][0] + wk[k][1]) + (wk[k][2] + wk[k][3]);
-        swd[k] = (wd[k][0] + wd[k][1]) + (wd[k][2] + wd[k][3]);
+        sw[k] = sum_s<S>(wk[k]);
+        swd[k] = sum_s<S>(wd[k]);
     }
 #pragma unroll
     for (int r = 0; r < D; ++r) {
@@ -662,9 +701,9 @@ __device__ __forceinline__ void gather_interior(const StepConsts& C, const float
 
 // General gather (stencil partly outside the grid: those nodes are skipped,
 // as in the reference, and the partial weight sum is returned).
-template <int D>
+template <int D, int S = 4>
 __device__ __forceinline__ float gather_clipped(const StepConsts& C, const float4* __restrict__ gv, const int* base,
-                                             const float (*wk)[4], const float (*off)[4], float* nv, float* nB,
+                                             const float (*wk)[S], const float (*off)[S], float* nv, float* nB,
                                              float* nx) {
     const int ext[3] = {C.W, C.H, C.Dp};
 #pragma unroll
@@ -672,11 +711,11 @@ __device__ __forceinline__ float gather_clipped(const StepConsts& C, const float
 #pragma unroll
     for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
     float wsum = 0.f;
-    const int nzs = (D == 3) ? 4 : 1;
-    for (int a = 0; a < 4; ++a) {
+    const int nzs = (D == 3) ? S : 1;
+    for (int a = 0; a < S; ++a) {
         const int ix = base[0] + a;
         if (ix < 0 || ix > ext[0]) continue;
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < S; ++b) {
             const int iy = base[1] + b;
             if (iy < 0 || iy > ext[1]) continue;
             for (int c = 0; c < nzs; ++c) {
@@ -713,12 +752,13 @@ __device__ __forceinline__ int queue_slot(const SlowQueue& Q) {
     return __shfl_sync(act, slot, leader) + __popc(act & ((1u << lane) - 1));
 }
 
-template <int D>
 #ifndef MPM_G2P_MIN_BLOCKS
 #define MPM_G2P_MIN_BLOCKS 2
 #endif
+template <int D, int S = 4>
 __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                        SlowQueue Q, unsigned* __restrict__ status) {
+    using St = Stencil<S>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     const int n = P.n;
@@ -726,17 +766,17 @@ __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particle
 #pragma unroll
     for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
     int base[3] = {0, 0, 0};
-    float wk[3][4], off[3][4];
+    float wk[3][S], off[3][S];
     bool interior = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
         const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-        base[k] = stencil_base(x[k], ext);
-        interior = interior && base[k] >= 0 && base[k] + 3 <= ext;
+        base[k] = St::base(x[k], ext);
+        interior = interior && base[k] >= 0 && base[k] + (S - 1) <= ext;
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
+        for (int o = 0; o < S; ++o) {
             const float dist = x[k] - float(base[k] + o);
-            wk[k][o] = bspline_n(dist);
+            wk[k][o] = St::w(dist);
             off[k][o] = -dist;
         }
     }
@@ -745,7 +785,7 @@ __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particle
         return;
     }
     float nv[D], nx[D], nB[D * D];
-    gather_interior<D>(C, gv, base, wk, off, nv, nB, nx);
+    gather_interior<D, S>(C, gv, base, wk, off, nv, nB, nx);
     bool finite = true;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
@@ -765,7 +805,7 @@ __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particle
         for (int c = 0; c < D; ++c) {
             float s = Fe[r * D + c];
 #pragma unroll
-            for (int k = 0; k < D; ++k) s += (C.dt * 3.f * nB[r * D + k]) * Fe[k * D + c];
+            for (int k = 0; k < D; ++k) s += (C.dt * St::DINV * nB[r * D + k]) * Fe[k * D + c];
             Fh[r * D + c] = s;
         }
     float sig[D * D];
@@ -776,7 +816,7 @@ __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particle
 #pragma unroll
         for (int k = 0; k < D * D; ++k) {
             P.Fe[k * n + i] = Fh[k];
-            P.A[k * n + i] = 3.f * mass * nB[k] - 3.f * C.dt * vol * sig[k];
+            P.A[k * n + i] = St::DINV * mass * nB[k] - St::DINV * C.dt * vol * sig[k];
         }
     } else {
         const int slot = queue_slot(Q);
@@ -797,7 +837,7 @@ struct PairLog {
 
 // One queued particle: the full return map for an out-of-band trial F (entry
 // i), or the whole G2P with a grid-clipped stencil (entry -1 - i).
-template <int D>
+template <int D, int S = 4>
 __device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepConsts& C, const float4* __restrict__ gv,
                                                  const SlowQueue& Q, int e, unsigned* __restrict__ status,
                                                  PairLog L = PairLog{nullptr, nullptr, 0}) {
@@ -813,20 +853,20 @@ __device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepC
 #pragma unroll
         for (int k = 0; k < D; ++k) x[k] = P.x[k * n + i];
         int base[3] = {0, 0, 0};
-        float wk[3][4], off[3][4];
+        float wk[3][S], off[3][S];
 #pragma unroll
         for (int k = 0; k < D; ++k) {
             const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-            base[k] = stencil_base(x[k], ext);
+            base[k] = Stencil<S>::base(x[k], ext);
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
+            for (int o = 0; o < S; ++o) {
                 const float dist = x[k] - float(base[k] + o);
-                wk[k][o] = bspline_n(dist);
+                wk[k][o] = Stencil<S>::w(dist);
                 off[k][o] = -dist;
             }
         }
         float nv[D], nx[D];
-        const float wsum = gather_clipped<D>(C, gv, base, wk, off, nv, B, nx);
+        const float wsum = gather_clipped<D, S>(C, gv, base, wk, off, nv, B, nx);
         bool finite = true;
 #pragma unroll
         for (int k = 0; k < D; ++k) {
@@ -844,7 +884,7 @@ __device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepC
             for (int c = 0; c < D; ++c) {
                 float s = Fe[r * D + c];
 #pragma unroll
-                for (int k = 0; k < D; ++k) s += (C.dt * 3.f * B[r * D + k]) * Fe[k * D + c];
+                for (int k = 0; k < D; ++k) s += (C.dt * Stencil<S>::DINV * B[r * D + k]) * Fe[k * D + c];
                 Fh[r * D + c] = s;
             }
     }
@@ -854,7 +894,7 @@ __device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepC
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P.Fe[k * n + i] = Fe[k];
     P.Jp[i] = Jp;
-    mls_affine<D>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
+    mls_affine<D, S>(C, B, Fe, Jp, P.mass ? P.mass[i] : P.mass_u, P.vol ? P.vol[i] : P.vol_u, A);
 #pragma unroll
     for (int k = 0; k < D * D; ++k) P.A[k * n + i] = A[k];
     if (!isfinite(Jp)) raise_flag(status, 1u);
@@ -870,12 +910,12 @@ __device__ __forceinline__ void g2p_queued_exact(const Particles& P, const StepC
     }
 }
 
-template <int D>
+template <int D, int S = 4>
 __global__ void __launch_bounds__(256) k_g2p_plastic(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                      SlowQueue Q, PairLog L, unsigned* __restrict__ status) {
     const int m = *Q.count;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
-        if (Q.list[e] != kQueueDone) g2p_queued_exact<D>(P, C, gv, Q, e, status, L);
+        if (Q.list[e] != kQueueDone) g2p_queued_exact<D, S>(P, C, gv, Q, e, status, L);
 }
 
 // ---------------------------------------------------------------------------

@@ -10,8 +10,17 @@
 
 namespace mpm {
 
-enum : int { kMLS = 0, kClassic = 1 };
+// Formulations: kMLS the reference GPU shaders (cubic stencil, D^-1 = 3);
+// kClassic the reference CPU path (2D); kQuad the MLS step on the quadratic
+// B-spline stencil (3 nodes per axis, D^-1 = 4), which the reference does not
+// have.
+enum : int { kMLS = 0, kClassic = 1, kQuad = 2 };
 enum : int { kBoundaryFriction = 0, kBoundarySticky = 1 };
+
+// Nodes per axis of a formulation's stencil, and the formulation whose SVD and
+// stress a formulation uses (kQuad shares the shaders' math).
+constexpr int stencil_of(int form) { return form == kQuad ? 3 : 4; }
+constexpr int math_form(int form) { return form == kClassic ? kClassic : kMLS; }
 
 // Cubic B-spline N(x) and dN/dx with support |x| < 2:
 // src/gpu/shaders/2d/common.glsl:43-69 (src/cpu/Grid.h:86-116). pow(a, 3.0)
@@ -23,6 +32,14 @@ template <typename R> __device__ __forceinline__ R bspline_n(R x) {
     R a = fabs(x);
     if (a < R(1)) return R(0.5) * a * a * a - a * a + R(2) / R(3);
     if (a < R(2)) { R t = R(2) - a; return t * t * t * (R(1) / R(6)); }
+    return R(0);
+}
+// Quadratic B-spline N(x) with support |x| < 1.5 (the standard MLS-MPM
+// kernel: 3/4 - x^2 inside |x| < 1/2, (3/2 - |x|)^2 / 2 outside).
+template <typename R> __device__ __forceinline__ R quad_n(R x) {
+    R a = fabs(x);
+    if (a < R(0.5)) return R(0.75) - a * a;
+    if (a < R(1.5)) { R t = R(1.5) - a; return R(0.5) * t * t; }
     return R(0);
 }
 template <typename R> __device__ __forceinline__ R bspline_dn(R x) {

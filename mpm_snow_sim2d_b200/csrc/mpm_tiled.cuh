@@ -41,29 +41,33 @@ struct TileInfo {
     int* sval;
 };
 
-template <int D> __device__ __forceinline__ int cell_clamped(float x, int ext) {
+// The sort cell of a coordinate: floor(x + SHIFT) clamped to the grid, i.e.
+// base + 1 of the stencil (the cell for the cubic stencil, the nearest node
+// for the quadratic), so that particles sharing a stencil sort together.
+template <int S> __device__ __forceinline__ int cell_clamped(float x, int ext) {
+    if constexpr (Stencil<S>::SHIFT != 0.f) x += Stencil<S>::SHIFT;
     const int c = int(fminf(fmaxf(x, 0.f), float(ext) - 0.5f));
     return c < 0 ? 0 : (c >= ext ? ext - 1 : c);
 }
 
-template <int D> __device__ __forceinline__ int tile_of_slot(const Particles& P, const StepConsts& C,
-                                                            const TileInfo& TI, int i) {
+template <int D, int S> __device__ __forceinline__ int tile_of_slot(const Particles& P, const StepConsts& C,
+                                                                   const TileInfo& TI, int i) {
     constexpr int T = TileGeom<D>::T;
     const int ext[3] = {C.W, C.H, C.Dp};
     int t = 0;
 #pragma unroll
-    for (int k = D - 1; k >= 0; --k) t = t * TI.tiles[k] + cell_clamped<D>(P.x[k * P.n + i], ext[k]) / T;
+    for (int k = D - 1; k >= 0; --k) t = t * TI.tiles[k] + cell_clamped<S>(P.x[k * P.n + i], ext[k]) / T;
     return t;
 }
 
 // ---------------------------------------------------------------------------
 // Counting sort by tile.
 
-template <int D>
+template <int D, int S = 4>
 __global__ void __launch_bounds__(256) k_sort_count(Particles P, StepConsts C, TileInfo TI) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    const int t = tile_of_slot<D>(P, C, TI, i);
+    const int t = tile_of_slot<D, S>(P, C, TI, i);
     TI.key[i] = t;
     const unsigned act = __activemask();
     const unsigned peers = __match_any_sync(act, t);
@@ -161,7 +165,7 @@ constexpr int kCellSortMax = 64;              // ... when no cell holds more par
 // cell and an insertion sort by id inside each cell (one thread per cell);
 // larger tiles a bitonic network (in shared memory up to kSortSmem, else in
 // global scratch). The result is the same order either way.
-template <int D>
+template <int D, int S = 4>
 __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __restrict__ id_src, SortBuffers dst,
                                                    StepConsts C, TileInfo TI) {
     static_assert(TileGeom<D>::BN == kTileCells, "a tile has 64 cells");
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
             const int src = TI.perm[start + j];
             int cl = 0;
 #pragma unroll
-            for (int k = D - 1; k >= 0; --k) cl = cl * T + cell_clamped<D>(P.x[k * n + src], ext[k]) % T;
+            for (int k = D - 1; k >= 0; --k) cl = cl * T + cell_clamped<S>(P.x[k * n + src], ext[k]) % T;
             key[j] = ((unsigned long long)cl << 32) | (unsigned)id_src[src];
             val[j] = src;
             if (counting) atomicAdd(&s_cnt[cl], 1);
@@ -294,12 +298,13 @@ namespace mpm {
 
 // ---------------------------------------------------------------------------
 // Warp-chunk P2G (MLS). The sorted slot array is cut into fixed chunks of
-// WarpGeom<D>::CHUNK slots; each warp takes one chunk at a time, with no
+// WarpGeom<D, S>::CHUNK slots; each warp takes one chunk at a time, with no
 // CTA-wide synchronisation. In the chunk, maximal runs of consecutive slots
-// whose particles share their current cell are grouped; one thread per (run,
-// x-offset) [3D] or per run [2D] accumulates the run's 16 nodes x (1 + D)
-// channels in FP32 registers, in slot order, and adds them as int64 fixed
-// point to the global sums. The grouping is a function of the slot order (the
+// whose particles share their current stencil are grouped; SPLIT threads per
+// run [3D: one per (x-offset, share of the y-offsets)] or one per run [2D]
+// accumulate the run's S^D nodes x (1 + D) channels in FP32 registers, in slot
+// order, and add them as int64 fixed point to the global sums. S is the
+// stencil width: 4 (cubic) or 3 (quadratic; unused payload entries are 0). The grouping is a function of the slot order (the
 // deterministic sort order, kept between sorts), so the sums are bit-identical
 // run to run; particles that drifted to another cell since the last sort just
 // form shorter runs.
@@ -310,7 +315,7 @@ namespace mpm {
 //            with yd[b] = wy[b] (b - 1 - fy), zd[c] = wz[c] (c - 1 - fz) and
 //            s_r = m v_r - fx A_r0 (f = x - cell: the particle's offset in its cell)
 //   2D (20): wx[4] | wy[4] | fx fy m mv0 | mv1 A00 A01 A10 | A11 pad pad pad
-template <int D> struct WarpGeom;
+template <int D, int S = 4> struct WarpGeom;
 #ifndef MPM_P2G_CHUNK3
 #define MPM_P2G_CHUNK3 48
 #endif
@@ -319,12 +324,15 @@ template <int D> struct WarpGeom;
 #endif
 // 3D: SPLIT threads per run, each holding 16 * 4 / SPLIT nodes (x-offset a,
 // and 16 / SPLIT of the y-offsets) x 4 channels.
-template <> struct WarpGeom<3> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 36; };
-template <> struct WarpGeom<2> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
+template <> struct WarpGeom<3, 4> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 36; };
+template <> struct WarpGeom<2, 4> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
+// quadratic: 3 threads per run in 3D (one per x-offset, 9 nodes each)
+template <> struct WarpGeom<3, 3> { static constexpr int CHUNK = 48, SPLIT = 3, PS = 36; };
+template <> struct WarpGeom<2, 3> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
 constexpr int kP2GWarps = 8;
 
-template <int D> struct P2GWarpSmem {
-    using W = WarpGeom<D>;
+template <int D, int S = 4> struct P2GWarpSmem {
+    using W = WarpGeom<D, S>;
     float4 pay[kP2GWarps][W::CHUNK * W::PS / 4];
     int key[kP2GWarps][W::CHUNK];
     int run[kP2GWarps][W::CHUNK + 1];
@@ -339,22 +347,23 @@ __device__ __forceinline__ void red_fixed(unsigned long long* p, float v, float 
     atomicAdd(p, (unsigned long long)__float2ll_rn(v * scale));
 }
 
-template <int D>
 #ifndef MPM_P2G_MIN_BLOCKS
 #define MPM_P2G_MIN_BLOCKS 3
 #endif
+template <int D, int S = 4>
 __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 2) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
                                                               unsigned long long* __restrict__ acc,
                                                               unsigned* __restrict__ status) {
-    using W = WarpGeom<D>;
+    using W = WarpGeom<D, S>;
+    using St = Stencil<S>;
     constexpr int T = TileGeom<D>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    P2GWarpSmem<D>& S = *reinterpret_cast<P2GWarpSmem<D>*>(smem_raw);
+    P2GWarpSmem<D, S>& SM = *reinterpret_cast<P2GWarpSmem<D, S>*>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float4* pay = S.pay[wid];
+    float4* pay = SM.pay[wid];
     float* payf = reinterpret_cast<float*>(pay);
-    int* key = S.key[wid];
-    int* run = S.run[wid];
+    int* key = SM.key[wid];
+    int* run = SM.run[wid];
     const int n = P.n;
     const int nchunks = (n + W::CHUNK - 1) / W::CHUNK;
     for (int chunk = blockIdx.x * kP2GWarps + wid; chunk < nchunks; chunk += gridDim.x * kP2GWarps) {
@@ -372,9 +381,9 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
             for (int k = D - 1; k >= 0; --k) {
                 const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
                 const float x = P.x[k * n + i];
-                const int base = stencil_base(x, extk);
+                const int base = St::base(x, extk);
 #pragma unroll
-                for (int o = 0; o < 4; ++o) q[4 * k + o] = bspline_n(x - float(base + o));
+                for (int o = 0; o < 4; ++o) q[4 * k + o] = o < S ? St::w(x - float(base + o)) : 0.f;
                 f[k] = x - float(base + 1);
                 mv[k] = mass * P.v[k * n + i];
                 k3 = k3 * (extk + 18) + (base + 9);  // cell key: base + 9 >= 0
@@ -424,9 +433,9 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 kk /= (extk + 18);
             }
             if constexpr (D == 3) {
-                constexpr int NB = 16 / W::SPLIT;  // y-offsets per thread
-                constexpr int NN = NB * 4;         // nodes per thread
-                const int ax = a % 4, by0 = (a / 4) * NB;
+                constexpr int NB = S * S / W::SPLIT;  // y-offsets per thread
+                constexpr int NN = NB * S;            // nodes per thread
+                const int ax = a % S, by0 = (a / S) * NB;
                 float am[NN], a0[NN], a1[NN], a2[NN];
 #pragma unroll
                 for (int k = 0; k < NN; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
@@ -451,13 +460,13 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
 #pragma unroll
                     for (int bb = 0; bb < NB; ++bb) {
                         const int b = by0 + bb;
-                        const float Y = NB == 4 ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
-                        const float Yd = NB == 4 ? Ydv[bb] : (b == 0 ? yd.x : b == 1 ? yd.y : b == 2 ? yd.z : yd.w);
+                        const float Y = NB == S ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
+                        const float Yd = NB == S ? Ydv[bb] : (b == 0 ? yd.x : b == 1 ? yd.y : b == 2 ? yd.z : yd.w);
                         const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
                         const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const int idx = bb * 4 + cc;
+                        for (int cc = 0; cc < S; ++cc) {
+                            const int idx = bb * S + cc;
                             am[idx] += mY * Z[cc];
                             a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
                             a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
@@ -474,16 +483,16 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
                     raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
                 const int gx = cell[0] - 1 + ax;
-                const bool inside = gx >= 0 && gx <= C.W && cell[1] >= 1 && cell[1] + 2 <= C.H && cell[2] >= 1 &&
-                                    cell[2] + 2 <= C.Dp;
+                const bool inside = gx >= 0 && gx <= C.W && cell[1] >= 1 && cell[1] + (S - 2) <= C.H &&
+                                    cell[2] >= 1 && cell[2] + (S - 2) <= C.Dp;
                 if (inside) {
                     const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1 + by0)) * C.nx + gx;
                     const long long sy = C.nx, sz = (long long)C.nx * C.ny;
 #pragma unroll
                     for (int bb = 0; bb < NB; ++bb)
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const int idx = bb * 4 + cc;
+                        for (int cc = 0; cc < S; ++cc) {
+                            const int idx = bb * S + cc;
                             unsigned long long* p0 = acc + (g0 + bb * sy + cc * sz);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -493,10 +502,10 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 } else {
                     bool outside = false;
                     for (int bb = 0; bb < NB; ++bb)
-                        for (int cc = 0; cc < 4; ++cc) {
+                        for (int cc = 0; cc < S; ++cc) {
                             const int gy = cell[1] - 1 + by0 + bb, gz = cell[2] - 1 + cc;
                             if (gx < 0 || gx > C.W || gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
-                            const int idx = bb * 4 + cc;
+                            const int idx = bb * S + cc;
                             unsigned long long* p0 = acc + (((long long)gz * C.ny + gy) * C.nx + gx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -508,16 +517,16 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 if (gx >= 0 && gx <= C.W) {
                     // node blocks holding the thread's in-grid nodes (empty range: none)
                     const int y0 = max(0, cell[1] - 1 + by0), y1 = min(C.H, cell[1] - 2 + by0 + NB);
-                    const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + 2);
+                    const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + (S - 2));
                     if (y0 <= y1 && z0 <= z1)
                         for (int bz = z0 / T; bz <= z1 / T; ++bz)
                             for (int by = y0 / T; by <= y1 / T; ++by)
                                 mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
                 }
             } else {
-                float am[16], a0[16], a1[16];
+                float am[S * S], a0[S * S], a1[S * S];
 #pragma unroll
-                for (int k = 0; k < 16; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
+                for (int k = 0; k < S * S; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
                 for (int j = j0; j < j1; ++j) {
                     const float4* pp = pay + j * (W::PS / 4);
                     const float4 wx = pp[0], wy = pp[1], p2 = pp[2], p3 = pp[3], p4 = pp[4];
@@ -526,15 +535,15 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                     const float Y[4] = {wy.x, wy.y, wy.z, wy.w};
                     float Yd[4];
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) Yd[b] = Y[b] * (float(b - 1) - p2.y);
+                    for (int b = 0; b < S; ++b) Yd[b] = Y[b] * (float(b - 1) - p2.y);
 #pragma unroll
-                    for (int aa = 0; aa < 4; ++aa) {
+                    for (int aa = 0; aa < S; ++aa) {
                         const float X = Xv[aa], Xd = X * (float(aa - 1) - p2.x);
                         const float e0 = p2.w * X + p3.y * Xd, e1 = p3.x * X + p3.w * Xd;
                         const float f0 = p3.z * X, f1 = p4.x * X, mX = p2.z * X;
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            const int idx = aa * 4 + b;
+                        for (int b = 0; b < S; ++b) {
+                            const int idx = aa * S + b;
                             am[idx] += mX * Y[b];
                             a0[idx] += e0 * Y[b] + f0 * Yd[b];
                             a1[idx] += e1 * Y[b] + f1 * Yd[b];
@@ -543,20 +552,20 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 }
                 float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
-                for (int k = 0; k < 16; ++k) {
+                for (int k = 0; k < S * S; ++k) {
                     mx_m = fmaxf(mx_m, fabsf(am[k]));
                     mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fabsf(a1[k])));
                 }
                 if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
                     raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
-                const bool inside = cell[0] >= 1 && cell[0] + 2 <= C.W && cell[1] >= 1 && cell[1] + 2 <= C.H;
+                const bool inside = cell[0] >= 1 && cell[0] + (S - 2) <= C.W && cell[1] >= 1 && cell[1] + (S - 2) <= C.H;
                 if (inside) {
                     const long long g0 = (long long)(cell[1] - 1) * C.nx + (cell[0] - 1);
 #pragma unroll
-                    for (int aa = 0; aa < 4; ++aa)
+                    for (int aa = 0; aa < S; ++aa)
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            const int idx = aa * 4 + b;
+                        for (int b = 0; b < S; ++b) {
+                            const int idx = aa * S + b;
                             unsigned long long* p0 = acc + (g0 + aa + (long long)b * C.nx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -564,11 +573,11 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                         }
                 } else {
                     bool outside = false;
-                    for (int aa = 0; aa < 4; ++aa)
-                        for (int b = 0; b < 4; ++b) {
+                    for (int aa = 0; aa < S; ++aa)
+                        for (int b = 0; b < S; ++b) {
                             const int gx = cell[0] - 1 + aa, gy = cell[1] - 1 + b;
                             if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
-                            const int idx = aa * 4 + b;
+                            const int idx = aa * S + b;
                             unsigned long long* p0 = acc + ((long long)gy * C.nx + gx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -576,8 +585,8 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                         }
                     if (outside) raise_flag(status, 4u);
                 }
-                const int x0 = max(0, cell[0] - 1), x1 = min(C.W, cell[0] + 2);
-                const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + 2);
+                const int x0 = max(0, cell[0] - 1), x1 = min(C.W, cell[0] + (S - 2));
+                const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + (S - 2));
                 if (x0 <= x1 && y0 <= y1)
                     for (int by = y0 / T; by <= y1 / T; ++by)
                         for (int bx = x0 / T; bx <= x1 / T; ++bx) mark_block_once(TI, by * TI.nblk[0] + bx);

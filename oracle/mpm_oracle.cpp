@@ -5,12 +5,16 @@
 //   * double: the FP64 oracle the CUDA solver is checked against;
 //   * float (+ OpenMP): the multi-core CPU baseline ("port") timed by bench.py.
 //
-// Two formulations, both in the reference's grid units (dx = 1, node i at x = i):
+// Three formulations, all in the reference's grid units (dx = 1, node i at x = i):
 //   MLS     — the reference GPU path, src/gpu/shaders/{2d,3d}/{common,p2g,
 //             grid_update,g2p}.glsl (force folded into momentum, C = 3 B).
 //   CLASSIC — the reference CPU path, src/cpu/{Grid,Particles}.cpp (separate
 //             grid force f = sum grad(w) A_p, grad(v) = sum v_col (x) grad(w),
 //             Eigen JacobiSVD conventions). 2D only, as in the reference.
+//   QUAD    — the MLS step on the quadratic B-spline stencil (3 nodes per axis
+//             from floor(x - 1/2), C = 4 B, stress factor 4); the reference has
+//             no quadratic variant, so this is the MLS restatement with the
+//             textbook quadratic kernel and D^-1 = 4 substituted.
 //
 // Every function cites the reference lines it restates. Matrices are row-major
 // (M[r*D+c]); GLSL mat constructors are column-major and are translated here.
@@ -30,7 +34,7 @@
 
 namespace orc {
 
-enum { MLS = 0, CLASSIC = 1 };
+enum { MLS = 0, CLASSIC = 1, QUAD = 2 };
 enum { BOUNDARY_FRICTION = 0, BOUNDARY_STICKY = 1 };
 
 template <typename R> struct Params {
@@ -46,6 +50,22 @@ template <typename R> inline R bspline_n(R x) {
     if (a < R(2)) { R t = R(2) - a; return t * t * t / R(6); }
     return R(0);
 }
+// Quadratic B-spline (QUAD): 3/4 - x^2 for |x| < 1/2, (3/2 - |x|)^2 / 2 for |x| < 3/2.
+template <typename R> inline R quad_n(R x) {
+    R a = std::fabs(x);
+    if (a < R(0.5)) return R(0.75) - a * a;
+    if (a < R(1.5)) { R t = R(1.5) - a; return R(0.5) * t * t; }
+    return R(0);
+}
+
+// Stencil of a formulation: first node per axis, nodes per axis, weight, D^-1.
+inline int stencil_nodes(int form) { return form == QUAD ? 3 : 4; }
+template <typename R> inline int stencil_first(R x, int form) {
+    return form == QUAD ? int(std::floor(x - R(0.5))) : int(x) - 1;
+}
+template <typename R> inline R stencil_w(R d, int form) { return form == QUAD ? quad_n(d) : bspline_n(d); }
+template <typename R> inline R stencil_dinv(int form) { return form == QUAD ? R(4) : R(3); }
+
 template <typename R> inline R bspline_dn(R x) {
     R a = std::fabs(x);
     if (a < R(1)) return R(1.5) * a * x - R(2) * x;
@@ -349,7 +369,10 @@ template <int D, typename R> void p2g(const Params<R>& p, State<D, R>& s, Grid<D
         const R* Fp = s.Fp + pi * D * D;
         const R mass = s.mass[pi], vol = s.vol[pi];
         R st[D * D];
-        if (p.formulation == MLS) {
+        const bool mls = p.formulation != CLASSIC;
+        const int S = stencil_nodes(p.formulation);
+        const R dinv = stencil_dinv<R>(p.formulation);
+        if (mls) {
             if (vol == R(0)) continue;  // p2g.glsl:42
             stress<D>(p, Fe, Fp, st);
         } else {
@@ -358,10 +381,10 @@ template <int D, typename R> void p2g(const Params<R>& p, State<D, R>& s, Grid<D
             else { stress<D>(p, Fe, Fp, st); for (int i = 0; i < D * D; ++i) st[i] *= vol; }
         }
         int base[3] = {0, 0, 0};
-        for (int k = 0; k < D; ++k) base[k] = int(x[k]) - 1;
-        const int nzs = D == 3 ? 4 : 1;
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b < 4; ++b)
+        for (int k = 0; k < D; ++k) base[k] = stencil_first(x[k], p.formulation);
+        const int nzs = D == 3 ? S : 1;
+        for (int a = 0; a < S; ++a)
+            for (int b = 0; b < S; ++b)
                 for (int c = 0; c < nzs; ++c) {
                     int idx[3] = {base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0};
                     if (idx[0] < 0 || idx[0] > p.width || idx[1] < 0 || idx[1] > p.height) continue;
@@ -370,18 +393,18 @@ template <int D, typename R> void p2g(const Params<R>& p, State<D, R>& s, Grid<D
                     R dist[3], w = R(1), dw[3] = {1, 1, 1}, Nk[3], dNk[3];
                     for (int k = 0; k < D; ++k) {
                         dist[k] = x[k] - R(idx[k]);
-                        Nk[k] = bspline_n(dist[k]);
+                        Nk[k] = stencil_w(dist[k], p.formulation);
                         dNk[k] = bspline_dn(dist[k]);
                         w *= Nk[k];
                     }
                     const R m = w * mass;
-                    if (p.formulation == MLS) {
+                    if (mls) {
                         R wv[3];
                         for (int r = 0; r < D; ++r) {
                             R Bd = 0, Sd = 0;
                             for (int k = 0; k < D; ++k) { Bd += B[r * D + k] * (-dist[k]); Sd += st[r * D + k] * dist[k]; }
-                            R apic = v[r] + R(3) * Bd;
-                            R force = vol * Sd * R(3) * p.dt;
+                            R apic = v[r] + dinv * Bd;
+                            R force = vol * Sd * dinv * p.dt;
                             wv[r] = m * apic + w * force;
                         }
                         add_to(&g.mass[cid], m, atomic);
@@ -416,7 +439,7 @@ template <int D, typename R> void grid_update(const Params<R>& p, Grid<D, R>& g,
         if (m < R(1e-6)) continue;
         R vel[3] = {0, 0, 0}, loc[3] = {0, 0, 0};
         const int gaxis = 1;  // gravity acts along y in 2D and 3D
-        if (p.formulation == MLS) {
+        if (p.formulation != CLASSIC) {
             for (int k = 0; k < D; ++k) vel[k] = g.mom[id * D + k] / m;
             vel[gaxis] += p.gravity * p.dt;
         } else {
@@ -455,12 +478,13 @@ template <int D, typename R> void g2p(const Params<R>& p, State<D, R>& s, const 
         R* Fp = s.Fp + pi * D * D;
         R old[3] = {0, 0, 0};
         for (int k = 0; k < D; ++k) old[k] = x[k];
+        const int NS = stencil_nodes(p.formulation);
         int base[3] = {0, 0, 0};
-        for (int k = 0; k < D; ++k) base[k] = int(old[k]) - 1;
+        for (int k = 0; k < D; ++k) base[k] = stencil_first(old[k], p.formulation);
         R nv[3] = {0, 0, 0}, nx[3] = {0, 0, 0}, nB[9] = {0}, gv[9] = {0};
-        const int nzs = D == 3 ? 4 : 1;
-        for (int a = 0; a < 4; ++a)
-            for (int b = 0; b < 4; ++b)
+        const int nzs = D == 3 ? NS : 1;
+        for (int a = 0; a < NS; ++a)
+            for (int b = 0; b < NS; ++b)
                 for (int c = 0; c < nzs; ++c) {
                     int idx[3] = {base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0};
                     if (idx[0] < 0 || idx[0] > p.width || idx[1] < 0 || idx[1] > p.height) continue;
@@ -469,7 +493,7 @@ template <int D, typename R> void g2p(const Params<R>& p, State<D, R>& s, const 
                     R dist[3], w = R(1), Nk[3], dNk[3];
                     for (int k = 0; k < D; ++k) {
                         dist[k] = old[k] - R(idx[k]);
-                        Nk[k] = bspline_n(dist[k]);
+                        Nk[k] = stencil_w(dist[k], p.formulation);
                         dNk[k] = bspline_dn(dist[k]);
                         w *= Nk[k];
                     }
@@ -492,10 +516,11 @@ template <int D, typename R> void g2p(const Params<R>& p, State<D, R>& s, const 
                 }
         for (int k = 0; k < D; ++k) { v[k] = nv[k]; x[k] = nx[k]; }
         for (int i = 0; i < D * D; ++i) B[i] = nB[i];
-        // F_E_hat = (I + dt L) F_E with L = 3 B (MLS, g2p.glsl:74-75) or grad v (CLASSIC).
+        // F_E_hat = (I + dt L) F_E with L = 3 B (MLS, g2p.glsl:74-75), 4 B (QUAD)
+        // or grad v (CLASSIC).
         R L[D * D], A[D * D], Fh[D * D];
         for (int i = 0; i < D * D; ++i) {
-            L[i] = p.formulation == MLS ? R(3) * nB[i] : gv[i];
+            L[i] = p.formulation != CLASSIC ? stencil_dinv<R>(p.formulation) * nB[i] : gv[i];
             A[i] = ((i % (D + 1) == 0) ? R(1) : R(0)) + p.dt * L[i];
         }
         matmul<D>(A, Fe, Fh);
@@ -557,6 +582,7 @@ static int step_impl(const orc_params* q, int64_t n, R* x, R* v, R* B, R* Fe, R*
                      const R* vol, int32_t nsteps, int32_t threads) {
     if (!q || n < 0 || nsteps < 0) return 1;
     if (q->dim != 2 && q->dim != 3) return 1;
+    if (q->formulation < orc::MLS || q->formulation > orc::QUAD) return 1;
     if (q->dim == 3 && q->formulation == orc::CLASSIC) return 11;  // the reference CPU path is 2D only
     if (threads < 1) threads = 1;
     orc::Params<R> p = to_params<R>(q);
