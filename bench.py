@@ -302,6 +302,32 @@ def batched_scenes(args, torch):
     }
 
 
+def quadratic_variant(args, torch, scene, bytes_per_step_fn):
+    """The same workload on the quadratic stencil (3^d nodes, D^-1 = 4):
+    device time per step with CUDA events on the solver's stream."""
+    from mpm_snow_sim2d_b200 import Solver
+    stream = torch.cuda.Stream()
+    sc = scene.with_(formulation=2)
+    with Solver.from_scene(sc, sort_period=args.sort_period) as q:
+        q.set_stream(stream.cuda_stream)
+        q.Step(args.warmup)
+        m, _ = q.rasterize()
+        active = int((m > 0).sum())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        q.Step(args.quad_steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.quad_steps
+        stages = {k: v / args.quad_steps for k, v in q.step_profiled(args.quad_steps).items()}
+        flags = q.status()
+    step_bytes = bytes_per_step_fn(active)
+    return {"formulation": "MLS quadratic (3^d nodes, D^-1 = 4)", "steps": args.quad_steps, "ms_per_step": ms,
+            "value": scene.count / (ms / 1e3), "unit": UNIT, "stages_ms": stages, "active_nodes": active,
+            "step_achieved_gbs": step_bytes / (ms / 1e3) / 1e9, "status_flags": flags}
+
+
 def cpu_port_time(scene, target_s=12.0, max_steps=20):
     """FP32 OpenMP port of the reference MLS step on all host cores."""
     from oracle import oracle as O
@@ -384,6 +410,7 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-latency-calls", type=int, default=50)
+    ap.add_argument("--quad-steps", type=int, default=500, help="timed steps of the quadratic-stencil line (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -488,6 +515,14 @@ def main():
         except Exception as e:  # reported next to the headline, never required for it
             mlp = {"error": str(e)}
 
+    quad = None
+    if world == 1 and args.quad_steps > 0:
+        try:
+            quad = quadratic_variant(args, torch, scene, lambda act: n * (p2g_b + g2p_b) + act * (grid_b + g2p_nb))
+            quad["step_frac"] = quad["step_achieved_gbs"] / peak
+        except Exception as e:  # reported next to the headline, never required for it
+            quad = {"error": str(e)}
+
     batch = None
     if world == 1 and not args.no_batch:
         try:
@@ -520,6 +555,7 @@ def main():
             "status_flags": flags,
             "cpu_baseline": cpu,
             "mlp_vs_plain": mlp,
+            "quadratic": quad,
             "batched": batch,
         }
         print(json.dumps(line), flush=True)
