@@ -4,11 +4,14 @@
     python -m mpm_snow_sim2d_b200.run impact64 --steps 100 --plasticity mlp
     python -m mpm_snow_sim2d_b200.run c4 --scenes 64 --steps 10 --batch-threads 1024
     python -m mpm_snow_sim2d_b200.run c1 --steps 1000 --frames frames/
+    python -m mpm_snow_sim2d_b200.run c3 --steps 4 --formulation quadratic
+    python -m mpm_snow_sim2d_b200.run reference2d --steps 6600 --frames frames/
 
 Prints the particle count, the device status word and the wall time; used for
 profiling captures and quick checks. Workloads: see scenes.workload(); "impact64" is the training set-up of the
 learned return map (a 6 m/s snowball impact on a slab, 64^3); "c4" the first
-`--scenes` scenes of the batched workload, run as one batch.
+`--scenes` scenes of the batched workload, run as one batch; "reference2d" /
+"reference3d" the reference's default two-snowball scene (scenes.reference_snowballs).
 """
 from __future__ import annotations
 
@@ -24,6 +27,8 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--sort-period", type=int, default=0)
     ap.add_argument("--plasticity", choices=["exact", "mlp"], default="exact")
+    ap.add_argument("--formulation", choices=["mls", "classic", "quadratic"], default=None,
+                    help="override the scene's formulation (quadratic: 3^d-node stencil)")
     ap.add_argument("--frames", default=None, help="write a PNG frame every --frame-steps steps to this directory")
     ap.add_argument("--frame-steps", type=int, default=0,
                     help="steps per frame (0: 1 / (SAVE_FPS dt), SAVE_FPS = 30 as in Parameters.h:69)")
@@ -47,8 +52,14 @@ def main(argv=None) -> int:
     if args.workload == "impact64":
         from .mlp_train import impact_scene
         scene = impact_scene(6.0, seed=777002, W=64, steps=args.steps)
+    elif args.workload in ("reference2d", "reference3d"):
+        # the reference's default two-snowball scene, sampled on the device
+        scene = scenes.reference_snowballs(2 if args.workload == "reference2d" else 3)
     else:
         scene = scenes.workload(args.workload)
+    if args.formulation:
+        scene = scene.with_(formulation={"mls": _lib.FORMULATION_MLS, "classic": _lib.FORMULATION_CLASSIC,
+                                         "quadratic": _lib.FORMULATION_MLS_QUADRATIC}[args.formulation])
     with Solver.from_scene(scene, sort_period=args.sort_period) as s:
         if args.plasticity == "mlp":
             from .mlp import DEFAULT_WEIGHTS, Mlp
