@@ -78,10 +78,27 @@ __device__ __forceinline__ int stencil_base(float x, int extent) {
 // MLS factor D^-1, and the shift that makes floor(x + SHIFT) = base + 1 (the
 // particle's cell for the cubic stencil, its nearest node for the quadratic).
 template <int S> struct Stencil;
+// weights(x, base, w) gives all S weights of a particle at x: the kernel's
+// pieces as polynomials of t = x - (base + 1) where t is in the regular range
+// (every particle whose stencil base came from its own position), else the
+// kernel evaluated node by node (positions clamped far outside the grid).
 template <> struct Stencil<4> {  // cubic, the reference's: nodes int(x) - 1 .. int(x) + 2
     static constexpr float DINV = 3.f, SHIFT = 0.f;
     __device__ static __forceinline__ int base(float x, int ext) { return stencil_base(x, ext); }
     __device__ static __forceinline__ float w(float d) { return bspline_n(d); }
+    __device__ static __forceinline__ void weights(float x, int b, float* wt) {
+        const float t = x - float(b + 1);
+        if (t >= 0.f && t < 1.f) {
+            const float s = 1.f - t, t2 = t * t, t3 = t2 * t;
+            wt[0] = s * s * s * (1.f / 6.f);                           // (2 - |1 + t|)^3 / 6
+            wt[1] = 0.5f * t3 - t2 + (2.f / 3.f);                       // |t|^3 / 2 - t^2 + 2/3
+            wt[2] = (0.5f * t2 - 0.5f * t3) + (0.5f * t + (1.f / 6.f));  // the inner piece at 1 - t
+            wt[3] = t3 * (1.f / 6.f);                                   // (2 - |t - 2|)^3 / 6
+            return;
+        }
+#pragma unroll
+        for (int o = 0; o < 4; ++o) wt[o] = bspline_n(x - float(b + o));
+    }
 };
 template <> struct Stencil<3> {  // quadratic: nodes floor(x - 1/2) .. floor(x - 1/2) + 2
     static constexpr float DINV = 4.f, SHIFT = 0.5f;
@@ -89,6 +106,18 @@ template <> struct Stencil<3> {  // quadratic: nodes floor(x - 1/2) .. floor(x -
         return int(floorf(fminf(fmaxf(x, -8.f), float(ext) + 8.f) - 0.5f));
     }
     __device__ static __forceinline__ float w(float d) { return quad_n(d); }
+    __device__ static __forceinline__ void weights(float x, int b, float* wt) {
+        const float t = x - float(b + 1);
+        if (t >= -0.5f && t < 0.5f) {
+            const float a = 0.5f - t, c = 0.5f + t;
+            wt[0] = 0.5f * a * a;
+            wt[1] = 0.75f - t * t;
+            wt[2] = 0.5f * c * c;
+            return;
+        }
+#pragma unroll
+        for (int o = 0; o < 3; ++o) wt[o] = quad_n(x - float(b + o));
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -753,10 +782,13 @@ __device__ __forceinline__ int queue_slot(const SlowQueue& Q) {
 }
 
 #ifndef MPM_G2P_MIN_BLOCKS
-#define MPM_G2P_MIN_BLOCKS 2
+#define MPM_G2P_MIN_BLOCKS 4
+#endif
+#ifndef MPM_G2P_MIN_BLOCKS_Q
+#define MPM_G2P_MIN_BLOCKS_Q 4
 #endif
 template <int D, int S = 4>
-__global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
+__global__ void __launch_bounds__(256, S == 3 ? MPM_G2P_MIN_BLOCKS_Q : MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particles P, StepConsts C, const float4* __restrict__ gv,
                                                        SlowQueue Q, unsigned* __restrict__ status) {
     using St = Stencil<S>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -773,12 +805,9 @@ __global__ void __launch_bounds__(256, MPM_G2P_MIN_BLOCKS) k_g2p_gather(Particle
         const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
         base[k] = St::base(x[k], ext);
         interior = interior && base[k] >= 0 && base[k] + (S - 1) <= ext;
+        St::weights(x[k], base[k], wk[k]);
 #pragma unroll
-        for (int o = 0; o < S; ++o) {
-            const float dist = x[k] - float(base[k] + o);
-            wk[k][o] = St::w(dist);
-            off[k][o] = -dist;
-        }
+        for (int o = 0; o < S; ++o) off[k][o] = float(base[k] + o) - x[k];
     }
     if (!interior) {  // stencil partly outside the grid: the general kernel does it all
         Q.list[queue_slot(Q)] = -1 - i;

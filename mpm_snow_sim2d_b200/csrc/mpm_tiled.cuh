@@ -326,8 +326,15 @@ template <int D, int S = 4> struct WarpGeom;
 // and 16 / SPLIT of the y-offsets) x 4 channels.
 template <> struct WarpGeom<3, 4> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 36; };
 template <> struct WarpGeom<2, 4> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
-// quadratic: 3 threads per run in 3D (one per x-offset, 9 nodes each)
-template <> struct WarpGeom<3, 3> { static constexpr int CHUNK = 48, SPLIT = 3, PS = 36; };
+// quadratic: MPM_P2G_SPLIT3Q threads per run in 3D (3: one per x-offset, 9
+// nodes each; 9: one per (x, y)-offset, 3 nodes each)
+#ifndef MPM_P2G_CHUNK3Q
+#define MPM_P2G_CHUNK3Q 48
+#endif
+#ifndef MPM_P2G_SPLIT3Q
+#define MPM_P2G_SPLIT3Q 3
+#endif
+template <> struct WarpGeom<3, 3> { static constexpr int CHUNK = MPM_P2G_CHUNK3Q, SPLIT = MPM_P2G_SPLIT3Q, PS = 36; };
 template <> struct WarpGeom<2, 3> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
 constexpr int kP2GWarps = 8;
 
@@ -382,8 +389,10 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
                 const float x = P.x[k * n + i];
                 const int base = St::base(x, extk);
+                float wt[S];
+                St::weights(x, base, wt);
 #pragma unroll
-                for (int o = 0; o < 4; ++o) q[4 * k + o] = o < S ? St::w(x - float(base + o)) : 0.f;
+                for (int o = 0; o < 4; ++o) q[4 * k + o] = o < S ? wt[o] : 0.f;
                 f[k] = x - float(base + 1);
                 mv[k] = mass * P.v[k * n + i];
                 k3 = k3 * (extk + 18) + (base + 9);  // cell key: base + 9 >= 0
