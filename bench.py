@@ -46,7 +46,7 @@ UNIT = "particle-updates/s"
 DEFAULT_SORT_PERIOD = 16  # the solver's re-sort interval when mpm_params.sort_period is 0
 # DRAM bytes (read + write) per launch of the dominant kernels, from one full
 # ncu capture of the same scene (dram__bytes_read.sum + dram__bytes_write.sum).
-NCU_TRAFFIC = {("c3", "p2g"): 113.1e6, ("c3", "g2p"): 254.4e6}
+NCU_TRAFFIC = {("c3", "p2g"): 113.1e6, ("c3", "g2p"): 315.1e6}
 
 # Algorithmic bytes (minimal FP32 SoA state, uniform mass/volume).
 # Per particle-step: P2G reads x, v, B, F_E, J_p; G2P reads x, F_E, J_p and
