@@ -301,7 +301,7 @@ namespace mpm {
 // WarpGeom<D, S>::CHUNK slots; each warp takes one chunk at a time, with no
 // CTA-wide synchronisation. In the chunk, maximal runs of consecutive slots
 // whose particles share their current stencil are grouped; SPLIT threads per
-// run [3D: one per (x-offset, share of the y-offsets)] or one per run [2D]
+// run [3D: one per (x-offset, share of the y-offsets); 2D: one per x-offset]
 // accumulate the run's S^D nodes x (1 + D) channels in FP32 registers, in slot
 // order, and add them as int64 fixed point to the global sums. S is the
 // stencil width: 4 (cubic) or 3 (quadratic; unused payload entries are 0). The grouping is a function of the slot order (the
@@ -325,7 +325,14 @@ template <int D, int S = 4> struct WarpGeom;
 // 3D: SPLIT threads per run, each holding 16 * 4 / SPLIT nodes (x-offset a,
 // and 16 / SPLIT of the y-offsets) x 4 channels.
 template <> struct WarpGeom<3, 4> { static constexpr int CHUNK = MPM_P2G_CHUNK3, SPLIT = MPM_P2G_SPLIT3, PS = 36; };
-template <> struct WarpGeom<2, 4> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
+// 2D: MPM_P2G_SPLIT2 threads per run (1: all 16 nodes; 4: one node column each)
+#ifndef MPM_P2G_SPLIT2
+#define MPM_P2G_SPLIT2 4
+#endif
+#ifndef MPM_P2G_CHUNK2
+#define MPM_P2G_CHUNK2 64
+#endif
+template <> struct WarpGeom<2, 4> { static constexpr int CHUNK = MPM_P2G_CHUNK2, SPLIT = MPM_P2G_SPLIT2, PS = 20; };
 // quadratic: MPM_P2G_SPLIT3Q threads per run in 3D (3: one per x-offset, 9
 // nodes each; 9: one per (x, y)-offset, 3 nodes each)
 #ifndef MPM_P2G_CHUNK3Q
@@ -335,7 +342,9 @@ template <> struct WarpGeom<2, 4> { static constexpr int CHUNK = 128, SPLIT = 1,
 #define MPM_P2G_SPLIT3Q 3
 #endif
 template <> struct WarpGeom<3, 3> { static constexpr int CHUNK = MPM_P2G_CHUNK3Q, SPLIT = MPM_P2G_SPLIT3Q, PS = 36; };
-template <> struct WarpGeom<2, 3> { static constexpr int CHUNK = 128, SPLIT = 1, PS = 20; };
+template <> struct WarpGeom<2, 3> {
+    static constexpr int CHUNK = MPM_P2G_CHUNK2, SPLIT = MPM_P2G_SPLIT2 == 1 ? 1 : 3, PS = 20;
+};
 constexpr int kP2GWarps = 8;
 
 template <int D, int S = 4> struct P2GWarpSmem {
@@ -357,8 +366,11 @@ __device__ __forceinline__ void red_fixed(unsigned long long* p, float v, float 
 #ifndef MPM_P2G_MIN_BLOCKS
 #define MPM_P2G_MIN_BLOCKS 3
 #endif
+#ifndef MPM_P2G_MIN_BLOCKS_2D
+#define MPM_P2G_MIN_BLOCKS_2D 2
+#endif
 template <int D, int S = 4>
-__global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 2) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
+__global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : MPM_P2G_MIN_BLOCKS_2D) k_p2g_warp(Particles P, StepConsts C, TileInfo TI,
                                                               unsigned long long* __restrict__ acc,
                                                               unsigned* __restrict__ status) {
     using W = WarpGeom<D, S>;
@@ -533,9 +545,13 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                                 mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
                 }
             } else {
-                float am[S * S], a0[S * S], a1[S * S];
+                // 2D: SPLIT threads per run, each holding NA = S / SPLIT x-offsets
+                // (all S y-offsets) x 3 channels
+                constexpr int NA = S / W::SPLIT;
+                const int gx0 = cell[0] - 1 + a * NA;  // first node column of this thread
+                float am[NA * S], a0[NA * S], a1[NA * S];
 #pragma unroll
-                for (int k = 0; k < S * S; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
+                for (int k = 0; k < NA * S; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
                 for (int j = j0; j < j1; ++j) {
                     const float4* pp = pay + j * (W::PS / 4);
                     const float4 wx = pp[0], wy = pp[1], p2 = pp[2], p3 = pp[3], p4 = pp[4];
@@ -546,13 +562,15 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
 #pragma unroll
                     for (int b = 0; b < S; ++b) Yd[b] = Y[b] * (float(b - 1) - p2.y);
 #pragma unroll
-                    for (int aa = 0; aa < S; ++aa) {
-                        const float X = Xv[aa], Xd = X * (float(aa - 1) - p2.x);
+                    for (int i = 0; i < NA; ++i) {
+                        const int aa = a * NA + i;
+                        const float X = NA == S ? Xv[i] : payf[j * W::PS + aa];
+                        const float Xd = X * (float(aa - 1) - p2.x);
                         const float e0 = p2.w * X + p3.y * Xd, e1 = p3.x * X + p3.w * Xd;
                         const float f0 = p3.z * X, f1 = p4.x * X, mX = p2.z * X;
 #pragma unroll
                         for (int b = 0; b < S; ++b) {
-                            const int idx = aa * S + b;
+                            const int idx = i * S + b;
                             am[idx] += mX * Y[b];
                             a0[idx] += e0 * Y[b] + f0 * Yd[b];
                             a1[idx] += e1 * Y[b] + f1 * Yd[b];
@@ -561,32 +579,32 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 }
                 float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
-                for (int k = 0; k < S * S; ++k) {
+                for (int k = 0; k < NA * S; ++k) {
                     mx_m = fmaxf(mx_m, fabsf(am[k]));
                     mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fabsf(a1[k])));
                 }
                 if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
                     raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
-                const bool inside = cell[0] >= 1 && cell[0] + (S - 2) <= C.W && cell[1] >= 1 && cell[1] + (S - 2) <= C.H;
+                const bool inside = gx0 >= 0 && gx0 + (NA - 1) <= C.W && cell[1] >= 1 && cell[1] + (S - 2) <= C.H;
                 if (inside) {
-                    const long long g0 = (long long)(cell[1] - 1) * C.nx + (cell[0] - 1);
+                    const long long g0 = (long long)(cell[1] - 1) * C.nx + gx0;
 #pragma unroll
-                    for (int aa = 0; aa < S; ++aa)
+                    for (int i = 0; i < NA; ++i)
 #pragma unroll
                         for (int b = 0; b < S; ++b) {
-                            const int idx = aa * S + b;
-                            unsigned long long* p0 = acc + (g0 + aa + (long long)b * C.nx);
+                            const int idx = i * S + b;
+                            unsigned long long* p0 = acc + (g0 + i + (long long)b * C.nx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
                             red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
                         }
                 } else {
                     bool outside = false;
-                    for (int aa = 0; aa < S; ++aa)
+                    for (int i = 0; i < NA; ++i)
                         for (int b = 0; b < S; ++b) {
-                            const int gx = cell[0] - 1 + aa, gy = cell[1] - 1 + b;
+                            const int gx = gx0 + i, gy = cell[1] - 1 + b;
                             if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
-                            const int idx = aa * S + b;
+                            const int idx = i * S + b;
                             unsigned long long* p0 = acc + ((long long)gy * C.nx + gx);
                             red_fixed(p0, am[idx], C.sm);
                             red_fixed(p0 + C.nodes, a0[idx], C.sp);
@@ -594,7 +612,7 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                         }
                     if (outside) raise_flag(status, 4u);
                 }
-                const int x0 = max(0, cell[0] - 1), x1 = min(C.W, cell[0] + (S - 2));
+                const int x0 = max(0, gx0), x1 = min(C.W, gx0 + (NA - 1));
                 const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + (S - 2));
                 if (x0 <= x1 && y0 <= y1)
                     for (int by = y0 / T; by <= y1 / T; ++by)
