@@ -167,12 +167,9 @@ __device__ __forceinline__ void batch_p2g(const BatchBuffers& P, long long N, co
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             base[k] = stencil_base(x[k], ext[k]);
+            Stencil<4>::weights(x[k], base[k], wk[k]);
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
-                const float dist = x[k] - float(base[k] + o);
-                wk[k][o] = bspline_n(dist);
-                off[k][o] = -dist;
-            }
+            for (int o = 0; o < 4; ++o) off[k][o] = float(base[k] + o) - x[k];
         }
         bool outside = false;
 #pragma unroll
@@ -222,12 +219,9 @@ __device__ __forceinline__ void batch_g2p(const BatchBuffers& P, long long N, co
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             base[k] = stencil_base(x[k], ext[k]);
+            Stencil<4>::weights(x[k], base[k], wk[k]);
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
-                const float dist = x[k] - float(base[k] + o);
-                wk[k][o] = bspline_n(dist);
-                off[k][o] = -dist;
-            }
+            for (int o = 0; o < 4; ++o) off[k][o] = float(base[k] + o) - x[k];
         }
         uint32_t row[4];
         bool row_in[4];
