@@ -270,14 +270,18 @@ REFERENCE_DEFAULT = dict(width=200, height=100, depth=100, margin=2, radius=15.0
                          nu=0.2, youngs=1.4e5, rho=400.0)
 
 
-def reference_snowballs(dim: int = 2, seed: int = 1, steps: int = 6600, rounds: int = 30) -> Scene:
+def reference_snowballs(dim: int = 2, seed: int = 1, steps: int = 6600, rounds: int = 30, sampler=None) -> Scene:
     """The reference's two-snowball scene with particles from the device
     Poisson-disk sampler (needs a GPU). Per snowball, as
     src/gpu/GPUSolver.cpp:99-155: min_dist = radius / NUM_PARTICLES^(1/dim),
     vol = (2 pi r^2 in 2D | 4/3 pi r^3 in 3D) / samples, mass = vol RHO / 100.
     The default 6600 steps are the reference's 200 frames at 30 frames/s.
+    `sampler(dim, shapes, min_dist, seed, rounds)` replaces the device sampler
+    (a restatement with the same output, for fixtures made without a GPU).
     """
     from .sampling import ball, sample_shapes
+
+    sample_shapes = sampler or sample_shapes
 
     R = REFERENCE_DEFAULT
     r = R["radius"]

@@ -5,7 +5,7 @@ reference, compiled unmodified by oracle/build_oracle.py) on small seeded
 scenes and stores the particle state after selected steps, together with the
 scene itself, as compressed .npz files in this directory.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 Needs the reference tree (to build the driver); the fixtures it writes are
 committed so that tests run without it.
@@ -25,7 +25,24 @@ from mpm_snow_sim2d_b200 import scenes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from oracle.build_oracle import build_refcpu  # noqa: E402
 
+def _reference_default_2d():
+    """The reference's default 2D scene (src/shared/Parameters.h:30-80) with the
+    particles the device sampler draws for seed 11, here from its bit-exact CPU
+    restatement (oracle/sample_ref.py)."""
+    from oracle import sample_ref
+
+    def sampler(dim, shapes, md, seed, rounds):
+        full = [dict(kind=s["kind"], center=tuple(s["center"]) + (0.0,) * (3 - len(s["center"])),
+                     radius=s["radius"], half=tuple(s["half"]) + (0.0,) * (3 - len(s["half"]))) for s in shapes]
+        return sample_ref.sample_shapes(dim, full, md, seed, rounds)
+
+    return scenes.reference_snowballs(2, seed=11, sampler=sampler)
+
+
 CASES = {
+    # the reference's own default scene: two snowballs thrown at each other, 12,686
+    # particles, dt 1e-3; they meet near step 875
+    "refcpu_reference_default2d": dict(scene=_reference_default_2d, dumps=(1, 500, 1000)),
     # three falling blocks, 1 particle per cell (1106 particles), 1000 steps of dt 1e-4
     "refcpu_blocks2d_ppc1": dict(scene=lambda: scenes.snow_blocks_2d(ppc=1, seed=2001), dumps=(1, 10, 100, 1000)),
     # one block driven into the floor: wall separation, Coulomb friction and plastic flow
@@ -55,12 +72,14 @@ def save_case(name: str, scene, dumps) -> Path:
     return path
 
 
-def main() -> None:
+def main(names=None) -> None:
     if build_refcpu() is None:
         raise SystemExit("the reference tree is needed to build oracle/_ref/refcpu_driver")
     for name, case in CASES.items():
+        if names and name not in names:
+            continue
         save_case(name, case["scene"](), case["dumps"])
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -127,7 +127,7 @@ def test_mls_3d_snowball_slab_1000_steps(gpu_lib, oracle_mod):
     _check_vs_fp32_reference(state_errors(got[1000], ref[1000], 3), r32[1000], "step 1000")
 
 
-@pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d"])
+@pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d", "refcpu_reference_default2d"])
 def test_classic_matches_reference_cpu(gpu_lib, oracle_mod, case):
     """CLASSIC formulation vs the reference's compiled src/cpu (golden fixtures).
     Both are FP32 with different operation order; each is held to the FP64

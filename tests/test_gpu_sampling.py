@@ -87,3 +87,14 @@ def test_reference_default_scene_against_oracle(gpu_lib, oracle_mod, dim, steps)
     _check_vs_fp32_reference(state_errors(got[1], ref[1], dim), r32[1], f"{dim}D step 1", TIGHT)
     for s in steps[1:]:
         _check_vs_fp32_reference(state_errors(got[s], ref[s], dim), r32[s], f"{dim}D step {s}", TARGET)
+
+
+def test_reference_default_scene_matches_golden_fixture(gpu_lib):
+    """The fixture refcpu_reference_default2d was made without a GPU from the
+    sampler's CPU restatement; the device must draw the same particles."""
+    from golden_io import load_case
+    from mpm_snow_sim2d_b200 import scenes
+    sc = scenes.reference_snowballs(2, seed=11)
+    golden, _ = load_case("refcpu_reference_default2d")
+    assert np.array_equal(sc.position.view(np.uint32), golden.position.view(np.uint32))
+    assert np.array_equal(sc.volume, golden.volume) and np.array_equal(sc.velocity, golden.velocity)

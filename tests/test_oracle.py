@@ -49,10 +49,18 @@ BANDS = {
         200: dict(x=5e-5, v=8e-4, B=2.5e-4, F=8e-5, Jp=6e-5),
         400: dict(x=1.2e-4, v=3e-3, B=2e-4, F=2e-4, Jp=1.2e-4),
     },
+    # the reference's default scene: free flight to step ~875 (the FP32 position
+    # update sum w (x_i + dt v_i) with x_i ~ 100 drifts systematically), then
+    # the collision with plastic flow
+    "refcpu_reference_default2d": {
+        1: dict(x=5e-7, v=5e-7, B=2e-7, F=6e-7, Jp=6e-7),
+        500: dict(x=1e-4, v=8e-5, B=1e-6, F=3e-6, Jp=2e-6),
+        1000: dict(x=2e-4, v=1e-3, B=2e-4, F=4e-4, Jp=5e-4),
+    },
 }
 
 
-@pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d"])
+@pytest.mark.parametrize("case", ["refcpu_blocks2d_ppc1", "refcpu_impact2d", "refcpu_reference_default2d"])
 def test_oracle_classic_matches_reference_cpu(oracle_mod, case):
     """FP64 restatement of src/cpu vs the reference's compiled CPU code."""
     scene, dumps = load_case(case)
