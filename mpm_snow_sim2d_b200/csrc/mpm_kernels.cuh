@@ -482,6 +482,21 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
     const int nzs = (D == 3) ? S : 1;
     float wsum = 0.f;
     bool clipped = false;
+    // CLASSIC grad v = sum v_col (x) grad w. With the whole stencil in the grid,
+    // sum grad w = 0, so any constant may be taken off v_col first: the
+    // particle's old velocity, which leaves small differences to sum instead
+    // of ~|v| terms that cancel (the reference sums v_col itself; the exact
+    // value is the same).
+    float vref[3] = {0.f, 0.f, 0.f};
+    if (FORM == kClassic) {
+        bool whole = true;
+#pragma unroll
+        for (int k = 0; k < D; ++k) whole = whole && base[k] >= 0 && base[k] + (S - 1) <= lim[k];
+        if (whole) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) vref[k] = P.v[k * n + i];
+        }
+    }
 #pragma unroll
     for (int a = 0; a < S; ++a) {
         const int ix = base[0] + a;
@@ -520,7 +535,7 @@ __global__ void __launch_bounds__(256) k_g2p_simple(Particles P, StepConsts C, c
 #pragma unroll
                     for (int r = 0; r < D; ++r)
 #pragma unroll
-                        for (int k = 0; k < D; ++k) gvel[r * D + k] += vc[r] * dw[k];
+                        for (int k = 0; k < D; ++k) gvel[r * D + k] += (vc[r] - vref[r]) * dw[k];
                 }
             }
         }
