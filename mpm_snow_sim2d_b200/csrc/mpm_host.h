@@ -16,6 +16,10 @@ inline mpm_status validate_params(const mpm_params* p, std::string& why) {
     if (p->width < 1 || p->height < 1 || (p->dim == 3 && p->depth < 1)) { why = "grid extent must be >= 1 cell"; return MPM_ERR_INVALID_ARGUMENT; }
     const double nodes = double(p->width + 1) * (p->height + 1) * (p->dim == 3 ? p->depth + 1 : 1);
     if (nodes > 2.0e9) { why = "grid too large"; return MPM_ERR_INVALID_ARGUMENT; }
+    if (p->dim == 3 && (p->width > 2000000 || p->height > 2000000 || p->depth > 2000000)) {
+        why = "3D grid extents are limited to 2,000,000 cells per axis";  // 21-bit stencil keys in P2G
+        return MPM_ERR_INVALID_ARGUMENT;
+    }
     if (!(p->delta_time > 0.f) || !std::isfinite(p->delta_time)) { why = "delta_time must be > 0"; return MPM_ERR_INVALID_ARGUMENT; }
     if (p->formulation != MPM_FORMULATION_MLS && p->formulation != MPM_FORMULATION_CLASSIC &&
         p->formulation != MPM_FORMULATION_MLS_QUADRATIC) { why = "unknown formulation"; return MPM_ERR_INVALID_ARGUMENT; }

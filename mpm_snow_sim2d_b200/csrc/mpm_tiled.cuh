@@ -347,10 +347,18 @@ template <> struct WarpGeom<2, 3> {
 };
 constexpr int kP2GWarps = 8;
 
+// A particle's stencil as one word: base + 9 (>= 0) per axis in KEY_BITS-bit
+// fields, so that runs compare one word and decode with shifts.
+template <int D> struct StencilKey {
+    static constexpr int BITS = D == 3 ? 21 : 32;
+    static constexpr unsigned long long MASK = (1ull << BITS) - 1;
+};
+constexpr unsigned long long kNoStencil = ~0ull;
+
 template <int D, int S = 4> struct P2GWarpSmem {
     using W = WarpGeom<D, S>;
     float4 pay[kP2GWarps][W::CHUNK * W::PS / 4];
-    int key[kP2GWarps][W::CHUNK];
+    unsigned long long key[kP2GWarps][W::CHUNK];  // stencil key (kNoStencil: nothing to scatter)
     int run[kP2GWarps][W::CHUNK + 1];
 };
 
@@ -381,7 +389,7 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float4* pay = SM.pay[wid];
     float* payf = reinterpret_cast<float*>(pay);
-    int* key = SM.key[wid];
+    unsigned long long* key = SM.key[wid];
     int* run = SM.run[wid];
     const int n = P.n;
     const int nchunks = (n + W::CHUNK - 1) / W::CHUNK;
@@ -392,9 +400,9 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
             const int i = s0 + j;
             const float mass = P.mass ? P.mass[i] : P.mass_u;
             const float vol = P.vol ? P.vol[i] : P.vol_u;
-            if (vol == 0.f) { key[j] = -1; continue; }  // p2g.glsl:42
+            if (vol == 0.f) { key[j] = kNoStencil; continue; }  // p2g.glsl:42
             float* q = payf + j * W::PS;
-            int k3 = 0;
+            unsigned long long k3 = 0;
             float f[3], mv[3];
 #pragma unroll
             for (int k = D - 1; k >= 0; --k) {
@@ -407,7 +415,7 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
                 for (int o = 0; o < 4; ++o) q[4 * k + o] = o < S ? wt[o] : 0.f;
                 f[k] = x - float(base + 1);
                 mv[k] = mass * P.v[k * n + i];
-                k3 = k3 * (extk + 18) + (base + 9);  // cell key: base + 9 >= 0
+                k3 |= (unsigned long long)(base + 9) << (StencilKey<D>::BITS * k);  // base + 9 >= 0
             }
             if constexpr (D == 3) {
                 float A[9];
@@ -444,15 +452,12 @@ __global__ void __launch_bounds__(kP2GWarps * 32, D == 3 ? MPM_P2G_MIN_BLOCKS : 
         for (int u = lane; u < nruns * W::SPLIT; u += 32) {
             const int r = u / W::SPLIT, a = u % W::SPLIT;
             const int j0 = run[r], j1 = run[r + 1];
-            int kk = key[j0];
-            if (kk < 0) continue;
+            const unsigned long long kk = key[j0];
+            if (kk == kNoStencil) continue;
             int cell[3] = {0, 0, 0};
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-                cell[k] = kk % (extk + 18) - 8;  // stored base + 9; cell = base + 1
-                kk /= (extk + 18);
-            }
+            for (int k = 0; k < D; ++k)  // stored base + 9; cell = base + 1
+                cell[k] = int((kk >> (StencilKey<D>::BITS * k)) & StencilKey<D>::MASK) - 8;
             if constexpr (D == 3) {
                 constexpr int NB = S * S / W::SPLIT;  // y-offsets per thread
                 constexpr int NN = NB * S;            // nodes per thread
