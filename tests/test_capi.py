@@ -74,6 +74,12 @@ def test_create_rejects_bad_arguments(lib):
     bad = MpmParams.from_buffer_copy(p)
     bad.dim, bad.formulation = 3, 1
     assert lib.mpm_create(C.byref(bad), C.byref(init), C.byref(h)) == 10
+    bad = MpmParams.from_buffer_copy(p)
+    bad.formulation = 3  # unknown (0 MLS, 1 CLASSIC, 2 quadratic)
+    assert lib.mpm_create(C.byref(bad), C.byref(init), C.byref(h)) == 1
+    bad = MpmParams.from_buffer_copy(p)
+    bad.dim, bad.width, bad.height, bad.depth = 3, 2_000_001, 10, 10  # past the 3D per-axis cap
+    assert lib.mpm_create(C.byref(bad), C.byref(init), C.byref(h)) == 1
     assert lib.mpm_create(C.byref(p), None, C.byref(h)) == 1
 
 
