@@ -191,7 +191,12 @@ mpm_status mpm_sample_shapes(int32_t dim, const mpm_shape* shapes, int32_t nshap
         return MPM_ERR_OUT_OF_MEMORY;
     }
     mpm_status st = MPM_OK;
-    cudaMemset(cells, 0, sizeof(float4) * ncells);
+    if (cudaMemset(cells, 0, sizeof(float4) * ncells) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(cells);
+        cudaFree(live);
+        return MPM_ERR_CUDA;
+    }
     const int threads = 256;
     k_sample_live<<<(unsigned)((ncells + threads - 1) / threads), threads>>>(G, S, ncells, live);
     const int pz_n = dim == 3 ? 3 : 1;
