@@ -650,12 +650,14 @@ mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, 
     if (uni_m && n > 0) s->mass_u = massv[0];
     else if (n > 0) {
         if (dalloc(&s->mass, (size_t)n)) return bail(MPM_ERR_OUT_OF_MEMORY);
-        cudaMemcpy(s->mass, massv.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+        if (cudaMemcpy(s->mass, massv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(MPM_ERR_CUDA);
     }
     if (uni_v && n > 0) s->vol_u = volv[0];
     else if (n > 0) {
         if (dalloc(&s->vol, (size_t)n)) return bail(MPM_ERR_OUT_OF_MEMORY);
-        cudaMemcpy(s->vol, volv.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+        if (cudaMemcpy(s->vol, volv.data(), sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(MPM_ERR_CUDA);
     }
 
     // SoA upload: F_E = I, B = 0, J_p = 1 (Particle ctor, src/cpu/Particles.cpp:7-19).
