@@ -218,7 +218,8 @@ template <int D, int S> cudaError_t launch_sort(mpm_solver* s) {
     k_sort_count<D, S><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
     k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
     k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
-    k_tile_sort<D, S><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C, s->ti);
+    k_tile_sort<D, S><<<s->sms * SortGeom<D>::CTAS_PER_SM, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C,
+                                                                               s->ti);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     swap_buffers(s);

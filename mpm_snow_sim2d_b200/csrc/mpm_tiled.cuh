@@ -37,7 +37,7 @@ struct TileInfo {
     int* perm;         // sort scratch: slot order by tile (source slots)
     int* tile_list;    // non-empty tiles of the last sort
     int* n_tile_list;  // device scalar
-    unsigned long long* skey;  // global sort scratch (tiles above kSortSmem particles)
+    unsigned long long* skey;  // global sort scratch (tiles above SortGeom<D>::SMEM particles)
     int* sval;
 };
 
@@ -77,38 +77,58 @@ __global__ void __launch_bounds__(256) k_sort_count(Particles P, StepConsts C, T
 
 // Single-CTA exclusive scans of the tile counts and of the non-empty tiles;
 // writes each tile's first slot and the list of non-empty tiles, and clears
-// the cursors for the bucket pass.
+// the cursors for the bucket pass. Rounds of 1024 consecutive tiles (coalesced
+// loads, eight rounds' loads issued together), each a warp-shuffle scan plus a
+// scan of the 32 warp totals.
 __global__ void __launch_bounds__(1024) k_sort_scan(TileInfo TI) {
-    __shared__ int s_cnt[1024], s_ne[1024];
-    const int nt = TI.n_tiles, tid = threadIdx.x;
-    const int chunk = (nt + 1023) / 1024;
-    const int lo = min(nt, tid * chunk), hi = min(nt, lo + chunk);
-    int c = 0, ne = 0;
-    for (int t = lo; t < hi; ++t) {
-        const int n = TI.tile_count[t];
-        c += n;
-        ne += n > 0;
-    }
-    s_cnt[tid] = c;
-    s_ne[tid] = ne;
+    constexpr int R = 8;
+    __shared__ int s_wc[32], s_wn[32], s_tc, s_tn, s_base, s_lbase;
+    const int nt = TI.n_tiles, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_base = 0; s_lbase = 0; }
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scans
-        const int a = tid >= off ? s_cnt[tid - off] : 0;
-        const int d = tid >= off ? s_ne[tid - off] : 0;
-        __syncthreads();
-        s_cnt[tid] += a;
-        s_ne[tid] += d;
-        __syncthreads();
+    for (int r0 = 0; r0 < nt; r0 += 1024 * R) {
+        int cv[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const int idx = r0 + q * 1024 + tid;
+            cv[q] = idx < nt ? TI.tile_count[idx] : 0;
+        }
+#pragma unroll 1
+        for (int q = 0; q < R && r0 + q * 1024 < nt; ++q) {
+            const int idx = r0 + q * 1024 + tid;
+            const int c = cv[q], ne = c > 0;
+            int ic = c, in = ne;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, ic, off), v = __shfl_up_sync(0xffffffffu, in, off);
+                if (lane >= off) { ic += u; in += v; }
+            }
+            if (lane == 31) { s_wc[warp] = ic; s_wn[warp] = in; }
+            __syncthreads();
+            if (warp == 0) {
+                const int wc = s_wc[lane], wn = s_wn[lane];
+                int jc = wc, jn = wn;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, jc, off), v = __shfl_up_sync(0xffffffffu, jn, off);
+                    if (lane >= off) { jc += u; jn += v; }
+                }
+                s_wc[lane] = jc - wc;  // exclusive warp offsets
+                s_wn[lane] = jn - wn;
+                if (lane == 31) { s_tc = jc; s_tn = jn; }
+            }
+            __syncthreads();
+            if (idx < nt) {
+                TI.tile_start[idx] = s_base + s_wc[warp] + ic - c;
+                TI.tile_cursor[idx] = 0;
+                if (ne) TI.tile_list[s_lbase + s_wn[warp] + in - 1] = idx;  // non-empty tiles in tile order
+            }
+            __syncthreads();
+            if (tid == 0) { s_base += s_tc; s_lbase += s_tn; }
+            __syncthreads();
+        }
     }
-    int base = s_cnt[tid] - c, lbase = s_ne[tid] - ne;
-    for (int t = lo; t < hi; ++t) {
-        const int n = TI.tile_count[t];
-        TI.tile_start[t] = base;
-        TI.tile_cursor[t] = 0;
-        if (n > 0) TI.tile_list[lbase++] = t;  // non-empty tiles in tile order
-        base += n;
-    }
-    if (tid == 1023) *TI.n_tile_list = s_ne[1023];
+    if (tid == 0) *TI.n_tile_list = s_lbase;
 }
 
 struct SortBuffers {
@@ -153,23 +173,29 @@ __device__ void bitonic_sort_padded(K* key, V* val, int m) {
     }
 }
 
-constexpr int kSortSmem = 4032;  // particles per tile sorted in shared memory (12 B each, within 48 KB)
+// Particles per tile sorted in shared memory (12 B each) and CTAs per SM of
+// the sort: 3D tiles (4^3 cells) rarely hold more than ~1000 particles, so a
+// 24 KB buffer lets eight sorting CTAs share an SM; 2D tiles (8^2 cells) hold
+// more and keep the 48 KB buffer.
+template <int D> struct SortGeom;
+template <> struct SortGeom<3> { static constexpr int SMEM = 2048, CTAS_PER_SM = 8; };
+template <> struct SortGeom<2> { static constexpr int SMEM = 4032, CTAS_PER_SM = 4; };
 constexpr int kTileCells = 64;   // cells per tile: 4^3 in 3D, 8^2 in 2D
-constexpr int kCountSortMax = kSortSmem / 2;  // tiles up to this size: counting sort (two halves)
-constexpr int kCellSortMax = 64;              // ... when no cell holds more particles than this
+constexpr int kCellSortMax = 64;  // counting sort when no cell of the tile holds more particles than this
 
 // One CTA per non-empty tile: order the tile's particles by (cell in tile,
 // particle id) -- a function of the state alone -- and gather their state into
-// the destination buffers in that order. Tiles of up to kCountSortMax
-// particles whose cells hold at most kCellSortMax each take a counting sort by
+// the destination buffers in that order. Tiles of up to SMEM / 2 particles
+// whose cells hold at most kCellSortMax each take a counting sort by
 // cell and an insertion sort by id inside each cell (one thread per cell);
-// larger tiles a bitonic network (in shared memory up to kSortSmem, else in
+// larger tiles a bitonic network (in shared memory up to SMEM, else in
 // global scratch). The result is the same order either way.
 template <int D, int S = 4>
 __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __restrict__ id_src, SortBuffers dst,
                                                    StepConsts C, TileInfo TI) {
     static_assert(TileGeom<D>::BN == kTileCells, "a tile has 64 cells");
     constexpr int T = TileGeom<D>::T;
+    constexpr int kSortSmem = SortGeom<D>::SMEM, kCountSortMax = kSortSmem / 2;
     __shared__ unsigned long long s_key[kSortSmem];
     __shared__ int s_val[kSortSmem];
     __shared__ int s_cnt[kTileCells], s_off[kTileCells];

@@ -166,8 +166,9 @@ def test_classic_matches_reference_cpu(gpu_lib, oracle_mod, case):
 @pytest.mark.parametrize("case", ["impact3d", "dense3d", "dense2d"])
 def test_run_to_run_bitwise_determinism(gpu_lib, case):
     """Bit-identical grid sums and particle state across runs. dense3d has
-    ~1000 particles per 4^3 tile (tiles split into several work items);
-    dense2d has >4032 particles per 8^2 tile (sorted in global memory)."""
+    ~1000 particles per 4^3 tile (counting sort and, above 1024, the bitonic
+    network in shared memory); dense2d has >4032 particles per 8^2 tile (sorted
+    in global memory)."""
     from mpm_snow_sim2d_b200 import Solver, scenes
     sc = {"impact3d": lambda: scenes.impact_3d(),
           "dense3d": lambda: scenes.snowball_on_slab_3d(W=32, ppc=16),
