@@ -43,7 +43,6 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-updates/s (P2G+grid+G2P), plain vs MLP-plasticity, 1 B200, % HBM peak"
 UNIT = "particle-updates/s"
-DEFAULT_SORT_PERIOD = 16  # the solver's re-sort interval when mpm_params.sort_period is 0
 # DRAM bytes (read + write) per launch of the dominant kernels, from one full
 # ncu capture of the same scene (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {("c3", "p2g"): 113.1e6, ("c3", "g2p"): 315.1e6}
@@ -162,12 +161,12 @@ def make_scene(name):
     return scenes.workload(name)
 
 
-def kernel_launches(steps, step0, sort_period):
-    """Kernels the tiled 3D/2D MLS step enqueues for steps [step0, step0 + steps):
-    P2G, grid update, G2P gather and G2P plastic every step, plus the four sort
-    kernels (count, scan, bucket, per-tile sort) on multiples of sort_period."""
-    sorts = sum(1 for k in range(step0, step0 + steps) if sort_period > 0 and k % sort_period == 0)
-    return 4 * steps + 4 * sorts
+def kernel_launches(steps, sorts, auto_period):
+    """Kernels the tiled 3D/2D MLS step enqueues over `steps` steps with `sorts`
+    re-binning sorts: P2G, grid update, G2P gather and G2P plastic every step,
+    the four sort kernels (count, scan, bucket, per-tile sort) per sort, and with
+    the auto period the velocity maximum that picks each period's length."""
+    return 4 * steps + (5 if auto_period else 4) * sorts
 
 
 def rel_l2(a, b):
@@ -444,8 +443,6 @@ def main():
     # warm-up, then active-node count (untimed P2G-only pass)
     solver.Step(args.warmup)
     torch.cuda.synchronize()
-    step0 = solver.step_count
-    sort_period = args.sort_period if args.sort_period > 0 else DEFAULT_SORT_PERIOD
     m, _ = solver.rasterize()
     active = int((m > 0).sum())
 
@@ -453,6 +450,7 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    sorts0, _ = solver.sort_stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(device) as clocks:
         e0.record(stream)
@@ -462,6 +460,8 @@ def main():
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1))
     flags = solver.status()
+    sorts1, period_end = solver.sort_stats()
+    timed_sorts = sorts1 - sorts0
     value = job_rate(world, scene.count, args.steps, ms / 1e3)
 
     # ---- per-stage device time (events between kernels), for the roofline ----
@@ -545,12 +545,14 @@ def main():
             "data": f"synthetic (seeded {scene.name} scene, {scene.count} particles)",
             "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]}", "particles": scene.count,
                        "nodes": scene.nodes, "active_nodes": active, "plasticity": "exact",
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
+                       "sort_period": (f"auto ({timed_sorts} sorts in the timed steps, last period {period_end})"
+                                       if args.sort_period <= 0 else args.sort_period)},
             "roofline": roofline,
             "stages_ms": stage_avg,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": ke},
-            "gpu_launches": kernel_launches(args.steps, step0, sort_period),
+            "gpu_launches": kernel_launches(args.steps, timed_sorts, args.sort_period <= 0),
             "clocks": clocks.summary(),
             "status_flags": flags,
             "cpu_baseline": cpu,

@@ -95,7 +95,10 @@ typedef struct mpm_params {
     int32_t border_margin; /* BORDER_MARGIN (cells)                             */
     int32_t formulation;   /* mpm_formulation                                   */
     int32_t boundary;      /* mpm_boundary                                      */
-    int32_t sort_period;   /* steps between particle re-binning (0 = auto)      */
+    int32_t sort_period;   /* steps between particle re-binning; 0 = auto: each
+                              period is 4..32 steps, the longest over which the
+                              fastest particle (at the start of the previous
+                              period) moves at most a quarter cell             */
     float delta_time;      /* DELTA_TIME                                        */
     float gravity;         /* GRAVITY (along -y when negative), grid units/s^2  */
     float friction;        /* FRICTION (Coulomb coefficient at the walls)       */
@@ -160,6 +163,10 @@ MPM_API mpm_status mpm_get_positions(mpm_solver* solver, float* out, size_t cap_
 
 /* Number of particles and the dimension. */
 MPM_API mpm_status mpm_get_info(const mpm_solver* solver, int64_t* count, int32_t* dim);
+
+/* Particle re-binning sorts run so far and the current sort period (steps).
+ * No counterpart in the reference (which does not sort its particles). */
+MPM_API mpm_status mpm_get_sort_stats(const mpm_solver* solver, int64_t* sorts, int32_t* period);
 
 /* Full particle state, host copies in creation order (the SSBO contents of
  * bindings 0-6, src/gpu/GPUSolver.cpp:166-172, minus mass/volume). */

@@ -120,6 +120,7 @@ SIGNATURES = {
     "mpm_get_mlp_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mpm_pair_log_enable": (C.c_int, [_P, C.c_int64]),
     "mpm_pair_log_read": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_int64)]),
+    "mpm_get_sort_stats": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "mpm_sample_shapes": (C.c_int, [C.c_int32, C.POINTER(MpmShape), C.c_int32, C.c_float, C.c_uint64, C.c_int32,
                                      C.POINTER(C.c_float), C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
     "mpm_render_params_default": (None, [C.POINTER(MpmRenderParams)]),

@@ -61,6 +61,19 @@ template <int D, int S> __device__ __forceinline__ int tile_of_slot(const Partic
 }
 
 // ---------------------------------------------------------------------------
+// Largest |v_k| over all particle velocity components (non-negative floats
+// order as their bit patterns; NaN is skipped), for the auto sort period.
+__global__ void __launch_bounds__(256) k_max_abs(const float* __restrict__ v, long long count,
+                                                 unsigned* __restrict__ out) {
+    float m = 0.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(v[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
+}
+
+// ---------------------------------------------------------------------------
 // Counting sort by tile.
 
 template <int D, int S = 4>

@@ -144,6 +144,12 @@ class Solver:
         check(self._lib.mpm_get_step(self._h, C.byref(s)), self._h)
         return int(s.value)
 
+    def sort_stats(self):
+        """(sorts run so far, current sort period in steps)."""
+        n, k = C.c_int64(), C.c_int32()
+        check(self._lib.mpm_get_sort_stats(self._h, C.byref(n), C.byref(k)), self._h)
+        return int(n.value), int(k.value)
+
     def fixed_point(self):
         a, b = C.c_int32(), C.c_int32()
         check(self._lib.mpm_get_fixed_point(self._h, C.byref(a), C.byref(b)), self._h)

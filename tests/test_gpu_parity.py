@@ -316,3 +316,30 @@ def test_stale_tile_order_matches_oracle(gpu_lib, oracle_mod, dim):
     got, flags = _gpu_run(sc, steps, sort_period=100000)
     assert flags & 1 == 0
     _check_vs_fp32_reference(state_errors(got[150], ref[150], dim), r32[150], "step 150")
+
+
+def test_auto_sort_period(gpu_lib):
+    """sort_period 0: each period is the longest of {4, 6, 8, 12, 16, 24, 32}
+    steps over which the fastest particle moves at most a quarter cell."""
+    from mpm_snow_sim2d_b200 import Solver, scenes
+    slow = scenes.snow_blocks_2d(steps=100).with_(gravity=0.0)
+    slow = slow.with_(velocity=np.tile(np.float32([0.0, -50.0]), (slow.count, 1)))  # 0.005 cells/step
+    with Solver.from_scene(slow) as s:
+        s.Step(64)
+        sorts, period = s.sort_stats()
+    assert period == 32 and sorts == 2
+    mid = slow.with_(velocity=np.tile(np.float32([0.0, -180.0]), (slow.count, 1)))  # 0.018: 12 steps, 0.22 cells
+    with Solver.from_scene(mid) as s:
+        s.Step(48)
+        sorts, period = s.sort_stats()
+    assert period == 12 and sorts == 4
+    fast = scenes.impact_2d()  # up to ~4.1 m/s on a 128 grid, dt 1e-4: ~0.052 cells/step
+    with Solver.from_scene(fast) as s:
+        s.Step(40)
+        sorts, period = s.sort_stats()
+    assert period == 4 and sorts == 10
+    # a fixed period is kept as given
+    with Solver.from_scene(fast, sort_period=16) as s:
+        s.Step(40)
+        sorts, period = s.sort_stats()
+    assert period == 16 and sorts == 3
