@@ -97,8 +97,8 @@ typedef struct mpm_params {
     int32_t boundary;      /* mpm_boundary                                      */
     int32_t sort_period;   /* steps between particle re-binning; 0 = auto: each
                               period is 4..32 steps, the longest over which the
-                              fastest particle (at the start of the previous
-                              period) moves at most a quarter cell             */
+                              fastest particle (two periods earlier) moves at
+                              most a quarter cell                              */
     float delta_time;      /* DELTA_TIME                                        */
     float gravity;         /* GRAVITY (along -y when negative), grid units/s^2  */
     float friction;        /* FRICTION (Coulomb coefficient at the walls)       */

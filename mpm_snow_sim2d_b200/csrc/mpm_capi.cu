@@ -69,18 +69,18 @@ struct mpm_solver {
     bool needs_sort = true;
     int sort_period = 8;
     // sort_period 0 (auto): each period's length follows from the fastest
-    // particle at the start of the previous period (so the host never waits for
-    // the period it is about to follow); a function of the state, so runs stay
-    // deterministic.
+    // particle two periods earlier (so the host waits for nothing the GPU has
+    // not long passed); a function of the state, so runs stay deterministic.
     bool auto_sort = false;
     int cur_K = 16;              // steps of the current period (auto)
     long long next_sort = 0;     // step of the next sort (auto)
     long long sorts_done = 0;    // sorts launched so far
-    unsigned* vmax_dev = nullptr;   // largest |v| component over the particles (float bits)
-    unsigned* vmax_host = nullptr;  // pinned copy of the last measurement
-    cudaEvent_t vmax_event = nullptr;
-    bool vmax_pending = false;   // a measurement for the next period is in flight
-    int next_K = 0;              // the next period's length when already decided (checkpoint)
+    unsigned* vmax_dev = nullptr;   // two slots: largest |v| component over the particles (float bits)
+    unsigned* vmax_host = nullptr;  // pinned copies
+    cudaEvent_t vmax_event[2] = {nullptr, nullptr};
+    struct PeriodPlan { int K; int slot; };  // the length of a coming period: K > 0, or pending in `slot`
+    PeriodPlan plan[2] = {};
+    int nplan = 0;                  // 0 after creation or a state upload
     int sms = 148;
     TileInfo ti{};
     SortBuffers alt{};
@@ -167,7 +167,8 @@ void release(mpm_solver* s) {
             if (g) cudaGraphExecDestroy(g);
     if (s->vmax_dev) cudaFree(s->vmax_dev);
     if (s->vmax_host) cudaFreeHost(s->vmax_host);
-    if (s->vmax_event) cudaEventDestroy(s->vmax_event);
+    for (auto ev : s->vmax_event)
+        if (ev) cudaEventDestroy(ev);
     if (s->mlp_counters) cudaFree(s->mlp_counters);
     if (s->log_data) cudaFree(s->log_data);
     if (s->log_n) cudaFree(s->log_n);
@@ -262,10 +263,11 @@ bool sort_due(const mpm_solver* s) {
 // which the fastest particle moves at most a quarter cell (measured on B200:
 // two snowballs colliding at ~0.04 cells/step run 15% faster than with a fixed
 // 16-step period; a snowball falling onto a resting slab, ~0.02, is unchanged).
-// The maximum is measured at the start of every period and used for the next
-// one, read back through pinned memory without waiting for the stream; the
-// first period after creation or a state upload measures its own start (one
-// synchronisation).
+// The maximum is measured at the start of every period and used two periods
+// later, read back through pinned memory: the host then waits only for work the
+// GPU finished a period ago, and stays ahead of it. The first period after
+// creation or a state upload measures its own start (one synchronisation) and
+// uses it for the next one as well.
 int period_for(const mpm_solver* s, unsigned vmax_bits) {
     float vmax;
     std::memcpy(&vmax, &vmax_bits, sizeof(float));
@@ -276,33 +278,49 @@ int period_for(const mpm_solver* s, unsigned vmax_bits) {
     return 4;
 }
 
-cudaError_t measure_vmax(mpm_solver* s) {
-    cudaError_t e = cudaMemsetAsync(s->vmax_dev, 0, sizeof(unsigned), s->stream);
+cudaError_t measure_vmax(mpm_solver* s, int slot) {
+    cudaError_t e = cudaMemsetAsync(s->vmax_dev + slot, 0, sizeof(unsigned), s->stream);
     if (e != cudaSuccess) return e;
     if (s->n > 0) {
-        k_max_abs<<<s->sms * 4, 256, 0, s->stream>>>(s->v, (long long)s->n * s->dim, s->vmax_dev);
+        k_max_abs<<<s->sms * 4, 256, 0, s->stream>>>(s->v, (long long)s->n * s->dim, s->vmax_dev + slot);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    if ((e = cudaMemcpyAsync(s->vmax_host, s->vmax_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream)) !=
-        cudaSuccess)
+    if ((e = cudaMemcpyAsync(s->vmax_host + slot, s->vmax_dev + slot, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             s->stream)) != cudaSuccess)
         return e;
-    if ((e = cudaEventRecord(s->vmax_event, s->stream)) != cudaSuccess) return e;
-    s->vmax_pending = true;
-    return cudaSuccess;
+    return cudaEventRecord(s->vmax_event[slot], s->stream);
 }
 
+// Length of a planned period (waits for its measurement when still pending).
+cudaError_t resolve_plan(mpm_solver* s, const mpm_solver::PeriodPlan& p, int* K) {
+    if (p.K > 0) { *K = p.K; return cudaSuccess; }
+    cudaError_t e = cudaEventSynchronize(s->vmax_event[p.slot]);
+    if (e == cudaSuccess) *K = period_for(s, s->vmax_host[p.slot]);
+    return e;
+}
+
+// At the start of a period (auto): take the planned length and measure this
+// period's start for the period after next. The first period after creation or
+// a state upload measures its own start and uses it for the next one too.
 cudaError_t choose_period(mpm_solver* s) {
     if (!s->auto_sort || !sort_due(s)) return cudaSuccess;
     cudaError_t e;
-    if (s->next_K > 0) {
-        s->cur_K = s->next_K;
-        s->next_K = 0;
-    } else {
-        if (!s->vmax_pending && (e = measure_vmax(s)) != cudaSuccess) return e;
-        if ((e = cudaEventSynchronize(s->vmax_event)) != cudaSuccess) return e;
-        s->cur_K = period_for(s, *s->vmax_host);
+    if (s->nplan == 0) {
+        if ((e = measure_vmax(s, 0)) != cudaSuccess || (e = cudaEventSynchronize(s->vmax_event[0])) != cudaSuccess)
+            return e;
+        s->cur_K = period_for(s, s->vmax_host[0]);
+        s->plan[0] = {s->cur_K, 0};
+        s->plan[1] = {s->cur_K, 0};
+        s->nplan = 2;
+        return cudaSuccess;
     }
-    return measure_vmax(s);  // for the next period
+    const mpm_solver::PeriodPlan front = s->plan[0];
+    s->plan[0] = s->plan[1];
+    if ((e = resolve_plan(s, front, &s->cur_K)) != cudaSuccess) return e;
+    const int slot = s->plan[0].K > 0 ? 0 : 1 - s->plan[0].slot;  // not the slot still pending
+    if ((e = measure_vmax(s, slot)) != cudaSuccess) return e;
+    s->plan[1] = {0, slot};
+    return cudaSuccess;
 }
 
 template <int D, int S> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
@@ -487,9 +505,10 @@ mpm_status setup_tiled(mpm_solver* s) {
     s->cur_K = s->sort_period;
     s->next_sort = 0;
     if (s->sort_period > mpm_solver::kMaxPeriod) s->use_graphs = false;  // graphs are cached per period up to 64
-    if (dalloc(&s->vmax_dev, 1) ||
-        cudaHostAlloc(&s->vmax_host, sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->vmax_event, cudaEventDisableTiming) != cudaSuccess) {
+    if (dalloc(&s->vmax_dev, 2) ||
+        cudaHostAlloc(&s->vmax_host, 2 * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->vmax_event[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->vmax_event[1], cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
     }
@@ -907,8 +926,7 @@ mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
     if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
     s->needs_sort = true;
     s->needs_affine = true;
-    s->vmax_pending = false;  // the next period is measured from the uploaded state
-    s->next_K = 0;
+    s->nplan = 0;  // the next period is measured from the uploaded state
     return MPM_OK;
 }
 
@@ -976,8 +994,8 @@ constexpr int kSchedTag = 0x4B504552;  // extra record: auto sort schedule
 // i32x4 extra[n_extra]]. The slot order of the tiled path is saved so that a
 // resumed run groups particles exactly as the original did and continues
 // bit-identically. `extra` holds tagged records: with the auto sort period,
-// one {kSchedTag, period, steps to the next sort, next period (0: measure)};
-// unknown records are skipped on load.
+// one {kSchedTag, period, steps to the next sort, next two periods (8 bits
+// each; 0: measure)}; unknown records are skipped on load.
 mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
     const int D = s->dim;
@@ -989,12 +1007,9 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     const uint32_t has_order = (s->tiled && !s->needs_sort) ? 1u : 0u;
     std::vector<int> ids;
     // extra records: the auto sort schedule (period length, steps to the next sort)
-    int pending_K = s->next_K;
-    if (s->auto_sort && pending_K == 0 && s->vmax_pending) {
-        MPM_CUDA(s, cudaEventSynchronize(s->vmax_event));
-        pending_K = period_for(s, *s->vmax_host);
-    }
-    const int4 sched = make_int4(kSchedTag, s->cur_K, (int)(s->next_sort - s->step), pending_K);
+    int planned[2] = {0, 0};
+    for (int q = 0; s->auto_sort && q < s->nplan; ++q) MPM_CUDA(s, resolve_plan(s, s->plan[q], &planned[q]));
+    const int4 sched = make_int4(kSchedTag, s->cur_K, (int)(s->next_sort - s->step), planned[0] | (planned[1] << 8));
     const int32_t n_extra = s->auto_sort ? 1 : 0;
     if (has_order) {
         ids.resize(n);
@@ -1058,8 +1073,8 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
                 ok = std::fread(extra.data(), sizeof(int4), extra.size(), f) == extra.size();
                 for (size_t q = 0; ok && q < extra.size(); ++q)
                     if (extra[q].x == kSchedTag && extra[q].y >= 1 && extra[q].y <= mpm_solver::kMaxPeriod &&
-                        extra[q].z >= 0 && extra[q].z <= extra[q].y && extra[q].w >= 0 &&
-                        extra[q].w <= mpm_solver::kMaxPeriod) {
+                        extra[q].z >= 0 && extra[q].z <= extra[q].y && (extra[q].w & 0xff) <= mpm_solver::kMaxPeriod &&
+                        ((extra[q].w >> 8) & 0xff) <= mpm_solver::kMaxPeriod && (extra[q].w >> 16) == 0) {
                         sched_K = extra[q].y;
                         sched_next = extra[q].z;
                         sched_pending = extra[q].w;
@@ -1088,7 +1103,10 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     if (s->auto_sort) {  // resume the saved sort schedule (else sort at the next step)
         s->cur_K = sched_K > 0 ? sched_K : s->cur_K;
         s->next_sort = sched_K > 0 ? step + sched_next : step;
-        s->next_K = sched_K > 0 ? sched_pending : 0;
+        const int ka = sched_pending & 0xff, kb = (sched_pending >> 8) & 0xff;
+        s->nplan = (sched_K > 0 && ka > 0 && kb > 0) ? 2 : 0;
+        s->plan[0] = {ka, 0};
+        s->plan[1] = {kb, 0};
     }
     return MPM_OK;
 }

@@ -200,7 +200,8 @@ constexpr int kCellSortMax = 64;  // counting sort when no cell of the tile hold
 // particle id) -- a function of the state alone -- and gather their state into
 // the destination buffers in that order. Tiles of up to SMEM / 2 particles
 // whose cells hold at most kCellSortMax each take a counting sort by
-// cell and an insertion sort by id inside each cell (one thread per cell);
+// cell and a rank sort by id inside each cell (every item counts the smaller
+// ids of its cell, all threads at once);
 // larger tiles a bitonic network (in shared memory up to SMEM, else in
 // global scratch). The result is the same order either way.
 template <int D, int S = 4>
@@ -265,19 +266,17 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
                 val2[p] = val[j];
             }
             __syncthreads();
-            if (threadIdx.x < kTileCells) {
-                const int lo = s_off[threadIdx.x], hi = s_cnt[threadIdx.x];
-                for (int a = lo + 1; a < hi; ++a) {
-                    const unsigned long long k = key2[a];
-                    const int v = val2[a];
-                    int b = a - 1;
-                    while (b >= lo && key2[b] > k) { key2[b + 1] = key2[b]; val2[b + 1] = val2[b]; --b; }
-                    key2[b + 1] = k;
-                    val2[b + 1] = v;
-                }
+            // each item's place in its cell = the number of smaller keys there
+            // (keys are unique: cell and particle id), written back to the first half
+            for (int j = threadIdx.x; j < m; j += blockDim.x) {
+                const unsigned long long kj = key2[j];
+                const int c = (int)(kj >> 32), lo = s_off[c], hi = s_cnt[c];
+                int rank = 0;
+                for (int q = lo; q < hi; ++q) rank += key2[q] < kj;
+                key[lo + rank] = kj;
+                val[lo + rank] = val2[j];
             }
             __syncthreads();
-            val = val2;
         } else {
             bitonic_sort_padded(key, val, m);
         }
