@@ -272,9 +272,12 @@ int period_for(const mpm_solver* s, unsigned vmax_bits) {
     float vmax;
     std::memcpy(&vmax, &vmax_bits, sizeof(float));
     const double disp = double(vmax) * double(s->params.delta_time);  // cells per step
+#ifndef MPM_AUTO_SORT_CELLS
+#define MPM_AUTO_SORT_CELLS 0.25
+#endif
     const int choices[] = {32, 24, 16, 12, 8, 6, 4};
     for (int c : choices)
-        if (!(disp > 0.0) || disp * c <= 0.25) return c;
+        if (!(disp > 0.0) || disp * c <= MPM_AUTO_SORT_CELLS) return c;
     return 4;
 }
 
