@@ -419,8 +419,7 @@ cudaError_t dispatch_step(mpm_solver* s) {
         if (s->stencil == 3) return s->dim == 2 ? step_tiled<2, 3>(s) : step_tiled<3, 3>(s);
         return s->dim == 2 ? step_tiled<2, 4>(s) : step_tiled<3, 4>(s);
     }
-    if (s->dim == 2) return s->form == kClassic ? step_once<2, kClassic>(s) : step_once<2, kMLS>(s);
-    return step_once<3, kMLS>(s);
+    return step_once<2, kClassic>(s);  // the untiled path: CLASSIC, 2D
 }
 
 cudaError_t dispatch_p2g(mpm_solver* s) {
@@ -428,8 +427,7 @@ cudaError_t dispatch_p2g(mpm_solver* s) {
         if (s->stencil == 3) return s->dim == 2 ? launch_p2g_tiled<2, 3>(s) : launch_p2g_tiled<3, 3>(s);
         return s->dim == 2 ? launch_p2g_tiled<2, 4>(s) : launch_p2g_tiled<3, 4>(s);
     }
-    if (s->dim == 2) return s->form == kClassic ? launch_p2g<2, kClassic>(s) : launch_p2g<2, kMLS>(s);
-    return launch_p2g<3, kMLS>(s);
+    return launch_p2g<2, kClassic>(s);
 }
 
 // After a P2G-only pass: clear accumulators and node-block marks.
@@ -613,8 +611,7 @@ cudaError_t dispatch_stage(mpm_solver* s, int k) {
         if (s->stencil == 3) return s->dim == 2 ? stage_tiled<2, 3>(s, k) : stage_tiled<3, 3>(s, k);
         return s->dim == 2 ? stage_tiled<2, 4>(s, k) : stage_tiled<3, 4>(s, k);
     }
-    if (s->dim == 2) return s->form == kClassic ? stage<2, kClassic>(s, k) : stage<2, kMLS>(s, k);
-    return stage<3, kMLS>(s, k);
+    return stage<2, kClassic>(s, k);
 }
 }  // namespace
 
@@ -724,7 +721,7 @@ mpm_status mpm_create(const mpm_params* params, const mpm_particles_init* init, 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_NO_DEVICE;
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, k_grid_update<2, kMLS>) != cudaSuccess) { cudaGetLastError(); return MPM_ERR_NO_DEVICE; }
+    if (cudaFuncGetAttributes(&fa, k_grid_update<2, kClassic>) != cudaSuccess) { cudaGetLastError(); return MPM_ERR_NO_DEVICE; }
 
     mpm_solver* s = new mpm_solver();
     s->params = *params;
