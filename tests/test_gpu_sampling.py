@@ -98,3 +98,27 @@ def test_reference_default_scene_matches_golden_fixture(gpu_lib):
     golden, _ = load_case("refcpu_reference_default2d")
     assert np.array_equal(sc.position.view(np.uint32), golden.position.view(np.uint32))
     assert np.array_equal(sc.volume, golden.volume) and np.array_equal(sc.velocity, golden.velocity)
+
+
+def test_batch_scenes_with_device_sampling(gpu_lib):
+    """The batched workload's blocks filled by the device Poisson-disk sampler:
+    the same blocks and mean density as the uniform draw, the same mass per
+    scene, at least min_dist between particles; the batch steps them cleanly."""
+    from scipy.spatial import cKDTree
+    from mpm_snow_sim2d_b200 import scenes
+    from mpm_snow_sim2d_b200.batch import Batch
+    pois = [scenes.batch_scene_2d(i, steps=50, sampler="poisson") for i in range(4)]
+    unif = [scenes.batch_scene_2d(i, steps=50) for i in range(4)]
+    for p, u in zip(pois, unif):
+        assert (p.width, p.info["blocks"]) == (u.width, u.info["blocks"])
+        ratio = p.count / u.count
+        assert 0.85 < ratio < 1.15, ratio
+        assert abs(float(p.mass.astype(np.float64).sum()) / float(u.mass.astype(np.float64).sum()) - 1) < 1e-3
+        md = float(np.sqrt(scenes.POISSON_DENSITY_2D / int(u.name.split("ppc")[1])))
+        d, _ = cKDTree(p.position.astype(np.float64)).query(p.position.astype(np.float64), k=2)
+        assert d[:, 1].min() >= md * (1 - 1e-5)
+        again = scenes.batch_scene_2d(0, steps=50, sampler="poisson")
+    assert np.array_equal(again.position, pois[0].position)
+    with Batch(pois) as b:
+        b.step(50)
+        assert all(b.status(k) & 1 == 0 for k in range(len(pois)))
