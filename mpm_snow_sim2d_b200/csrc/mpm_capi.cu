@@ -158,7 +158,8 @@ void release(mpm_solver* s) {
         if (p) cudaFree(p);
     if (s->alt.id) cudaFree(s->alt.id);
     int* ti[] = {s->ti.key,      s->ti.tile_count, s->ti.tile_cursor, s->ti.tile_start, s->ti.mark, s->ti.mark_list,
-                 s->ti.n_marked, s->ti.perm,       s->ti.tile_list,   s->ti.n_tile_list, s->ti.sval};
+                 s->ti.n_marked, s->ti.perm,       s->ti.tile_list,   s->ti.n_tile_list, s->ti.sval,
+                 s->ti.p2g_next};
     if (s->ti.skey) cudaFree(s->ti.skey);
     for (int* p : ti)
         if (p) cudaFree(p);
@@ -327,6 +328,10 @@ cudaError_t choose_period(mpm_solver* s) {
 }
 
 template <int D, int S> cudaError_t launch_p2g_tiled_kernel(mpm_solver* s) {
+    if (P2GDynamic<D, S>::value) {
+        cudaError_t e = cudaMemsetAsync(s->ti.p2g_next, 0, sizeof(int), s->stream);
+        if (e != cudaSuccess) return e;
+    }
     k_p2g_warp<D, S><<<s->p2g_warp_grid, kP2GWarps * 32, sizeof(P2GWarpSmem<D, S>), s->stream>>>(
         particle_view(s), s->C, s->ti, s->acc, s->status);
     return cudaGetLastError();
@@ -459,7 +464,7 @@ mpm_status setup_tiled(mpm_solver* s) {
     if (dalloc(&ti.key, (size_t)n) || dalloc(&ti.tile_count, (size_t)ti.n_tiles) ||
         dalloc(&ti.tile_cursor, (size_t)ti.n_tiles) || dalloc(&ti.tile_start, (size_t)ti.n_tiles) ||
         dalloc(&ti.mark, (size_t)ti.n_blocks) || dalloc(&ti.mark_list, (size_t)ti.n_blocks) ||
-        dalloc(&ti.n_marked, 1) ||
+        dalloc(&ti.n_marked, 1) || dalloc(&ti.p2g_next, 1) ||
         dalloc(&ti.perm, (size_t)n) || dalloc(&ti.tile_list, (size_t)ti.n_tiles) || dalloc(&ti.n_tile_list, 1) ||
         dalloc(&ti.skey, (size_t)n) || dalloc(&ti.sval, (size_t)n) ||
         dalloc(&s->alt.x, (size_t)n * D) || dalloc(&s->alt.v, (size_t)n * D) || dalloc(&s->alt.B, (size_t)n * D * D) ||
