@@ -54,7 +54,8 @@ typedef enum mpm_status {
     MPM_ERR_STATE_MISMATCH = 8,       /* checkpoint does not match this solver */
     MPM_ERR_TIMEOUT = 9,              /* a bounded device-side wait gave up */
     MPM_ERR_UNSUPPORTED = 10,
-    MPM_ERR_CAPACITY = 11             /* a buffer or fixed device capacity is too small */
+    MPM_ERR_CAPACITY = 11,            /* a buffer or fixed device capacity is too small */
+    MPM_ERR_PARTICLE_OUT_OF_DOMAIN = 12 /* a particle's stencil reached outside the grid */
 } mpm_status;
 
 /* Device status word bits (mpm_get_status). Kernels set them with atomicOr
@@ -64,7 +65,8 @@ enum {
     MPM_FLAG_FIXED_POINT_OVERFLOW = 1u << 1,
     MPM_FLAG_PARTICLE_OUT_OF_DOMAIN = 1u << 2, /* a stencil reached outside the grid */
     MPM_FLAG_SVD_FP64_FALLBACK = 1u << 3,      /* informational: the FP64 SVD branch ran */
-    MPM_FLAG_TIMEOUT = 1u << 4
+    MPM_FLAG_TIMEOUT = 1u << 4                  /* reserved: no kernel of this library waits on the
+                                                   device (no spin on a flag or barrier), so none sets it */
 };
 
 typedef enum mpm_formulation {
@@ -187,6 +189,15 @@ MPM_API mpm_status mpm_rasterize(mpm_solver* solver, double* node_mass, double* 
 /* OR of every MPM_FLAG_* a kernel raised since creation (synchronises). */
 MPM_API mpm_status mpm_get_status(mpm_solver* solver, uint32_t* flags);
 
+/* The status word as an error code (synchronises): MPM_ERR_NAN_STATE,
+ * MPM_ERR_FIXED_POINT_OVERFLOW or MPM_ERR_PARTICLE_OUT_OF_DOMAIN for the
+ * first of those flags that is set, else MPM_OK (the informational FP64-SVD
+ * flag is not an error); mpm_last_error names every flag set. This replaces
+ * the reference's response to a non-finite stress, which prints and spins
+ * forever (src/cpu/Particles.cpp:50-61): here the step completes, the flag
+ * records what happened and the caller decides. */
+MPM_API mpm_status mpm_check_status(mpm_solver* solver);
+
 /* Launch work on this stream (a cudaStream_t) instead of the solver's own. */
 MPM_API mpm_status mpm_set_stream(mpm_solver* solver, void* cuda_stream);
 
@@ -249,7 +260,9 @@ MPM_API mpm_status mpm_mlp_train(mpm_mlp* mlp, int32_t steps, int32_t batch, flo
                                  uint32_t seed, float* loss_out);
 /* Mean-squared loss and its parameter gradient on the given pairs (no update). */
 MPM_API mpm_status mpm_mlp_gradient(mpm_mlp* mlp, const float* pairs, int64_t n, float* grad_out, float* loss_out);
-/* Denormalised outputs for rows whose first 10 floats are F_hat[9], J_p. */
+/* Denormalised outputs for rows whose first 10 floats are F_hat[9], J_p.
+ * The network's device (current at mpm_mlp_create) must be current; any other
+ * device returns MPM_ERR_INVALID_ARGUMENT before anything runs. */
 MPM_API mpm_status mpm_mlp_predict(mpm_mlp* mlp, const float* inputs, int64_t n, int32_t stride, float* out);
 
 /* mpm_mlp_predict without any device allocation (no counterpart in the
@@ -260,14 +273,20 @@ MPM_API mpm_status mpm_mlp_predict(mpm_mlp* mlp, const float* inputs, int64_t n,
  * This entry point stages rows and results in a fixed scratch array that is
  * part of the library's device image (MPM_MLP_NOALLOC_MAX_ROWS rows, 5.2 MB
  * per device), so it allocates nothing. n above that limit returns
- * MPM_ERR_CAPACITY; split larger batches. The first call on a device does a
- * one-time set-up (looks up the scratch address and opts the kernel into its
- * shared memory); make that first call before any stream capture begins on
- * the device. Nothing in the scratch has to start at zero: every element a
- * call reads was written earlier in the same call. Calls share the scratch of
- * their device, so two calls that overlap in time on the same device (from
- * two host threads) race: serialise them. Synchronous; the network's device
- * must be current. */
+ * MPM_ERR_CAPACITY; split larger batches.
+ * The first call on a device does a one-time set-up: it looks up the scratch
+ * address, opts the kernel into its shared memory and creates a non-blocking
+ * stream of its own for the copies and the launch (so calls neither wait for
+ * nor hold up the legacy default stream). With CUDA's lazy module loading
+ * (the default) that first call is also what loads this module onto the
+ * device, scratch array included, which does take device memory: make one
+ * warm-up call per device before the device's memory is reserved and before
+ * any stream capture begins on it. A set-up that fails is not remembered; the
+ * next call retries it. Nothing in the scratch has to start at zero: every
+ * element a call reads was written earlier in the same call. Calls share the
+ * scratch of their device, so two calls that overlap in time on the same
+ * device (from two host threads) race: serialise them. Synchronous. The
+ * network's device must be current (else MPM_ERR_INVALID_ARGUMENT). */
 #define MPM_MLP_NOALLOC_MAX_ROWS 65536
 MPM_API mpm_status mpm_mlp_predict_noalloc(mpm_mlp* mlp, const float* inputs, int64_t n, int32_t stride, float* out);
 

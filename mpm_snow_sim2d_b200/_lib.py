@@ -16,6 +16,7 @@ STATUS_NAMES = {
     0: "MPM_OK", 1: "MPM_ERR_INVALID_ARGUMENT", 2: "MPM_ERR_CUDA", 3: "MPM_ERR_OUT_OF_MEMORY",
     4: "MPM_ERR_NAN_STATE", 5: "MPM_ERR_FIXED_POINT_OVERFLOW", 6: "MPM_ERR_NO_DEVICE", 7: "MPM_ERR_IO",
     8: "MPM_ERR_STATE_MISMATCH", 9: "MPM_ERR_TIMEOUT", 10: "MPM_ERR_UNSUPPORTED", 11: "MPM_ERR_CAPACITY",
+    12: "MPM_ERR_PARTICLE_OUT_OF_DOMAIN",
 }
 FLAG_NAN_STATE = 1 << 0
 FLAG_FIXED_POINT_OVERFLOW = 1 << 1
@@ -94,6 +95,7 @@ SIGNATURES = {
     "mpm_set_state": (C.c_int, [_P, C.POINTER(MpmStateHost)]),
     "mpm_rasterize": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_size_t]),
     "mpm_get_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "mpm_check_status": (C.c_int, [_P]),
     "mpm_set_stream": (C.c_int, [_P, _P]),
     "mpm_save_state": (C.c_int, [_P, C.c_char_p]),
     "mpm_load_state": (C.c_int, [_P, C.c_char_p]),

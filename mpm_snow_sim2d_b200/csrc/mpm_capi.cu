@@ -118,7 +118,8 @@ const char* kStatusText[] = {"ok",
                              "checkpoint does not match this solver",
                              "device-side wait timed out",
                              "unsupported configuration",
-                             "capacity too small"};
+                             "capacity too small",
+                             "particle stencil outside the grid"};
 
 mpm_status fail(mpm_solver* s, mpm_status code, const std::string& what) {
     if (s) s->err = what;
@@ -969,6 +970,23 @@ mpm_status mpm_get_status(mpm_solver* s, uint32_t* flags) {
     return MPM_OK;
 }
 
+mpm_status mpm_check_status(mpm_solver* s) {
+    if (!s) return MPM_ERR_INVALID_ARGUMENT;
+    uint32_t f = 0;
+    mpm_status r = mpm_get_status(s, &f);
+    if (r != MPM_OK) return r;
+    std::string names;
+    const char* label[] = {"non-finite state", "fixed-point overflow", "stencil outside the grid", "FP64 SVD branch",
+                           "device wait timed out"};
+    for (int b = 0; b < 5; ++b)
+        if (f & (1u << b)) names += std::string(names.empty() ? "" : ", ") + label[b];
+    if (f & MPM_FLAG_NAN_STATE) return fail(s, MPM_ERR_NAN_STATE, "status flags: " + names);
+    if (f & MPM_FLAG_FIXED_POINT_OVERFLOW) return fail(s, MPM_ERR_FIXED_POINT_OVERFLOW, "status flags: " + names);
+    if (f & MPM_FLAG_PARTICLE_OUT_OF_DOMAIN) return fail(s, MPM_ERR_PARTICLE_OUT_OF_DOMAIN, "status flags: " + names);
+    if (f & MPM_FLAG_TIMEOUT) return fail(s, MPM_ERR_TIMEOUT, "status flags: " + names);
+    return MPM_OK;
+}
+
 mpm_status mpm_set_stream(mpm_solver* s, void* stream) {
     if (!s) return MPM_ERR_INVALID_ARGUMENT;
     MPM_CUDA(s, cudaStreamSynchronize(s->stream));
@@ -1120,6 +1138,30 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
 // Learned plasticity surrogate.
 
 int32_t mpm_mlp_param_count(void) { return MlpOff::total; }
+
+}  // extern "C"
+
+namespace {
+// The network's buffers live on the device that was current at
+// mpm_mlp_create; a kernel launched with another device current would be
+// handed pointers it cannot address. Refuse before any copy or launch.
+bool mlp_device_current(mpm_mlp* m, const char* who) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        m->err = std::string(who) + ": no usable current device";
+        return false;
+    }
+    if (dev != m->device) {
+        m->err = std::string(who) + ": the network lives on device " + std::to_string(m->device) + " but device " +
+                 std::to_string(dev) + " is current";
+        return false;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" {
 
 mpm_status mpm_mlp_create(uint64_t seed, mpm_mlp** out) {
     if (!out) return MPM_ERR_INVALID_ARGUMENT;
@@ -1301,6 +1343,7 @@ mpm_status mpm_mlp_gradient(mpm_mlp* m, const float* pairs, int64_t n, float* gr
 
 mpm_status mpm_mlp_predict(mpm_mlp* m, const float* inputs, int64_t n, int32_t stride, float* out) {
     if (!m || !inputs || !out || n < 1 || stride < 10 || n > (1 << 26)) return MPM_ERR_INVALID_ARGUMENT;
+    if (!mlp_device_current(m, "mpm_mlp_predict")) return MPM_ERR_INVALID_ARGUMENT;
     float *di = nullptr, *dout = nullptr;
     mpm_status st = MPM_OK;
     if (dalloc(&di, (size_t)n * stride) || dalloc(&dout, (size_t)n * kMlpOut)) st = MPM_ERR_OUT_OF_MEMORY;
@@ -1535,9 +1578,33 @@ constexpr int kNoallocRows = MPM_MLP_NOALLOC_MAX_ROWS;
 static __device__ __align__(256) float g_noalloc_scratch[(size_t)kNoallocRows * (kMlpIn + kMlpOut)];
 namespace {
 constexpr int kNoallocMaxDevices = 64;
-float* g_noalloc_ptr[kNoallocMaxDevices];
-cudaError_t g_noalloc_setup[kNoallocMaxDevices];
-std::once_flag g_noalloc_once[kNoallocMaxDevices];
+// Per device: the scratch address and a non-blocking stream of its own (so a
+// call neither waits for nor holds up work on the legacy default stream).
+// Set up under the mutex on the first call that succeeds; a failed set-up is
+// not remembered, so a later call tries again.
+struct NoallocDevice {
+    float* scratch = nullptr;
+    cudaStream_t stream = nullptr;
+    bool ready = false;
+};
+NoallocDevice g_noalloc[kNoallocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+cudaError_t noalloc_setup(int dev) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoallocDevice& d = g_noalloc[dev];
+    if (d.ready) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (!d.scratch) e = cudaGetSymbolAddress(reinterpret_cast<void**>(&d.scratch), g_noalloc_scratch);
+    if (e == cudaSuccess) e = mlp_kernel_attrs();
+    if (e == cudaSuccess && !d.stream) e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    d.ready = true;
+    return cudaSuccess;
+}
 }  // namespace
 
 extern "C" {
@@ -1549,32 +1616,31 @@ mpm_status mpm_mlp_predict_noalloc(mpm_mlp* m, const float* inputs, int64_t n, i
                  std::to_string(kNoallocRows) + " rows";
         return MPM_ERR_CAPACITY;
     }
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
-        cudaGetLastError();
-        m->err = "mpm_mlp_predict_noalloc: no usable current device";
+    if (!mlp_device_current(m, "mpm_mlp_predict_noalloc")) return MPM_ERR_INVALID_ARGUMENT;
+    const int dev = m->device;
+    if (dev < 0 || dev >= kNoallocMaxDevices) {
+        m->err = "mpm_mlp_predict_noalloc: device ordinal beyond the supported range";
+        return MPM_ERR_UNSUPPORTED;
+    }
+    cudaError_t e = noalloc_setup(dev);
+    if (e != cudaSuccess) {
+        m->err = std::string("mpm_mlp_predict_noalloc: scratch set-up failed: ") + cudaGetErrorString(e);
         return MPM_ERR_CUDA;
     }
-    std::call_once(g_noalloc_once[dev], [dev] {
-        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&g_noalloc_ptr[dev]), g_noalloc_scratch);
-        if (e == cudaSuccess) e = mlp_kernel_attrs();
-        g_noalloc_setup[dev] = e;
-    });
-    if (g_noalloc_setup[dev] != cudaSuccess) {
-        m->err = std::string("mpm_mlp_predict_noalloc: scratch set-up failed: ") + cudaGetErrorString(g_noalloc_setup[dev]);
-        return MPM_ERR_CUDA;
-    }
-    float* din = g_noalloc_ptr[dev];
+    const NoallocDevice& d = g_noalloc[dev];
+    float* din = d.scratch;
     float* dout = din + (size_t)kNoallocRows * kMlpIn;
-    cudaError_t e = cudaMemcpy2D(din, sizeof(float) * kMlpIn, inputs, sizeof(float) * (size_t)stride,
-                                 sizeof(float) * kMlpIn, (size_t)n, cudaMemcpyHostToDevice);
+    e = cudaMemcpy2DAsync(din, sizeof(float) * kMlpIn, inputs, sizeof(float) * (size_t)stride, sizeof(float) * kMlpIn,
+                          (size_t)n, cudaMemcpyHostToDevice, d.stream);
     if (e == cudaSuccess) {
         const int64_t rows = kMlpWarps * 32;
-        k_mlp_forward<<<(unsigned)((n + rows - 1) / rows), kMlpWarps * 32, sizeof(MlpWarpSmem)>>>(
+        k_mlp_forward<<<(unsigned)((n + rows - 1) / rows), kMlpWarps * 32, sizeof(MlpWarpSmem), d.stream>>>(
             din, kMlpIn, (int)n, m->wbf, m->w, m->norm, dout);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(float) * kMlpOut * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout, sizeof(float) * kMlpOut * (size_t)n, cudaMemcpyDeviceToHost, d.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d.stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         m->err = std::string("mpm_mlp_predict_noalloc: ") + cudaGetErrorString(e);

@@ -129,6 +129,15 @@ class Solver:
         check(self._lib.mpm_get_status(self._h, C.byref(f)), self._h)
         return int(f.value)
 
+    def check_status(self) -> int:
+        """The status word as an mpm_status code (0 when no error flag is set);
+        last_error() names the flags."""
+        return int(self._lib.mpm_check_status(self._h))
+
+    def last_error(self) -> str:
+        raw = self._lib.mpm_last_error(self._h)
+        return raw.decode() if raw else ""
+
     def set_stream(self, cuda_stream_handle: int) -> None:
         check(self._lib.mpm_set_stream(self._h, C.c_void_p(cuda_stream_handle)), self._h)
 

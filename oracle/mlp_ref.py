@@ -91,3 +91,24 @@ def loss_and_grad(params, pairs, norm, bf16_emulation=True):
         o, sz = OFF[name_b]
         g[o:o + sz] = grads[l][1]
     return loss, g
+
+
+def forward(params, rows, norm, bf16_emulation=True):
+    """Denormalised network outputs (F_E' - F_hat, log J_p' - log J_p) for rows
+    whose first 10 values are F_hat[9], J_p: the quantity mpm_mlp_predict and
+    mpm_mlp_predict_noalloc return. Returns (outputs, normalised outputs)."""
+    in_mean, in_std, out_mean, out_std = (np.asarray(a, np.float64) for a in norm)
+    r = (lambda a: bf16(a)) if bf16_emulation else (lambda a: np.asarray(a, np.float64))
+    rows = np.asarray(rows, np.float32)
+    n = rows.shape[0]
+    pairs = np.zeros((n, 20), np.float64)
+    pairs[:, :10] = rows[:, :10]
+    x = np.zeros((n, 16))
+    x[:, :10] = (features(pairs) - in_mean) / in_std
+    h = r(x)
+    layers = unpack(params)
+    for l, (W, b) in enumerate(layers):
+        y = h @ r(W).T + b
+        h = r(gelu(y)) if l < 3 else y
+    out_n = h[:, :10]
+    return out_n * out_std + out_mean, out_n
