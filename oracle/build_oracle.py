@@ -11,6 +11,13 @@
   vendored Eigen lacks Core, and the three helpers.h conversions). Built only
   when the reference tree is present; nothing is copied out of it and the
   binary stays in the git-ignored oracle/_ref/.
+* ``oracle/_ref/libshader_ref.so`` — the reference's GPU path: its GLSL compute
+  shaders (src/gpu/shaders/{2d,3d}) turned into C++ by oracle/shader/glsl_cpp.py
+  (generated fragments in oracle/_ref/shader/) and run on the CPU by
+  oracle/shader/shader_runner.cpp against the vendored glm 0.9.7.1.
+
+The reference tree is found at $MPM_REFERENCE_ROOT, else as the directory
+`reference` beside this repository's root.
 """
 from __future__ import annotations
 
@@ -20,11 +27,12 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_ROOT = Path(os.environ.get("MPM_REFERENCE_ROOT", "/root/reference"))
+REF_ROOT = Path(os.environ.get("MPM_REFERENCE_ROOT") or (HERE.parent.parent / "reference"))
 ORACLE_LIB = HERE / "liboracle_mpm.so"
 REF_DIR = HERE / "_ref"
 REFCPU = REF_DIR / "refcpu_driver"
 POISSON = {2: REF_DIR / "poisson2d", 3: REF_DIR / "poisson3d"}
+SHADER_LIB = REF_DIR / "libshader_ref.so"
 
 
 def _stale(target: Path, deps) -> bool:
@@ -94,10 +102,30 @@ def build_poisson(force: bool = False) -> dict:
     return dict(POISSON)
 
 
+def build_shader_ref(force: bool = False) -> Path | None:
+    """The reference's GLSL step compiled for the CPU; None when neither the
+    reference tree nor an earlier build is present."""
+    shaders = REF_ROOT / "src" / "gpu" / "shaders"
+    if not (shaders / "3d" / "p2g.glsl").exists():
+        return SHADER_LIB if SHADER_LIB.exists() else None
+    from .shader.glsl_cpp import generate
+    gen_dir = REF_DIR / "shader"
+    incs = generate(shaders, gen_dir)
+    runner = HERE / "shader" / "shader_runner.cpp"
+    if force or _stale(SHADER_LIB, incs + [runner, HERE / "shader" / "glsl_cpp.py"]):
+        tmp = SHADER_LIB.with_suffix(".so.tmp")
+        # GLSL reads unsuffixed floating literals as single precision
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-fsingle-precision-constant",
+              "-I", str(gen_dir), "-I", str(REF_ROOT / "external" / "glm-0.9.7.1"), str(runner), "-o", str(tmp)])
+        os.replace(tmp, SHADER_LIB)
+    return SHADER_LIB
+
+
 def build_all(force: bool = False) -> None:
     build_oracle(force)
     build_refcpu(force)
     build_poisson(force)
+    build_shader_ref(force)
 
 
 if __name__ == "__main__":

@@ -44,10 +44,11 @@ template <typename R> struct Params {
 
 // ---------------------------------------------------------------------------
 // Cubic B-spline, src/gpu/shaders/2d/common.glsl:43-69 (= src/cpu/Grid.h:86-116)
+// (the shader's pow form, so that the FP32 instantiation rounds as the shader does)
 template <typename R> inline R bspline_n(R x) {
     R a = std::fabs(x);
-    if (a < R(1)) return R(0.5) * a * a * a - a * a + R(2) / R(3);
-    if (a < R(2)) { R t = R(2) - a; return t * t * t / R(6); }
+    if (a < R(1)) return (R(0.5) * std::pow(a, R(3))) - std::pow(a, R(2)) + R(2) / R(3);
+    if (a < R(2)) return std::pow(R(2) - a, R(3)) / R(6);
     return R(0);
 }
 // Quadratic B-spline (QUAD): 3/4 - x^2 for |x| < 1/2, (3/2 - |x|)^2 / 2 for |x| < 3/2.
@@ -115,7 +116,9 @@ template <typename R> void svd2_glsl(const R* M, R* U, R* S, R* V) {
     S[1] = std::sqrt(std::max(dg[3], R(1e-12)));
     R MV[4];
     matmul<2>(M, V, MV);
-    for (int r = 0; r < 2; ++r) { U[r * 2 + 0] = MV[r * 2 + 0] / S[0]; U[r * 2 + 1] = MV[r * 2 + 1] / S[1]; }
+    // U = M V diag(1 / Sigma), the reciprocals formed first as in the shader
+    const R i0 = R(1) / S[0], i1 = R(1) / S[1];
+    for (int r = 0; r < 2; ++r) { U[r * 2 + 0] = MV[r * 2 + 0] * i0; U[r * 2 + 1] = MV[r * 2 + 1] * i1; }
     if (det<2>(U) < R(0)) { U[1] = -U[1]; U[3] = -U[3]; S[1] = -S[1]; }
 }
 
@@ -250,11 +253,14 @@ template <int D, typename R> void stress(const Params<R>& p, const R* Fe, const 
     matmul<D>(U, Vt, Rm);
     R h = std::exp(p.xi * (R(1) - Jp));
     R mu = p.mu * h, la = p.lambda * h;
+    // evaluated in glm's order, as both reference paths write it:
+    // ((2 mu) (F - R)) F^T + ((lambda (J_e - 1)) J_e) I
+    const R two_mu = R(2) * mu, dg = (la * (Je - R(1))) * Je;
     R FmR[D * D], FeT[D * D], P[D * D];
-    for (int i = 0; i < D * D; ++i) FmR[i] = Fe[i] - Rm[i];
+    for (int i = 0; i < D * D; ++i) FmR[i] = two_mu * (Fe[i] - Rm[i]);
     transpose<D>(Fe, FeT);
     matmul<D>(FmR, FeT, P);
-    for (int i = 0; i < D * D; ++i) out[i] = R(2) * mu * P[i] + ((i % (D + 1) == 0) ? la * (Je - R(1)) * Je : R(0));
+    for (int i = 0; i < D * D; ++i) out[i] = P[i] + ((i % (D + 1) == 0) ? dg : R(0));
 }
 
 // ---------------------------------------------------------------------------
@@ -400,11 +406,16 @@ template <int D, typename R> void p2g(const Params<R>& p, State<D, R>& s, Grid<D
                     const R m = w * mass;
                     if (mls) {
                         R wv[3];
+                        // p2g.glsl:80-86 in glm's order: v + (3 B) (-dist) and
+                        // (((V sigma) dist) 3) dt
                         for (int r = 0; r < D; ++r) {
                             R Bd = 0, Sd = 0;
-                            for (int k = 0; k < D; ++k) { Bd += B[r * D + k] * (-dist[k]); Sd += st[r * D + k] * dist[k]; }
-                            R apic = v[r] + dinv * Bd;
-                            R force = vol * Sd * dinv * p.dt;
+                            for (int k = 0; k < D; ++k) {
+                                Bd += (dinv * B[r * D + k]) * (-dist[k]);
+                                Sd += (vol * st[r * D + k]) * dist[k];
+                            }
+                            R apic = v[r] + Bd;
+                            R force = (Sd * dinv) * p.dt;
                             wv[r] = m * apic + w * force;
                         }
                         add_to(&g.mass[cid], m, atomic);
@@ -622,6 +633,21 @@ void orc_bspline_f64(double x, double* n, double* dn) { *n = orc::bspline_n(x); 
 void orc_svd_f64(int32_t dim, int32_t formulation, const double* M, double* U, double* S, double* V) {
     if (dim == 2) orc::svd<2>(M, U, S, V, formulation);
     else orc::svd<3>(M, U, S, V, formulation);
+}
+
+// FP32 instantiations of the same helpers (compared with the reference's
+// shader functions compiled for the CPU, oracle/shader/shader_runner.cpp).
+void orc_bspline_f32(float x, float* n, float* dn) { *n = orc::bspline_n(x); *dn = orc::bspline_dn(x); }
+
+void orc_svd_f32(int32_t dim, int32_t formulation, const float* M, float* U, float* S, float* V) {
+    if (dim == 2) orc::svd<2>(M, U, S, V, formulation);
+    else orc::svd<3>(M, U, S, V, formulation);
+}
+
+void orc_collide_f32(const orc_params* q, const float* loc, const float* vel, float* vcol, float* vfric) {
+    orc::Params<float> p = to_params<float>(q);
+    if (q->dim == 2) orc::collide<2>(p, loc, vel, vcol, vfric);
+    else orc::collide<3>(p, loc, vel, vcol, vfric);
 }
 
 void orc_stress_f64(const orc_params* q, const double* Fe, const double* Fp, double* out) {

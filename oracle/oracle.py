@@ -58,6 +58,13 @@ def lib():
         L.orc_stress_f64.restype = None
         L.orc_collide_f64.argtypes = [C.POINTER(OrcParams), dp, dp, dp, dp]
         L.orc_collide_f64.restype = None
+        fp = C.POINTER(C.c_float)
+        L.orc_bspline_f32.argtypes = [C.c_float, fp, fp]
+        L.orc_bspline_f32.restype = None
+        L.orc_svd_f32.argtypes = [C.c_int32, C.c_int32, fp, fp, fp, fp]
+        L.orc_svd_f32.restype = None
+        L.orc_collide_f32.argtypes = [C.POINTER(OrcParams), fp, fp, fp, fp]
+        L.orc_collide_f32.restype = None
         L.orc_p2g_f64.argtypes = [C.POINTER(OrcParams), C.c_int64] + [dp] * 9
         L.orc_max_threads.restype = C.c_int
         _lib = L
