@@ -11,12 +11,16 @@ is larger than the 126 MB L2, so no flush is needed between steps).
 
 * value     device time (CUDA events on the solver's stream) for K steps with
             state resident in HBM; max over ranks; N ranks run independent
-            replicas (the path does not shard across GPUs here).
+            replicas (the path does not shard across GPUs here). The K-step
+            loop is repeated until 200 ms have passed (so that the clock
+            sampler sees the timed region); value is the median repetition.
 * e2e       the same metric through the public C ABI with host buffers: every
             step uploads the particle state from pinned host memory
             (mpm_set_state), steps, and reads the state back (mpm_get_state).
 * roofline  the dominant kernel's algorithmic bytes / its CUDA-event duration,
-            against MEASURED_PEAKS.json's HBM copy bandwidth.
+            against MEASURED_PEAKS.json's HBM copy bandwidth; `traffic` is the
+            DRAM bytes per launch of that kernel from the ncu summary committed
+            under profiles/ (a "bench-traffic:" line), named in traffic_source.
 * cpu_baseline  the oracle's FP32 OpenMP port of the reference MLS step on the
             host cores, a bounded number of steps of the same scene.
 
@@ -43,9 +47,22 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-updates/s (P2G+grid+G2P), plain vs MLP-plasticity, 1 B200, % HBM peak"
 UNIT = "particle-updates/s"
-# DRAM bytes (read + write) per launch of the dominant kernels, from one full
-# ncu capture of the same scene (dram__bytes_read.sum + dram__bytes_write.sum).
-NCU_TRAFFIC = {("c3", "p2g"): 113.1e6, ("c3", "g2p"): 315.1e6}
+STAGE_KERNEL = {"p2g": "k_p2g_warp", "g2p": "k_g2p_gather", "g2p2g": "k_g2p2g", "grid_update": "k_grid_marked",
+                "return_map": "k_g2p_plastic"}
+
+
+def profile_traffic(workload: str, stage: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a
+    stage's kernel on a workload, from the ncu summaries under profiles/: lines
+    `bench-traffic: <kernel> <workload> <bytes per launch>`. (None, None) when
+    no summary holds one."""
+    kernel = STAGE_KERNEL.get(stage)
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) == 4 and parts[0] == "bench-traffic:" and parts[1] == kernel and parts[2] == workload:
+                return float(parts[3]), f"profiles/{f.name}"
+    return None, None
 
 # Algorithmic bytes (minimal FP32 SoA state, uniform mass/volume).
 # Per particle-step: P2G reads x, v, B, F_E, J_p; G2P reads x, F_E, J_p and
@@ -163,10 +180,37 @@ def make_scene(name):
 
 def kernel_launches(steps, sorts, auto_period):
     """Kernels the tiled 3D/2D MLS step enqueues over `steps` steps with `sorts`
-    re-binning sorts: P2G, grid update, G2P gather and G2P plastic every step,
-    the four sort kernels (count, scan, bucket, per-tile sort) per sort, and with
-    the auto period the velocity maximum that picks each period's length."""
+    re-binning sorts: four every step (fused transfer: grid update, the fused
+    G2P + next P2G, the queued particles' return map and their P2G; split
+    transfer: P2G, grid update, G2P gather, return map), the four sort kernels
+    (count, scan, bucket, per-tile sort) per sort, and with the auto period the
+    velocity maximum that picks each period's length."""
     return 4 * steps + (5 if auto_period else 4) * sorts
+
+
+def active_nodes_initial(scene) -> int:
+    """Grid nodes inside some particle's stencil at the scene's initial
+    positions (the cubic stencil int(x) - 1 .. int(x) + 2 per axis)."""
+    d = scene.dim
+    ext = [scene.width, scene.height, scene.depth][:d]
+    nx = [e + 1 for e in ext]
+    base = np.floor(np.clip(scene.position.astype(np.float64), -8, None)).astype(np.int64) - 1
+    marks = np.zeros(int(np.prod(nx)), bool)
+    offs = np.stack(np.meshgrid(*([np.arange(4)] * d), indexing="ij"), -1).reshape(-1, d)
+    for o in offs:
+        g = base + o
+        ok = np.all((g >= 0) & (g <= np.array(ext)), axis=1)
+        g = g[ok]
+        idx = g[:, 0] + nx[0] * g[:, 1] + (nx[0] * nx[1] * g[:, 2] if d == 3 else 0)
+        marks[idx] = True
+    return int(marks.sum())
+
+
+def config_of(args, scene, world) -> dict:
+    """The workload description both arms print."""
+    return {"workload": f"{args.workload}: {WORKLOADS[args.workload]}", "particles": scene.count,
+            "nodes": scene.nodes, "active_nodes_initial": active_nodes_initial(scene), "plasticity": "exact",
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
 
 
 def rel_l2(a, b):
@@ -219,7 +263,9 @@ def mlp_vs_plain(args, torch, stream):
         res[mode] = r
     for s in solvers.values():
         s.close()
-    g2p = lambda r: r["stages_ms"]["g2p"] + r["stages_ms"]["return_map"]
+    # G2P = the gather (with the fused transfer: the fused kernel, which also
+    # does the next step's P2G) + the return map of the queued particles
+    g2p = lambda r: r["stages_ms"].get("g2p", r["stages_ms"].get("g2p2g", 0.0)) + r["stages_ms"]["return_map"]
     return {
         "workload": f"{args.mlp_workload}: {WORKLOADS[args.mlp_workload]}", "particles": scene.count,
         "steps": args.mlp_steps, "tolerance": args.mlp_tolerance, "plain": res["exact"], "mlp": res["mlp"],
@@ -350,6 +396,25 @@ def refcpu_time(scene, steps, replicas):
     return scene.count * steps * replicas / info["loop_seconds"], info
 
 
+def reference_cpu_leg(steps):
+    """The reference's own CPU path (src/cpu compiled unmodified) on the 2D
+    three-block workload (128^2, 4 ppc): `steps` steps on one core, then one
+    independent single-threaded solver per host core at once."""
+    from mpm_snow_sim2d_b200 import scenes
+    from oracle import oracle as O
+    if not O.refcpu_available():
+        return {"unavailable": "oracle/_ref/refcpu_driver is not built"}
+    scene = scenes.workload("c1")
+    cores = os.cpu_count() or 1
+    one, info1 = refcpu_time(scene, steps, 1)
+    many, infon = refcpu_time(scene, steps, cores)
+    return {"workload": f"c1: {WORKLOADS['c1']}", "particles": scene.count, "steps": steps, "unit": UNIT,
+            "one_core": one, "all_cores": many, "cores": cores, "kind": "reference",
+            "sample": f"{steps} steps per solver; the reference's src/cpu (CLASSIC APIC, single-threaded) compiled "
+                      f"unmodified; all_cores = {cores} independent solvers at once",
+            "loop_seconds": {"one_core": info1.get("loop_seconds"), "all_cores": infon.get("loop_seconds")}}
+
+
 def run_reference_arm(args):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -383,7 +448,7 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
-        "config": {"workload": f"{args.workload}: {WORKLOADS.get(args.workload, '')}", "particles": scene.count},
+        "config": config_of(args, scene, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -410,6 +475,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-latency-calls", type=int, default=50)
     ap.add_argument("--quad-steps", type=int, default=500, help="timed steps of the quadratic-stencil line (0: skip)")
+    ap.add_argument("--refcpu-steps", type=int, default=1000,
+                    help="steps of the reference's compiled src/cpu on the 2D three-block workload (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -446,22 +513,33 @@ def main():
     m, _ = solver.rasterize()
     active = int((m > 0).sum())
 
-    # ---- timed region: K steps, state resident in HBM ----
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sorts0, _ = solver.sort_stats()
+    # ---- timed region: K steps, state resident in HBM, repeated until the
+    # repetitions span 200 ms (every rank runs the same count); value from the
+    # median repetition ----
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(device) as clocks:
+
+    def timed_k_steps():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         e0.record(stream)
         solver.Step(args.steps)
         e1.record(stream)
         e1.synchronize()
-    torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    sorts0, _ = solver.sort_stats()
+    reps_ms = []
+    with ClockSampler(device) as clocks:
+        reps_ms.append(timed_k_steps())
+        reps = int(max_over_ranks(float(max(1, -(-200.0 // max(reps_ms[0], 1e-3))))))
+        while len(reps_ms) < reps:
+            reps_ms.append(timed_k_steps())
+    ms = float(np.median(reps_ms))
     flags = solver.status()
     sorts1, period_end = solver.sort_stats()
-    timed_sorts = sorts1 - sorts0
+    timed_sorts = (sorts1 - sorts0) / len(reps_ms)
     value = job_rate(world, scene.count, args.steps, ms / 1e3)
 
     # ---- per-stage device time (events between kernels), for the roofline ----
@@ -494,17 +572,27 @@ def main():
     e2e_value = job_rate(world, n, ke, e2e_s)
 
     # ---- roofline of the dominant kernel ----
+    # Algorithmic bytes per launch: the split transfer's P2G reads x, v, B, F_E,
+    # J_p and its G2P reads x, F_E, J_p, writes x, v, B, F_E, J_p and reads
+    # the active nodes' velocities; the fused kernel does the G2P of a step and
+    # the P2G of the next, so it carries both particle terms (its P2G takes
+    # x, v, B, F_E, J_p from registers: its DRAM traffic is below this count).
     peak, peak_src = load_peaks()
     p2g_b, g2p_b = bytes_per_particle(d)
     grid_b, g2p_nb = bytes_per_node(d)
-    alg = {"p2g": n * p2g_b, "grid_update": active * grid_b, "g2p": n * g2p_b + active * g2p_nb}
+    if "g2p2g" in stage_avg:
+        alg = {"g2p2g": n * (p2g_b + g2p_b) + active * g2p_nb, "grid_update": active * grid_b}
+    else:
+        alg = {"p2g": n * p2g_b, "grid_update": active * grid_b, "g2p": n * g2p_b + active * g2p_nb}
     dom = max(alg, key=lambda k: stage_avg.get(k, 0.0))
     achieved = alg[dom] / (stage_avg[dom] / 1e3) / 1e9
     step_bytes = sum(alg.values())
     step_ms = ms / args.steps
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": NCU_TRAFFIC.get((args.workload, dom)), "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": alg[dom],
+    traffic, traffic_src = profile_traffic(args.workload, dom)
+    roofline = {"bound": "hbm", "kernel": STAGE_KERNEL[dom], "stage": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": alg[dom],
+                "kernel_ms": stage_avg[dom], "timing": "CUDA events on the solver's stream around the stage, every step",
                 "step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
                          "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
 
@@ -537,25 +625,33 @@ def main():
         except Exception as e:  # the CPU baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
+    refcpu_leg = None
+    if rank == 0 and world == 1 and args.refcpu_steps > 0:
+        try:
+            refcpu_leg = reference_cpu_leg(args.refcpu_steps)
+        except Exception as e:  # reported, never required
+            refcpu_leg = {"error": str(e)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": f"synthetic (seeded {scene.name} scene, {scene.count} particles)",
-            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]}", "particles": scene.count,
-                       "nodes": scene.nodes, "active_nodes": active, "plasticity": "exact",
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
-                       "sort_period": (f"auto ({timed_sorts} sorts in the timed steps, last period {period_end})"
-                                       if args.sort_period <= 0 else args.sort_period)},
+            "config": config_of(args, scene, world),
+            "sort_period": (f"auto ({timed_sorts:g} sorts per {args.steps} timed steps, last period {period_end})"
+                            if args.sort_period <= 0 else args.sort_period),
+            "active_nodes": active, "timed_repetitions": len(reps_ms),
+            "repetition_ms": reps_ms,
             "roofline": roofline,
             "stages_ms": stage_avg,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": ke},
-            "gpu_launches": kernel_launches(args.steps, timed_sorts, args.sort_period <= 0),
+            "gpu_launches": int(round(kernel_launches(args.steps, timed_sorts, args.sort_period <= 0))),
             "clocks": clocks.summary(),
             "status_flags": flags,
             "cpu_baseline": cpu,
+            "reference_cpu_2d": refcpu_leg,
             "mlp_vs_plain": mlp,
             "quadratic": quad,
             "batched": batch,

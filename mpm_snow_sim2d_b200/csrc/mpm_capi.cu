@@ -1,6 +1,7 @@
 // C ABI of the B200 MLS-MPM solver (include/mpm/mpm.h): device memory, the
 // step sequence, state import/export and checkpoints. The product path has no
 // CPU fallback: without a usable sm_100 device every create fails.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <random>
@@ -15,6 +16,7 @@
 #include "mpm/mpm.h"
 #include "mpm_kernels.cuh"
 #include "mpm_tiled.cuh"
+#include "mpm_fused.cuh"
 #include "mpm_mlp.cuh"
 #include "mpm_render.cuh"
 #include "mpm_host.h"
@@ -103,6 +105,14 @@ struct mpm_solver {
     long long log_cap = 0;
     bool needs_affine = true; // A must be recomputed from the state before the next P2G
     SlowQueue q{};
+    // fused transfer (tiled MLS path): one kernel per step does the G2P of the
+    // step and the P2G of the next; `acc_pending` says the grid sums of the
+    // current state are already in `acc` (else the next step starts with the
+    // P2G-only prologue).
+    bool fused = false;
+    bool acc_pending = false;
+    unsigned char* lone = nullptr;  // per slot: scattered one by one at the last fused step
+    int fused_grid = 0;
 };
 
 namespace {
@@ -177,6 +187,10 @@ void release(mpm_solver* s) {
     if (s->q.list) cudaFree(s->q.list);
     if (s->q.count) cudaFree(s->q.count);
     if (s->q.fh) cudaFree(s->q.fh);
+    if (s->q.slot) cudaFree(s->q.slot);
+    if (s->ti.tile_len) cudaFree(s->ti.tile_len);
+    if (s->ti.fused_next) cudaFree(s->ti.fused_next);
+    if (s->lone) cudaFree(s->lone);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -240,7 +254,9 @@ template <int D, int S> cudaError_t launch_sort(mpm_solver* s) {
     k_sort_count<D, S><<<blocks, threads, 0, s->stream>>>(particle_view(s), s->C, s->ti);
     k_sort_scan<<<1, 1024, 0, s->stream>>>(s->ti);
     k_sort_bucket<<<blocks, threads, 0, s->stream>>>(s->n, s->ti);
-    k_tile_sort<D, S><<<s->sms * SortGeom<D>::CTAS_PER_SM, 256, 0, s->stream>>>(particle_view(s), s->id, s->alt, s->C,
+    SortBuffers dst = s->alt;
+    if (s->fused) dst.A = nullptr;  // the fused path keeps A only within a step
+    k_tile_sort<D, S><<<s->sms * SortGeom<D>::CTAS_PER_SM, 256, 0, s->stream>>>(particle_view(s), s->id, dst, s->C,
                                                                                s->ti);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -395,6 +411,45 @@ template <int D, int S> cudaError_t launch_p2g_tiled(mpm_solver* s) {
     return launch_p2g_tiled_kernel<D, S>(s);
 }
 
+// ---- fused transfer ----
+
+// The fused kernel over the tiles of the last sort: G2P (this step) + P2G (next
+// step), or with G2P = false the P2G of the stored state (prologue).
+template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
+    cudaError_t e = cudaMemsetAsync(s->ti.fused_next, 0, sizeof(int), s->stream);
+    if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return e;
+    if (s->n == 0) return cudaSuccess;
+    k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
+        particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->lone, s->status);
+    return cudaGetLastError();
+}
+
+// Queued particles after the G2P part: their return map (learned and/or
+// exact), then their P2G for the next step one by one.
+template <int D, int S> cudaError_t launch_queued_fused(mpm_solver* s) {
+    if (s->n == 0) return cudaSuccess;
+    cudaError_t e = launch_return_map<D, S>(s);
+    if (e != cudaSuccess) return e;
+    k_p2g_lone<D, S><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->ti, s->q, s->acc, s->status);
+    return cudaGetLastError();
+}
+
+// The P2G of the current state when it is not pending yet: the sort first if
+// one is due (the kernel works on the tiles of the last sort).
+template <int D, int S> cudaError_t fused_prologue(mpm_solver* s) {
+    if (s->acc_pending) return cudaSuccess;
+    if (sort_due(s)) {
+        cudaError_t e = launch_sort<D, S>(s);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = launch_fused<D, S, false>(s);
+    if (e != cudaSuccess) return e;
+    s->acc_pending = true;
+    s->needs_affine = false;
+    return cudaSuccess;
+}
+
 template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
     k_grid_marked<D, kMLS><<<s->sms * 8, 256, 0, s->stream>>>(s->C, s->ti, s->acc, s->gv, s->status);
     cudaError_t e = cudaGetLastError();
@@ -402,7 +457,19 @@ template <int D> cudaError_t launch_grid_marked(mpm_solver* s) {
     return cudaSuccess;
 }
 
+// One fused step: [sort] grid update, fused G2P + next P2G, queued particles.
+template <int D, int S> cudaError_t step_fused(mpm_solver* s) {
+    cudaError_t e = fused_prologue<D, S>(s);
+    if (e != cudaSuccess) return e;
+    if (sort_due(s) && (e = launch_sort<D, S>(s)) != cudaSuccess) return e;
+    if ((e = launch_grid_marked<D>(s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream)) != cudaSuccess) return e;
+    if ((e = launch_fused<D, S, true>(s)) != cudaSuccess) return e;
+    return launch_queued_fused<D, S>(s);
+}
+
 template <int D, int S> cudaError_t step_tiled(mpm_solver* s) {
+    if (s->fused) return step_fused<D, S>(s);
     cudaError_t e = launch_p2g_tiled<D, S>(s);
     if (e != cudaSuccess) return e;
     e = launch_grid_marked<D>(s);
@@ -429,6 +496,10 @@ cudaError_t dispatch_step(mpm_solver* s) {
 }
 
 cudaError_t dispatch_p2g(mpm_solver* s) {
+    if (s->tiled && s->fused) {
+        if (s->stencil == 3) return s->dim == 2 ? fused_prologue<2, 3>(s) : fused_prologue<3, 3>(s);
+        return s->dim == 2 ? fused_prologue<2, 4>(s) : fused_prologue<3, 4>(s);
+    }
     if (s->tiled) {
         if (s->stencil == 3) return s->dim == 2 ? launch_p2g_tiled<2, 3>(s) : launch_p2g_tiled<3, 3>(s);
         return s->dim == 2 ? launch_p2g_tiled<2, 4>(s) : launch_p2g_tiled<3, 4>(s);
@@ -438,6 +509,7 @@ cudaError_t dispatch_p2g(mpm_solver* s) {
 
 // After a P2G-only pass: clear accumulators and node-block marks.
 cudaError_t clear_after_p2g(mpm_solver* s) {
+    s->acc_pending = false;
     if (s->tiled) {
         cudaError_t e = s->dim == 2 ? launch_grid_marked<2>(s) : launch_grid_marked<3>(s);
         if (e != cudaSuccess) return e;
@@ -503,9 +575,37 @@ mpm_status setup_tiled(mpm_solver* s) {
     }
     s->q.capacity = n > 0 ? n : 1;
     if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 1) ||
-        dalloc(&s->q.fh, (size_t)s->q.capacity * D * D)) {
+        dalloc(&s->q.fh, (size_t)s->q.capacity * D * D) || dalloc(&s->q.slot, (size_t)s->q.capacity) ||
+        dalloc(&ti.tile_len, (size_t)ti.n_tiles) || dalloc(&ti.fused_next, 1) || dalloc(&s->lone, (size_t)n)) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
+    }
+    if (cudaMemset(s->lone, 0, (size_t)(n > 0 ? n : 1)) != cudaSuccess) return MPM_ERR_CUDA;
+    {
+        // MPM_TRANSFER=split selects the separate P2G / G2P kernels (for comparison)
+        const char* tr = std::getenv("MPM_TRANSFER");
+        s->fused = !(tr && std::strcmp(tr, "split") == 0);
+    }
+    if (s->fused) {
+        const void* kfn;
+        size_t fsm;
+        const void* kpro;
+        if (D == 3) {
+            kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
+            kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false> : (const void*)k_g2p2g<3, 4, false>;
+            fsm = sizeof(FusedSmem<3>);
+        } else {
+            kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
+            kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false> : (const void*)k_g2p2g<2, 4, false>;
+            fsm = sizeof(FusedSmem<2>);
+        }
+        int per = 0;
+        cudaError_t ef = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+        if (ef == cudaSuccess) ef = cudaFuncSetAttribute(kpro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+        if (ef == cudaSuccess)
+            ef = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, FusedGeom<3>::THREADS, fsm);
+        if (ef != cudaSuccess || per < 1) return MPM_ERR_CUDA;
+        s->fused_grid = s->sms * per;
     }
     s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 16;
     s->auto_sort = s->params.sort_period <= 0;
@@ -612,7 +712,22 @@ template <int D, int S> cudaError_t stage_tiled(mpm_solver* s, int k) {
     if (k == 3) return launch_g2p_gather<D, S>(s);
     return launch_return_map<D, S>(s);
 }
+template <int D, int S> cudaError_t stage_fused(mpm_solver* s, int k) {
+    if (k == 0) return sort_due(s) ? launch_sort<D, S>(s) : cudaSuccess;
+    if (k == 1) return fused_prologue<D, S>(s);
+    if (k == 2) {
+        cudaError_t e = launch_grid_marked<D>(s);
+        if (e != cudaSuccess) return e;
+        return cudaMemsetAsync(s->ti.n_marked, 0, sizeof(int), s->stream);
+    }
+    if (k == 3) return launch_fused<D, S, true>(s);
+    return launch_queued_fused<D, S>(s);
+}
 cudaError_t dispatch_stage(mpm_solver* s, int k) {
+    if (s->tiled && s->fused) {
+        if (s->stencil == 3) return s->dim == 2 ? stage_fused<2, 3>(s, k) : stage_fused<3, 3>(s, k);
+        return s->dim == 2 ? stage_fused<2, 4>(s, k) : stage_fused<3, 4>(s, k);
+    }
     if (s->tiled) {
         if (s->stencil == 3) return s->dim == 2 ? stage_tiled<2, 3>(s, k) : stage_tiled<3, 3>(s, k);
         return s->dim == 2 ? stage_tiled<2, 4>(s, k) : stage_tiled<3, 4>(s, k);
@@ -836,7 +951,7 @@ mpm_status mpm_step(mpm_solver* s, int32_t nsteps) {
         const int K = s->auto_sort ? s->cur_K : s->sort_period;
         const bool period_start = s->auto_sort ? s->step >= s->next_sort : (K > 0 && s->step % K == 0);
         if (s->tiled && s->use_graphs && K > 0 && nsteps - k >= K && period_start && !s->needs_sort &&
-            !s->needs_affine) {
+            !s->needs_affine && (!s->fused || s->acc_pending)) {
             const int r = run_period_graph(s);
             if (r < 0) return MPM_ERR_CUDA;
             if (r > 0) {
@@ -855,7 +970,10 @@ mpm_status mpm_step(mpm_solver* s, int32_t nsteps) {
 
 int32_t mpm_stage_count(const mpm_solver*) { return kStages; }
 
-const char* mpm_stage_name(const mpm_solver*, int32_t k) {
+const char* mpm_stage_name(const mpm_solver* s, int32_t k) {
+    // fused path: "p2g" is the prologue (first step after creation or an
+    // upload), "g2p2g" the G2P of each step with the next step's P2G
+    if (s && s->tiled && s->fused && k == 3) return "g2p2g";
     return (k >= 0 && k < kStages) ? kStageNames[k] : "";
 }
 
@@ -930,6 +1048,12 @@ mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
     if (st->affine_b && (r = import_field(s, s->B, D * D, st->affine_b)) != MPM_OK) return r;
     if (st->elastic_f && (r = import_field(s, s->Fe, D * D, st->elastic_f)) != MPM_OK) return r;
     if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
+    if (s->fused) {
+        // the pending grid sums belong to the old state; the next step starts
+        // with the P2G-only prologue, every particle grouped
+        if (s->acc_pending) MPM_CUDA(s, clear_after_p2g(s));
+        MPM_CUDA(s, cudaMemsetAsync(s->lone, 0, (size_t)(s->n > 0 ? s->n : 1), s->stream));
+    }
     s->needs_sort = true;
     s->needs_affine = true;
     s->nplan = 0;  // the next period is measured from the uploaded state
@@ -944,7 +1068,7 @@ mpm_status mpm_rasterize(mpm_solver* s, double* node_mass, double* node_momentum
     if (e != cudaSuccess) return cuda_fail(s, e, "p2g launch");
     std::vector<long long> h((size_t)NA * s->nodes);
     MPM_CUDA(s, cudaMemcpyAsync(h.data(), s->acc, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost, s->stream));
-    MPM_CUDA(s, clear_after_p2g(s));
+    if (!(s->tiled && s->fused)) MPM_CUDA(s, clear_after_p2g(s));  // fused: these are the next step's sums
     MPM_CUDA(s, cudaStreamSynchronize(s->stream));
     const double ism = std::ldexp(1.0, -s->log2_sm), isp = std::ldexp(1.0, -s->log2_sp),
                  isf = std::ldexp(1.0, -s->log2_sf);
@@ -1010,6 +1134,8 @@ mpm_status mpm_get_fixed_point(const mpm_solver* s, int32_t* lm, int32_t* lp) {
 }
 
 constexpr int kSchedTag = 0x4B504552;  // extra record: auto sort schedule
+constexpr int kTileTag = 0x454C4954;   // extra record: {tag, tile, first slot, particles} of the last sort
+constexpr int kLoneTag = 0x454E4F4C;   // extra record: {tag, 64-slot word, bits 0-31, bits 32-63} of lone flags
 
 // Checkpoint: "MPMS" | u32 version=2 | i32 dim | i64 count | i32 W, H, D |
 // u64 params hash | i64 step | f32 x[n*d] v[n*d] B[n*d*d] Fe[n*d*d] Jp[n]
@@ -1018,7 +1144,11 @@ constexpr int kSchedTag = 0x4B504552;  // extra record: auto sort schedule
 // resumed run groups particles exactly as the original did and continues
 // bit-identically. `extra` holds tagged records: with the auto sort period,
 // one {kSchedTag, period, steps to the next sort, next two periods (8 bits
-// each; 0: measure)}; unknown records are skipped on load.
+// each; 0: measure)}; on the fused path one {kTileTag, tile, first slot,
+// count} per non-empty tile of the last sort (the particles' tiles at that
+// sort cannot be recomputed from their current positions) and {kLoneTag,
+// word, low bits, high bits} for each 64 slots holding particles the last step
+// scattered one by one; unknown records are skipped on load.
 mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
     const int D = s->dim;
@@ -1032,13 +1162,36 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     // extra records: the auto sort schedule (period length, steps to the next sort)
     int planned[2] = {0, 0};
     for (int q = 0; s->auto_sort && q < s->nplan; ++q) MPM_CUDA(s, resolve_plan(s, s->plan[q], &planned[q]));
-    const int4 sched = make_int4(kSchedTag, s->cur_K, (int)(s->next_sort - s->step), planned[0] | (planned[1] << 8));
-    const int32_t n_extra = s->auto_sort ? 1 : 0;
+    std::vector<int4> extra;
+    if (s->auto_sort)
+        extra.push_back(make_int4(kSchedTag, s->cur_K, (int)(s->next_sort - s->step), planned[0] | (planned[1] << 8)));
     if (has_order) {
         ids.resize(n);
         MPM_CUDA(s, cudaMemcpyAsync(ids.data(), s->id, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
         MPM_CUDA(s, cudaStreamSynchronize(s->stream));
     }
+    if (has_order && s->fused && n > 0) {
+        int ntl = 0;
+        MPM_CUDA(s, cudaMemcpy(&ntl, s->ti.n_tile_list, sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int> tl(ntl), tlen(ntl), tstart(s->ti.n_tiles);
+        if (ntl > 0) {
+            MPM_CUDA(s, cudaMemcpy(tl.data(), s->ti.tile_list, sizeof(int) * ntl, cudaMemcpyDeviceToHost));
+            MPM_CUDA(s, cudaMemcpy(tlen.data(), s->ti.tile_len, sizeof(int) * ntl, cudaMemcpyDeviceToHost));
+        }
+        MPM_CUDA(s, cudaMemcpy(tstart.data(), s->ti.tile_start, sizeof(int) * s->ti.n_tiles, cudaMemcpyDeviceToHost));
+        for (int e = 0; e < ntl; ++e) extra.push_back(make_int4(kTileTag, tl[e], tstart[tl[e]], tlen[e]));
+        if (s->acc_pending) {
+            std::vector<unsigned char> lone(n);
+            MPM_CUDA(s, cudaMemcpy(lone.data(), s->lone, n, cudaMemcpyDeviceToHost));
+            for (size_t w = 0; w * 64 < n; ++w) {
+                unsigned lo = 0, hi = 0;
+                for (size_t b = 0; b < 64 && w * 64 + b < n; ++b)
+                    if (lone[w * 64 + b]) (b < 32 ? lo : hi) |= 1u << (b & 31);
+                if (lo | hi) extra.push_back(make_int4(kLoneTag, (int)w, (int)lo, (int)hi));
+            }
+        }
+    }
+    const int32_t n_extra = (int32_t)extra.size();
     FILE* f = std::fopen(path, "wb");
     if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
     const uint32_t ver = 2;
@@ -1053,7 +1206,7 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     ok = ok && std::fwrite(&has_order, 4, 1, f) == 1;
     if (has_order) {
         ok = ok && std::fwrite(ids.data(), sizeof(int), n, f) == n && std::fwrite(&n_extra, 4, 1, f) == 1;
-        if (n_extra) ok = ok && std::fwrite(&sched, sizeof(int4), 1, f) == 1;
+        if (n_extra) ok = ok && std::fwrite(extra.data(), sizeof(int4), extra.size(), f) == extra.size();
     }
     ok = (std::fclose(f) == 0) && ok;
     return ok ? MPM_OK : fail(s, MPM_ERR_IO, "short write");
@@ -1085,6 +1238,8 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     std::vector<int> ids;
     int n_extra = 0;
     int sched_K = 0, sched_next = 0, sched_pending = 0;
+    std::vector<int4> tiles;                 // {tile, first slot, count} of the last sort (fused path)
+    std::vector<unsigned char> lone_flags;   // per slot (fused path)
     if (ok && ver == 2) {
         ok = std::fread(&has_order, 4, 1, f) == 1;
         if (ok && has_order) {
@@ -1101,6 +1256,13 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
                         sched_K = extra[q].y;
                         sched_next = extra[q].z;
                         sched_pending = extra[q].w;
+                    } else if (extra[q].x == kTileTag) {
+                        tiles.push_back(make_int4(extra[q].y, extra[q].z, extra[q].w, 0));
+                    } else if (extra[q].x == kLoneTag && extra[q].y >= 0 && (size_t)extra[q].y * 64 < n) {
+                        if (lone_flags.empty()) lone_flags.assign(n, 0);
+                        for (int b = 0; b < 64 && (size_t)extra[q].y * 64 + b < n; ++b)
+                            if (((unsigned)(b < 32 ? extra[q].z : extra[q].w) >> (b & 31)) & 1u)
+                                lone_flags[(size_t)extra[q].y * 64 + b] = kLoneScatter;
                     }
             }
             // every slot must name a distinct particle
@@ -1121,6 +1283,34 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     if (r != MPM_OK) return r;
     if (restore_order) {
         s->needs_sort = false;
+    }
+    if (restore_order && s->fused && n > 0) {
+        // the fused kernel walks the tiles of the last sort: restore them when
+        // the records are complete (disjoint, in slot order, covering every
+        // slot, tiles in range), else sort again (the run then continues
+        // correctly but no longer bit-identically)
+        std::sort(tiles.begin(), tiles.end(), [](const int4& a, const int4& b) { return a.y < b.y; });
+        bool good = !tiles.empty();
+        long long next = 0;
+        for (size_t e = 0; good && e < tiles.size(); ++e) {
+            good = tiles[e].x >= 0 && tiles[e].x < s->ti.n_tiles && tiles[e].y == next && tiles[e].z >= 1 &&
+                   (long long)tiles[e].y + tiles[e].z <= (long long)n && (e == 0 || tiles[e].x > tiles[e - 1].x);
+            next += tiles[e].z;
+        }
+        good = good && next == (long long)n;
+        if (good) {
+            const int ntl = (int)tiles.size();
+            std::vector<int> tl(ntl), tlen(ntl), tstart(s->ti.n_tiles, 0);
+            for (int e = 0; e < ntl; ++e) { tl[e] = tiles[e].x; tlen[e] = tiles[e].z; tstart[tiles[e].x] = tiles[e].y; }
+            MPM_CUDA(s, cudaMemcpy(s->ti.tile_list, tl.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice));
+            MPM_CUDA(s, cudaMemcpy(s->ti.tile_len, tlen.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice));
+            MPM_CUDA(s, cudaMemcpy(s->ti.tile_start, tstart.data(), sizeof(int) * s->ti.n_tiles, cudaMemcpyHostToDevice));
+            MPM_CUDA(s, cudaMemcpy(s->ti.n_tile_list, &ntl, sizeof(int), cudaMemcpyHostToDevice));
+            if (!lone_flags.empty())
+                MPM_CUDA(s, cudaMemcpy(s->lone, lone_flags.data(), n, cudaMemcpyHostToDevice));
+        } else {
+            s->needs_sort = true;
+        }
     }
     s->step = step;
     if (s->auto_sort) {  // resume the saved sort schedule (else sort at the next step)

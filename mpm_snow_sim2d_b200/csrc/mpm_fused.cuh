@@ -1,0 +1,692 @@
+// Fused transfer for the tiled MLS path: G2P of step n and P2G of step n+1 in
+// one kernel per step (the G2P2G scheme of Wang et al., "A Massively Parallel
+// and Scalable Multi-GPU Material Point Method", ACM TOG 39(4), 2020).
+//
+// One CTA per non-empty cell tile of the last sort (tiles handed out from a
+// counter). For its tile it
+//   1. stages the node velocities of a fixed box of BE^D nodes around the
+//      tile in shared memory (the stencils of every particle sorted into the
+//      tile that has since moved less than a cell);
+//   2. per particle (one thread each, in chunks of CHUNK slots): gathers the
+//      grid from that box (src/gpu/shaders/3d/g2p.glsl:28-71), updates x, v, B
+//      and the trial F_E, and when the return map is provably the identity
+//      (elastic band) computes the next step's P2G affine matrix
+//      A = 3 m B - 3 dt V sigma in registers (3d/p2g.glsl:44-90); the rest are
+//      queued for the exact (or learned) return map with their trial F;
+//   3. writes each in-band particle's P2G payload (stencil weights at the new
+//      position, m v, A) to shared memory, groups consecutive slots that share
+//      a stencil into runs, and SPLIT threads per run sum the run's node
+//      contributions in FP32 registers in slot order, then add them as int64
+//      fixed point to a shared-memory accumulator over the same node box;
+//   4. adds the box's non-zero sums to the global grid once per node and marks
+//      the touched node blocks for the grid update.
+// Particles whose stencil leaves the box (drifted more than a cell since the
+// sort) gather from and scatter to global memory directly. Queued particles
+// (out of the elastic band, or a stencil clipped by the grid edge) are
+// scattered one by one after their return map (k_p2g_lone).
+//
+// Determinism: every cross-run sum is an integer add, and the runs are a
+// function of the slot order, the chunk boundaries (fixed offsets inside a
+// tile) and which particles were queued -- all functions of the state. A
+// prologue pass of the same kernel (P2G only, reading the stored state)
+// reproduces the sums of a step boundary bit for bit when it is told which
+// particles were scattered one by one (the per-slot `lone` flags).
+#pragma once
+
+#include "mpm_tiled.cuh"
+
+namespace mpm {
+
+template <int D> struct FusedGeom {
+    static constexpr int T = TileGeom<D>::T;            // cells per tile edge: 4 (3D), 8 (2D)
+    static constexpr int BE = T + 5;                    // box edge in nodes: tile nodes - 2 .. tile + T + 2
+    static constexpr int BN = D == 3 ? BE * BE * BE : BE * BE;  // 729 (3D), 169 (2D)
+    static constexpr int NCH = 1 + D;                   // mass + momentum channels
+    static constexpr int THREADS = 256;
+    static constexpr int CHUNK = 256;                   // slots per pass (one per thread)
+    static constexpr int PS = WarpGeom<D, 4>::PS;       // payload floats per particle (3D 36, 2D 20)
+    static constexpr int KEYF = PS - 2;                 // payload floats holding the 64-bit stencil key
+};
+
+template <int D> struct FusedSmem {
+    using G = FusedGeom<D>;
+    float4 box[G::BN];                                  // 3D: (vf, wall flag); 2D: (vf, vc)
+    unsigned long long acc[G::NCH][G::BN];              // int64 fixed-point sums of the next step's P2G
+    float4 pay[G::CHUNK * G::PS / 4];
+    int run[G::CHUNK + 1];                              // start slot of each run, then the chunk end
+    unsigned starts[G::CHUNK / 32];                     // run-start ballot per warp
+    int tile;
+    unsigned bmask;                                     // node blocks (3^D around the tile) that received sums
+};
+
+#ifndef MPM_FUSED_MIN_BLOCKS
+#define MPM_FUSED_MIN_BLOCKS 3
+#endif
+
+// Per-slot flag of the last fused step: the particle was scattered one by one
+// (queued for the full return map); the P2G-only prologue scatters it the same
+// way so that resumed runs continue bit-identically.
+constexpr unsigned char kLoneScatter = 1;
+
+// ---------------------------------------------------------------------------
+// Interior gather from a node array with strides (sy, sz): the box in shared
+// memory (SMEM) or the global grid. Same sums and order as gather_interior.
+// `gc0`, `gsy`, `gsz`: the global node id of the first stencil node and the
+// global strides, for the wall-velocity pass (3D vc of nodes a wall moved is
+// only kept in global memory).
+template <int D, int S, bool SMEM, typename I>
+__device__ __forceinline__ void gather_nodes(const StepConsts& C, const float4* nodes, I c0, I sy, I sz,
+                                             const float4* __restrict__ gv, long long gc0, long long gsy, long long gsz,
+                                             const float (*wk)[S], const float (*off)[S], float* nv, float* nB,
+                                             float* nx) {
+    float wd[3][S];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+        for (int o = 0; o < S; ++o) wd[k][o] = wk[k][o] * off[k][o];
+    float vc[D];
+    bool wall = false;
+#pragma unroll
+    for (int r = 0; r < D; ++r) { nv[r] = 0.f; vc[r] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) nB[k] = 0.f;
+#pragma unroll 1
+    for (int a = 0; a < S; ++a) {
+        float Q[D], Qy[D], Qz[D], Qc[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r) { Q[r] = 0.f; Qy[r] = 0.f; Qz[r] = 0.f; Qc[r] = 0.f; }
+#pragma unroll
+        for (int b = 0; b < S; ++b) {
+            if constexpr (D == 3) {
+                float Pv[3] = {0.f, 0.f, 0.f}, Pd[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int c = 0; c < S; ++c) {
+                    const I cid = c0 + a + b * sy + c * sz;
+                    const float4 g = SMEM ? nodes[cid] : __ldg(&nodes[cid]);
+                    wall = wall || g.w != 0.f;
+                    const float z = wk[2][c], zd = wd[2][c];
+                    Pv[0] += z * g.x; Pv[1] += z * g.y; Pv[2] += z * g.z;
+                    Pd[0] += zd * g.x; Pd[1] += zd * g.y; Pd[2] += zd * g.z;
+                }
+                const float y = wk[1][b], yd = wd[1][b];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    Q[r] += y * Pv[r];
+                    Qy[r] += yd * Pv[r];
+                    Qz[r] += y * Pd[r];
+                }
+            } else {
+                const I cid = c0 + a + b * sy;
+                const float4 g = SMEM ? nodes[cid] : __ldg(&nodes[cid]);
+                const float y = wk[1][b], yd = wd[1][b];
+                Q[0] += y * g.x; Q[1] += y * g.y;
+                Qy[0] += yd * g.x; Qy[1] += yd * g.y;
+                Qc[0] += y * g.z; Qc[1] += y * g.w;
+            }
+        }
+        const float x = pick<S>(wk[0], a);
+        const float xd = pick<S>(wd[0], a);
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            nv[r] += x * Q[r];
+            nB[r * D + 0] += xd * Q[r];
+            nB[r * D + 1] += x * Qy[r];
+            if (D == 3) nB[r * D + 2] += x * Qz[r];
+            else vc[r] += x * Qc[r];
+        }
+    }
+    if constexpr (D == 3) {
+        if (!wall) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) vc[r] = nv[r];
+        } else {
+#pragma unroll 1
+            for (int a = 0; a < S; ++a) {
+                float Qc[3] = {0.f, 0.f, 0.f};
+#pragma unroll 1
+                for (int b = 0; b < S; ++b) {
+                    float Pc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int c = 0; c < S; ++c) {
+                        float f[3], g[3];
+                        load_node3(gv, C.nodes, gc0 + a + b * gsy + c * gsz, f, g);
+                        const float z = wk[2][c];
+                        Pc[0] += z * g[0]; Pc[1] += z * g[1]; Pc[2] += z * g[2];
+                    }
+                    const float y = wk[1][b];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) Qc[r] += y * Pc[r];
+                }
+                const float x = wk[0][a];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) vc[r] += x * Qc[r];
+            }
+        }
+    }
+    float sw[3], swd[3];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        sw[k] = sum_s<S>(wk[k]);
+        swd[k] = sum_s<S>(wd[k]);
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+        float t = swd[r];
+#pragma unroll
+        for (int l = 0; l < D; ++l)
+            if (l != r) t *= sw[l];
+        nx[r] = t + C.dt * vc[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2G payload of one particle at position x (layout of k_p2g_warp's payload;
+// the 64-bit stencil key goes in the last two floats).
+template <int D, int S>
+__device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, const float* x, const float* v,
+                                                          const float* A, float mass, float* q) {
+    using St = Stencil<S>;
+    unsigned long long k3 = 0;
+    float f[3], mv[3];
+#pragma unroll
+    for (int k = D - 1; k >= 0; --k) {
+        const int extk = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+        const int base = St::base(x[k], extk);
+        float wt[S];
+        St::weights(x[k], base, wt);
+#pragma unroll
+        for (int o = 0; o < 4; ++o) q[4 * k + o] = o < S ? wt[o] : 0.f;
+        f[k] = x[k] - float(base + 1);
+        mv[k] = mass * v[k];
+        k3 |= (unsigned long long)(base + 9) << (StencilKey<D>::BITS * k);
+    }
+    if constexpr (D == 3) {
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            q[12 + o] = q[4 + o] * (float(o - 1) - f[1]);
+            q[16 + o] = q[8 + o] * (float(o - 1) - f[2]);
+        }
+        reinterpret_cast<float4*>(q)[5] = make_float4(mass, mv[0] - f[0] * A[0], mv[1] - f[0] * A[3], mv[2] - f[0] * A[6]);
+        reinterpret_cast<float4*>(q)[6] = make_float4(A[0], A[3], A[6], A[1]);
+        reinterpret_cast<float4*>(q)[7] = make_float4(A[4], A[7], A[2], A[5]);
+        q[32] = A[8];
+        q[33] = 0.f;
+    } else {
+        reinterpret_cast<float4*>(q)[2] = make_float4(f[0], f[1], mass, mv[0]);
+        reinterpret_cast<float4*>(q)[3] = make_float4(mv[1], A[0], A[1], A[2]);
+        q[16] = A[3];
+        q[17] = 0.f;
+    }
+    return k3;
+}
+
+// Adds one int64 value: to the shared box (local index) or the global grid.
+__device__ __forceinline__ void add_fixed_shared(unsigned long long* p, float v, float scale) {
+    atomicAdd(p, (unsigned long long)__float2ll_rn(v * scale));
+}
+
+// ---------------------------------------------------------------------------
+// One work item of the run accumulation: split `a` of the run [j0, j1) with
+// stencil key kk. Sums in registers in slot order, then adds to the shared
+// box when the whole stencil lies in the box and in the grid, else to the
+// global grid (bounds-checked, marking node blocks). Same arithmetic as
+// k_p2g_warp.
+template <int D, int S>
+__device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& TI, FusedSmem<D>& SM, const int* bo,
+                                          int j0, int j1, unsigned long long kk, int a,
+                                          unsigned long long* __restrict__ acc, unsigned* __restrict__ status) {
+    using G = FusedGeom<D>;
+    using W = WarpGeom<D, S>;
+    constexpr int T = TileGeom<D>::T;
+    const float4* pay = SM.pay;
+    const float* payf = reinterpret_cast<const float*>(SM.pay);
+    int cell[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < D; ++k) cell[k] = int((kk >> (StencilKey<D>::BITS * k)) & StencilKey<D>::MASK) - 8;
+    // stencil nodes cell - 1 .. cell + S - 2 per axis
+    bool in_box = true, in_grid = true;
+    const int ext[3] = {C.W, C.H, C.Dp};
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        in_box = in_box && cell[k] - 1 - bo[k] >= 0 && cell[k] + S - 2 - bo[k] <= G::BE - 1;
+        in_grid = in_grid && cell[k] - 1 >= 0 && cell[k] + S - 2 <= ext[k];
+    }
+    if constexpr (D == 3) {
+        constexpr int NB = S * S / W::SPLIT;
+        constexpr int NN = NB * S;
+        const int ax = a % S, by0 = (a / S) * NB;
+        float am[NN], a0[NN], a1[NN], a2[NN];
+#pragma unroll
+        for (int k = 0; k < NN; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
+        const float da = float(ax - 1);
+        for (int j = j0; j < j1; ++j) {
+            const float4* pp = pay + j * (G::PS / 4);
+            const float alpha = payf[j * G::PS + ax];
+            const float4 wy = pp[1], wz = pp[2], yd = pp[3], zd = pp[4], ms = pp[5], q6 = pp[6], q7 = pp[7];
+            const float a22 = payf[j * G::PS + 32];
+            const float ad = alpha * da;
+            const float e0 = alpha * ms.y + ad * q6.x;
+            const float e1 = alpha * ms.z + ad * q6.y;
+            const float e2 = alpha * ms.w + ad * q6.z;
+            const float f0 = alpha * q6.w, f1 = alpha * q7.x, f2 = alpha * q7.y;
+            const float g0 = alpha * q7.z, g1 = alpha * q7.w, g2 = alpha * a22;
+            const float ma = ms.x * alpha;
+            const float Z[4] = {wz.x, wz.y, wz.z, wz.w};
+            const float Zd[4] = {zd.x, zd.y, zd.z, zd.w};
+            const float Yv[4] = {wy.x, wy.y, wy.z, wy.w};
+            const float Ydv[4] = {yd.x, yd.y, yd.z, yd.w};
+#pragma unroll
+            for (int bb = 0; bb < NB; ++bb) {
+                const int b = by0 + bb;
+                const float Y = NB == S ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
+                const float Yd = NB == S ? Ydv[bb] : (b == 0 ? yd.x : b == 1 ? yd.y : b == 2 ? yd.z : yd.w);
+                const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
+                const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
+#pragma unroll
+                for (int cc = 0; cc < S; ++cc) {
+                    const int idx = bb * S + cc;
+                    am[idx] += mY * Z[cc];
+                    a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
+                    a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
+                    a2[idx] += h2 * Z[cc] + k2 * Zd[cc];
+                }
+            }
+        }
+        float mx_m = 0.f, mx_p = 0.f;
+#pragma unroll
+        for (int k = 0; k < NN; ++k) {
+            mx_m = fmaxf(mx_m, fabsf(am[k]));
+            mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fmaxf(fabsf(a1[k]), fabsf(a2[k]))));
+        }
+        if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
+            raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
+        const int gx = cell[0] - 1 + ax;
+        if (in_box && in_grid) {
+            const int l0 = ((cell[2] - 1 - bo[2]) * G::BE + (cell[1] - 1 + by0 - bo[1])) * G::BE + (gx - bo[0]);
+#pragma unroll
+            for (int bb = 0; bb < NB; ++bb)
+#pragma unroll
+                for (int cc = 0; cc < S; ++cc) {
+                    const int idx = bb * S + cc, l = l0 + bb * G::BE + cc * G::BE * G::BE;
+                    add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
+                    add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
+                    add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
+                    add_fixed_shared(&SM.acc[3][l], a2[idx], C.sp);
+                }
+            return;
+        }
+        bool outside = false;
+        for (int bb = 0; bb < NB; ++bb)
+            for (int cc = 0; cc < S; ++cc) {
+                const int gy = cell[1] - 1 + by0 + bb, gz = cell[2] - 1 + cc;
+                if (gx < 0 || gx > C.W || gy < 0 || gy > C.H || gz < 0 || gz > C.Dp) { outside = true; continue; }
+                const int idx = bb * S + cc;
+                unsigned long long* p0 = acc + (((long long)gz * C.ny + gy) * C.nx + gx);
+                red_fixed(p0, am[idx], C.sm);
+                red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
+            }
+        if (outside) raise_flag(status, 4u);
+        if (gx >= 0 && gx <= C.W) {
+            const int y0 = max(0, cell[1] - 1 + by0), y1 = min(C.H, cell[1] - 2 + by0 + NB);
+            const int z0 = max(0, cell[2] - 1), z1 = min(C.Dp, cell[2] + (S - 2));
+            if (y0 <= y1 && z0 <= z1)
+                for (int bz = z0 / T; bz <= z1 / T; ++bz)
+                    for (int by = y0 / T; by <= y1 / T; ++by)
+                        mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
+        }
+    } else {
+        constexpr int NA = S / W::SPLIT;
+        const int gx0 = cell[0] - 1 + a * NA;
+        float am[NA * S], a0[NA * S], a1[NA * S];
+#pragma unroll
+        for (int k = 0; k < NA * S; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; }
+        for (int j = j0; j < j1; ++j) {
+            const float4* pp = pay + j * (G::PS / 4);
+            const float4 wx = pp[0], wy = pp[1], p2 = pp[2], p3 = pp[3];
+            const float a11 = payf[j * G::PS + 16];
+            // f = (p2.x, p2.y), m = p2.z, mv = (p2.w, p3.x), A = (p3.y p3.z | p3.w a11)
+            const float Xv[4] = {wx.x, wx.y, wx.z, wx.w};
+            const float Y[4] = {wy.x, wy.y, wy.z, wy.w};
+            float Yd[4];
+#pragma unroll
+            for (int b = 0; b < S; ++b) Yd[b] = Y[b] * (float(b - 1) - p2.y);
+#pragma unroll
+            for (int i = 0; i < NA; ++i) {
+                const int aa = a * NA + i;
+                const float X = NA == S ? Xv[i] : payf[j * G::PS + aa];
+                const float Xd = X * (float(aa - 1) - p2.x);
+                const float e0 = p2.w * X + p3.y * Xd, e1 = p3.x * X + p3.w * Xd;
+                const float f0 = p3.z * X, f1 = a11 * X, mX = p2.z * X;
+#pragma unroll
+                for (int b = 0; b < S; ++b) {
+                    const int idx = i * S + b;
+                    am[idx] += mX * Y[b];
+                    a0[idx] += e0 * Y[b] + f0 * Yd[b];
+                    a1[idx] += e1 * Y[b] + f1 * Yd[b];
+                }
+            }
+        }
+        float mx_m = 0.f, mx_p = 0.f;
+#pragma unroll
+        for (int k = 0; k < NA * S; ++k) {
+            mx_m = fmaxf(mx_m, fabsf(am[k]));
+            mx_p = fmaxf(mx_p, fmaxf(fabsf(a0[k]), fabsf(a1[k])));
+        }
+        if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
+            raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
+        if (in_box && in_grid) {
+            const int l0 = (cell[1] - 1 - bo[1]) * G::BE + (gx0 - bo[0]);
+#pragma unroll
+            for (int i = 0; i < NA; ++i)
+#pragma unroll
+                for (int b = 0; b < S; ++b) {
+                    const int idx = i * S + b, l = l0 + i + b * G::BE;
+                    add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
+                    add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
+                    add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
+                }
+            return;
+        }
+        bool outside = false;
+        for (int i = 0; i < NA; ++i)
+            for (int b = 0; b < S; ++b) {
+                const int gx = gx0 + i, gy = cell[1] - 1 + b;
+                if (gx < 0 || gx > C.W || gy < 0 || gy > C.H) { outside = true; continue; }
+                const int idx = i * S + b;
+                unsigned long long* p0 = acc + ((long long)gy * C.nx + gx);
+                red_fixed(p0, am[idx], C.sm);
+                red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+            }
+        if (outside) raise_flag(status, 4u);
+        const int x0 = max(0, gx0), x1 = min(C.W, gx0 + (NA - 1));
+        const int y0 = max(0, cell[1] - 1), y1 = min(C.H, cell[1] + (S - 2));
+        if (x0 <= x1 && y0 <= y1)
+            for (int by = y0 / T; by <= y1 / T; ++by)
+                for (int bx = x0 / T; bx <= x1 / T; ++bx) mark_block_once(TI, by * TI.nblk[0] + bx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One particle's P2G contribution to one stencil node, added on its own (no
+// grouping): the path of queued particles, shared by k_p2g_lone and the
+// prologue so both give the same int64 values.
+template <int D, int S>
+__device__ __forceinline__ void lone_node(const StepConsts& C, const TileInfo& TI, const float* x, const float* mv,
+                                          const float* A, float mass, int node, unsigned long long* __restrict__ acc,
+                                          unsigned* __restrict__ status) {
+    using St = Stencil<S>;
+    constexpr int T = TileGeom<D>::T;
+    const int ext[3] = {C.W, C.H, C.Dp};
+    int g[3] = {0, 0, 0};
+    float w = 1.f, d[3] = {0.f, 0.f, 0.f};
+    int rem = node;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int o = rem % S;
+        rem /= S;
+        const int base = St::base(x[k], ext[k]);
+        float wt[S];
+        St::weights(x[k], base, wt);
+        w *= pick<S>(wt, o);
+        g[k] = base + o;
+        d[k] = float(g[k]) - x[k];
+    }
+    if (g[0] < 0 || g[0] > C.W || g[1] < 0 || g[1] > C.H || (D == 3 && (g[2] < 0 || g[2] > C.Dp))) {
+        raise_flag(status, 4u);
+        return;
+    }
+    const long long id = ((long long)g[2] * C.ny + g[1]) * C.nx + g[0];
+    red_add(&acc[id], to_fixed(w * mass, C.sm, status));
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+        float s = mv[r];
+#pragma unroll
+        for (int k = 0; k < D; ++k) s += A[r * D + k] * d[k];
+        red_add(&acc[(1 + r) * C.nodes + id], to_fixed(w * s, C.sp, status));
+    }
+    const int b = D == 3 ? ((g[2] / T) * TI.nblk[1] + g[1] / T) * TI.nblk[0] + g[0] / T : (g[1] / T) * TI.nblk[0] + g[0] / T;
+    mark_block_once(TI, b);
+}
+
+// P2G of the queued particles after their return map: (particle, node) per
+// thread; x, v, A as the G2P and return-map kernels left them.
+template <int D, int S>
+__global__ void __launch_bounds__(256) k_p2g_lone(Particles P, StepConsts C, TileInfo TI, SlowQueue Q,
+                                                  unsigned long long* __restrict__ acc, unsigned* __restrict__ status) {
+    constexpr int NN = D == 3 ? S * S * S : S * S;
+    constexpr int PER = 256 / NN;
+    const int m = *Q.count;
+    const int node = threadIdx.x % NN, sub = threadIdx.x / NN;
+    if (sub >= PER) return;
+    const int n = P.n;
+    for (int e = blockIdx.x * PER + sub; e < m; e += gridDim.x * PER) {
+        const int i = Q.slot[e];
+        const float mass = P.mass ? P.mass[i] : P.mass_u;
+        const float vol = P.vol ? P.vol[i] : P.vol_u;
+        if (vol == 0.f) continue;
+        float x[D], mv[D], A[D * D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; mv[k] = mass * P.v[k * n + i]; }
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
+        lone_node<D, S>(C, TI, x, mv, A, mass, node, acc, status);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The fused kernel. G2P = true: one step (G2P of the state, then the next
+// step's P2G into `acc`). G2P = false: the P2G of the stored state only (the
+// prologue after creation, a state upload or a checkpoint load), reading B,
+// F_E, J_p and forming A as every other path does (mls_affine).
+template <int D, int S, bool G2P>
+__global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
+    k_g2p2g(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
+            SlowQueue Q, unsigned char* __restrict__ lone, unsigned* __restrict__ status) {
+    using G = FusedGeom<D>;
+    using W = WarpGeom<D, S>;
+    using St = Stencil<S>;
+    constexpr int T = G::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FusedSmem<D>& SM = *reinterpret_cast<FusedSmem<D>*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int n = P.n;
+    const int ntl = *TI.n_tile_list;
+    const long long gsy = C.nx, gsz = (long long)C.nx * C.ny;
+    for (;;) {
+        if (tid == 0) SM.tile = atomicAdd(TI.fused_next, 1);
+        __syncthreads();
+        const int e = SM.tile;
+        if (e >= ntl) break;
+        const int t = TI.tile_list[e];
+        const int start = TI.tile_start[t], m = TI.tile_len[e];
+        int tc[3] = {0, 0, 0}, bo[3] = {0, 0, 0};  // tile coordinates, box origin node
+        {
+            int r = t;
+#pragma unroll
+            for (int k = 0; k < D; ++k) { tc[k] = r % TI.tiles[k]; r /= TI.tiles[k]; bo[k] = tc[k] * T - 2; }
+        }
+        // stage the box: node velocities (G2P), zero sums
+        for (int l = tid; l < G::BN; l += G::THREADS) {
+            if constexpr (G2P) {
+                const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
+                const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (gx >= 0 && gx <= C.W && gy >= 0 && gy <= C.H && (D == 2 || (gz >= 0 && gz <= C.Dp)))
+                    v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
+                SM.box[l] = v;
+            }
+#pragma unroll
+            for (int c = 0; c < G::NCH; ++c) SM.acc[c][l] = 0ull;
+        }
+        if (tid == 0) SM.bmask = 0u;
+        __syncthreads();
+        for (int c0 = 0; c0 < m; c0 += G::CHUNK) {
+            const int cnt = min(G::CHUNK, m - c0);
+            const bool valid = tid < cnt;
+            const int i = start + c0 + tid;
+            unsigned long long key = kNoStencil;
+            float* q = reinterpret_cast<float*>(SM.pay) + tid * G::PS;
+            if (valid) {
+                const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
+                float x[D], v[D], A[D * D];
+                bool scatter = vol != 0.f;  // p2g.glsl:42
+                if constexpr (G2P) {
+                    float xo[D];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) xo[k] = P.x[k * n + i];
+                    int base[3] = {0, 0, 0};
+                    float wk[3][S], off[3][S];
+                    bool interior = true, boxed = true;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) {
+                        const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                        base[k] = St::base(xo[k], ext);
+                        interior = interior && base[k] >= 0 && base[k] + (S - 1) <= ext;
+                        boxed = boxed && base[k] - bo[k] >= 0 && base[k] + (S - 1) - bo[k] <= G::BE - 1;
+                        St::weights(xo[k], base[k], wk[k]);
+#pragma unroll
+                        for (int o = 0; o < S; ++o) off[k][o] = float(base[k] + o) - xo[k];
+                    }
+                    if (!interior) {
+                        // stencil partly outside the grid: the general kernel does the whole G2P
+                        const int slot = queue_slot(Q);
+                        Q.list[slot] = -1 - i;
+                        Q.slot[slot] = i;
+                        scatter = false;
+                    } else {
+                        float nv[D], nx[D], nB[D * D];
+                        const long long gc0 = (D == 3 ? base[2] * gsz : 0) + base[1] * gsy + base[0];
+                        if (boxed) {
+                            const int l0 = (D == 3 ? (base[2] - bo[2]) * G::BE * G::BE : 0) + (base[1] - bo[1]) * G::BE +
+                                           (base[0] - bo[0]);
+                            gather_nodes<D, S, true, int>(C, SM.box, l0, G::BE, G::BE * G::BE, gv, gc0, gsy, gsz, wk, off,
+                                                          nv, nB, nx);
+                        } else {
+                            gather_nodes<D, S, false, long long>(C, gv, gc0, gsy, gsz, gv, gc0, gsy, gsz, wk, off, nv, nB,
+                                                                 nx);
+                        }
+                        bool finite = true;
+#pragma unroll
+                        for (int k = 0; k < D; ++k) {
+                            x[k] = xo[k] + nx[k];
+                            v[k] = nv[k];
+                            P.v[k * n + i] = nv[k];
+                            P.x[k * n + i] = x[k];
+                            finite = finite && isfinite(x[k]);
+                        }
+                        if (!finite) raise_flag(status, 1u);
+#pragma unroll
+                        for (int k = 0; k < D * D; ++k) P.B[k * n + i] = nB[k];
+                        float Fe[D * D], Fh[D * D];
+#pragma unroll
+                        for (int k = 0; k < D * D; ++k) Fe[k] = P.Fe[k * n + i];
+#pragma unroll
+                        for (int r = 0; r < D; ++r)
+#pragma unroll
+                            for (int c = 0; c < D; ++c) {
+                                float s = Fe[r * D + c];
+#pragma unroll
+                                for (int k = 0; k < D; ++k) s += (C.dt * St::DINV * nB[r * D + k]) * Fe[k * D + c];
+                                Fh[r * D + c] = s;
+                            }
+                        float sig[D * D];
+                        const float Jp = P.Jp[i];
+                        if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s) &&
+                            hardened_stress_series<D>(Fh, Jp, C.mu0, C.la0, C.xi, sig)) {
+#pragma unroll
+                            for (int k = 0; k < D * D; ++k) {
+                                P.Fe[k * n + i] = Fh[k];
+                                A[k] = St::DINV * mass * nB[k] - St::DINV * C.dt * vol * sig[k];
+                            }
+                        } else {
+                            const int slot = queue_slot(Q);
+                            Q.list[slot] = i;
+                            Q.slot[slot] = i;
+#pragma unroll
+                            for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
+                            scatter = false;
+                        }
+                    }
+                    lone[i] = scatter || vol == 0.f ? 0 : kLoneScatter;
+                } else {
+                    float B[D * D], Fe[D * D];
+#pragma unroll
+                    for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
+#pragma unroll
+                    for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
+                    mls_affine<D, S>(C, B, Fe, P.Jp[i], mass, vol, A);
+                    if (scatter && lone && lone[i] == kLoneScatter) {
+                        // scattered one by one at the step that produced this state
+                        float mv[D];
+#pragma unroll
+                        for (int k = 0; k < D; ++k) mv[k] = mass * v[k];
+                        constexpr int NN = D == 3 ? S * S * S : S * S;
+                        for (int nd = 0; nd < NN; ++nd) lone_node<D, S>(C, TI, x, mv, A, mass, nd, acc, status);
+                        scatter = false;
+                    }
+                }
+                if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
+            }
+            reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
+            __syncthreads();
+            // runs: maximal stretches of consecutive slots with one stencil key
+            const unsigned long long* keyp = reinterpret_cast<const unsigned long long*>(
+                reinterpret_cast<const float*>(SM.pay) + G::KEYF);
+            auto key_at = [&](int j) { return keyp[j * (G::PS / 2)]; };
+            const bool is_start = valid && (tid == 0 || key_at(tid) != key_at(tid - 1));
+            const unsigned ballot = __ballot_sync(0xffffffffu, is_start);
+            if (lane == 0) SM.starts[wid] = ballot;
+            __syncthreads();
+            int nruns = 0, before = 0;
+#pragma unroll
+            for (int w = 0; w < G::CHUNK / 32; ++w) {
+                const int c = __popc(SM.starts[w]);
+                before += w < wid ? c : 0;
+                nruns += c;
+            }
+            if (is_start) SM.run[before + __popc(ballot & ((1u << lane) - 1))] = tid;
+            if (tid == 0) SM.run[nruns] = cnt;
+            __syncthreads();
+            for (int u = tid; u < nruns * W::SPLIT; u += G::THREADS) {
+                const int r = u / W::SPLIT, a = u % W::SPLIT;
+                const int j0 = SM.run[r], j1 = SM.run[r + 1];
+                const unsigned long long kk = key_at(j0);
+                if (kk == kNoStencil) continue;
+                fused_run<D, S>(C, TI, SM, bo, j0, j1, kk, a, acc, status);
+            }
+            __syncthreads();
+        }
+        // the box's sums into the global grid, once per node; mark node blocks
+        unsigned bits = 0u;
+        for (int l = tid; l < G::BN; l += G::THREADS) {
+            unsigned long long v[G::NCH];
+            bool any = false;
+#pragma unroll
+            for (int c = 0; c < G::NCH; ++c) { v[c] = SM.acc[c][l]; any = any || v[c] != 0ull; }
+            if (!any) continue;
+            const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
+            const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
+            // only runs wholly inside the grid add to the box: gx, gy, gz are in range
+            const long long gid = gz * gsz + gy * gsy + gx;
+#pragma unroll
+            for (int c = 0; c < G::NCH; ++c)
+                if (v[c] != 0ull) atomicAdd(&acc[c * C.nodes + gid], v[c]);
+            const int rx = gx / T - tc[0] + 1, ry = gy / T - tc[1] + 1, rz = D == 3 ? gz / T - tc[2] + 1 : 0;
+            bits |= 1u << ((rz * 3 + ry) * 3 + rx);
+        }
+        bits = __reduce_or_sync(0xffffffffu, bits);
+        if (lane == 0 && bits) atomicOr(&SM.bmask, bits);
+        __syncthreads();
+        constexpr int NBLK = D == 3 ? 27 : 9;
+        if (tid < NBLK && (SM.bmask >> tid) & 1u) {
+            const int rx = tid % 3, ry = (tid / 3) % 3, rz = tid / 9;
+            const int bx = tc[0] - 1 + rx, by = tc[1] - 1 + ry, bz = D == 3 ? tc[2] - 1 + rz : 0;
+            mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
+        }
+    }
+}
+
+}  // namespace mpm

@@ -613,6 +613,7 @@ struct SlowQueue {
     int* list;    // slots needing the full return map
     int* count;   // device scalar
     float* fh;    // trial F per queue entry, [D*D][capacity]
+    int* slot;    // fused path: the particle slot of each entry (kept when the entry is marked done)
     int capacity;
 };
 

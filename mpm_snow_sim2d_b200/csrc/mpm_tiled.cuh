@@ -38,6 +38,8 @@ struct TileInfo {
     int* tile_list;    // non-empty tiles of the last sort
     int* n_tile_list;  // device scalar
     int* p2g_next;     // device scalar: next P2G chunk to hand out (zeroed before each P2G)
+    int* tile_len;     // per entry of tile_list: particles of that tile at the last sort
+    int* fused_next;   // device scalar: next tile of the fused transfer (zeroed before each launch)
     unsigned long long* skey;  // global sort scratch (tiles above SortGeom<D>::SMEM particles)
     int* sval;
 };
@@ -289,7 +291,7 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
             for (int k = 0; k < D * D; ++k) {
                 dst.B[k * n + s] = P.B[k * n + src];
                 dst.Fe[k * n + s] = P.Fe[k * n + src];
-                dst.A[k * n + s] = P.A[k * n + src];
+                if (dst.A) dst.A[k * n + s] = P.A[k * n + src];
             }
             dst.Jp[s] = P.Jp[src];
             dst.id[s] = id_src[src];
@@ -297,7 +299,10 @@ __global__ void __launch_bounds__(256) k_tile_sort(Particles P, const int* __res
             if (P.vol) dst.vol[s] = P.vol[src];
         }
         __syncthreads();
-        if (threadIdx.x == 0) TI.tile_count[t] = 0;
+        if (threadIdx.x == 0) {
+            TI.tile_len[e] = m;
+            TI.tile_count[t] = 0;
+        }
         __syncthreads();
     }
 }
