@@ -41,17 +41,44 @@ def impact_scene(speed: float, seed: int, W: int = 64, steps: int = 200):
     return scenes._scene(f"impact_v{speed:.2f}", 3, W, 5e-5, steps, pos, vel, 8, dict(seed=seed))
 
 
+def collision_scene(speed: float, seed: int, W: int = 256, steps: int = 1000):
+    """Two snowballs of radius U(0.12, 0.16) thrown at each other at relative
+    speed `speed` m/s along a random direction near the x axis, a few cells
+    apart at the start (the two-snowball workload's set-up with other sizes,
+    speeds and seeds)."""
+    dx = 1.0 / W
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r = rng.uniform(0.12, 0.16)
+    gap = rng.uniform(2.0, 6.0) * dx
+    th, ph = rng.uniform(-0.3, 0.3), rng.uniform(-0.3, 0.3)
+    u = np.array([np.cos(th) * np.cos(ph), np.sin(th), np.cos(th) * np.sin(ph)])
+    c = np.array([0.5, rng.uniform(0.4, 0.6), 0.5])
+    ca, cb = c - u * (r + gap / 2), c + u * (r + gap / 2)
+    a = scenes._ball(rng, tuple(ca), r, 8, dx)
+    b = scenes._ball(rng, tuple(cb), r, 8, dx)
+    pos = np.concatenate([a, b])
+    vel = np.zeros_like(pos)
+    vel[: a.shape[0]] = u * speed / 2
+    vel[a.shape[0]:] = -u * speed / 2
+    return scenes._scene(f"collide_v{speed:.2f}", 3, W, 5e-5, steps, pos, vel, 8, dict(seed=seed))
+
+
 def collect_pairs(n_pairs: int, seed: int = 7, W: int = 64, steps: int = 1000, per_scene: int = 1_000_000,
-                  every: int = 10, verbose: bool = True) -> np.ndarray:
-    """Exact return-map pairs from seeded impacts, spread over each whole run:
-    the log holds every out-of-band particle of `every` steps, and each read
-    keeps a uniform random subset of per_scene / (steps / every) rows."""
+                  every: int = 10, verbose: bool = True, kind: str = "impact") -> np.ndarray:
+    """Exact return-map pairs from seeded impacts (kind "impact": snowball on
+    slab) or collisions (kind "collision": two snowballs), spread over each
+    whole run: the log holds every out-of-band particle of `every` steps, and
+    each read keeps a uniform random subset of per_scene / (steps / every)
+    rows."""
     rng = np.random.Generator(np.random.PCG64(seed))
     chunks, total, k = [], 0, 0
     reads = max(1, steps // every)
     while total < n_pairs:
         speed = float(rng.uniform(1.0, 8.0))
-        sc = impact_scene(speed, seed * 1000 + k, W=W, steps=steps)
+        if kind == "collision":
+            sc = collision_scene(speed, seed * 1000 + k, W=W, steps=steps)
+        else:
+            sc = impact_scene(speed, seed * 1000 + k, W=W, steps=steps)
         keep = max(1, min(per_scene, n_pairs - total) // reads)
         log_cap = every * sc.count
         taken = []
@@ -153,6 +180,9 @@ def main(argv=None) -> int:
     ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
     ap.add_argument("--save-pairs", default=None, help="also write the collected pairs as shards to this directory")
     ap.add_argument("--load-pairs", default=None, help="train on the shards in this directory instead of collecting")
+    ap.add_argument("--collision-pairs", type=int, default=0,
+                    help="pairs from colliding-snowball runs (256^3) collected in addition to the impacts")
+    ap.add_argument("--collision-grid", type=int, default=256)
     args = ap.parse_args(argv)
     _lib.load()
     t0 = time.perf_counter()
@@ -161,6 +191,10 @@ def main(argv=None) -> int:
         print(f"loaded {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
     else:
         pairs = collect_pairs(args.pairs, seed=args.seed)
+        if args.collision_pairs > 0:
+            coll = collect_pairs(args.collision_pairs, seed=args.seed + 1000, W=args.collision_grid,
+                                 kind="collision", per_scene=5_000_000)
+            pairs = np.concatenate([pairs, coll])
         print(f"collected {pairs.shape[0]} pairs in {time.perf_counter() - t0:.1f} s")
         if args.save_pairs:
             save_pair_shards(pairs, args.save_pairs)

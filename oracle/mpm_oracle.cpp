@@ -614,6 +614,14 @@ int orc_step_f64(const orc_params* q, int64_t n, double* x, double* v, double* B
     return step_impl<double>(q, n, x, v, B, Fe, Fp, mass, vol, nsteps, 1);
 }
 
+// FP64 on `threads` OpenMP threads (P2G adds with atomics, in no fixed order:
+// the sums agree with the single-threaded run to FP64 rounding). For the
+// workload-size parity runs.
+int orc_step_f64_mt(const orc_params* q, int64_t n, double* x, double* v, double* B, double* Fe, double* Fp,
+                    const double* mass, const double* vol, int32_t nsteps, int32_t threads) {
+    return step_impl<double>(q, n, x, v, B, Fe, Fp, mass, vol, nsteps, threads);
+}
+
 int orc_step_f32(const orc_params* q, int64_t n, float* x, float* v, float* B, float* Fe, float* Fp,
                  const float* mass, const float* vol, int32_t nsteps, int32_t threads) {
     return step_impl<float>(q, n, x, v, B, Fe, Fp, mass, vol, nsteps, threads);

@@ -51,6 +51,7 @@ def lib():
         dp, fp = C.POINTER(C.c_double), C.POINTER(C.c_float)
         L.orc_step_f64.argtypes = [C.POINTER(OrcParams), C.c_int64] + [dp] * 7 + [C.c_int32]
         L.orc_step_f32.argtypes = [C.POINTER(OrcParams), C.c_int64] + [fp] * 7 + [C.c_int32, C.c_int32]
+        L.orc_step_f64_mt.argtypes = [C.POINTER(OrcParams), C.c_int64] + [dp] * 7 + [C.c_int32, C.c_int32]
         L.orc_bspline_f64.argtypes = [C.c_double, dp, dp]
         L.orc_svd_f64.argtypes = [C.c_int32, C.c_int32, dp, dp, dp, dp]
         L.orc_svd_f64.restype = None
@@ -127,7 +128,8 @@ def run_oracle(scene, state: OracleState, nsteps: int, *, formulation=None, boun
         ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
         arrs = [state.position, state.velocity, state.affine_b, state.elastic_f, state.plastic_f, state.mass, state.volume]
         assert all(a.dtype == np.float64 and a.flags.c_contiguous for a in arrs)
-        rc = L.orc_step_f64(C.byref(p), n, *map(ptr, arrs), nsteps)
+        rc = (L.orc_step_f64(C.byref(p), n, *map(ptr, arrs), nsteps) if threads <= 1
+              else L.orc_step_f64_mt(C.byref(p), n, *map(ptr, arrs), nsteps, threads))
     if rc != 0:
         raise RuntimeError(f"oracle step failed with code {rc}")
     return state
