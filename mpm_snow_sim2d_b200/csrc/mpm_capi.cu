@@ -77,6 +77,7 @@ struct mpm_solver {
     int cur_K = 16;              // steps of the current period (auto)
     long long next_sort = 0;     // step of the next sort (auto)
     long long sorts_done = 0;    // sorts launched so far
+    long long sorted_at = -1;    // step at whose start the last sort ran (no second sort at that step)
     unsigned* vmax_dev = nullptr;   // two slots: largest |v| component over the particles (float bits)
     unsigned* vmax_host = nullptr;  // pinned copies
     cudaEvent_t vmax_event[2] = {nullptr, nullptr};
@@ -111,8 +112,8 @@ struct mpm_solver {
     // P2G-only prologue).
     bool fused = false;
     bool acc_pending = false;
-    unsigned char* lone = nullptr;  // per slot: scattered one by one at the last fused step
     int fused_grid = 0;
+    bool fused_sacc = true;         // run sums through a shared-memory node box (else straight to the grid)
 };
 
 namespace {
@@ -190,7 +191,6 @@ void release(mpm_solver* s) {
     if (s->q.slot) cudaFree(s->q.slot);
     if (s->ti.tile_len) cudaFree(s->ti.tile_len);
     if (s->ti.fused_next) cudaFree(s->ti.fused_next);
-    if (s->lone) cudaFree(s->lone);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -263,6 +263,7 @@ template <int D, int S> cudaError_t launch_sort(mpm_solver* s) {
     swap_buffers(s);
     s->needs_sort = false;
     s->next_sort = s->step + s->cur_K;
+    s->sorted_at = s->step;
     ++s->sorts_done;
     return cudaSuccess;
 }
@@ -272,7 +273,7 @@ template <int D, int S> cudaError_t launch_sort(mpm_solver* s) {
 bool sort_due(const mpm_solver* s) {
     if (s->needs_sort) return true;
     if (s->auto_sort) return s->step >= s->next_sort;
-    return s->sort_period > 0 && s->step % s->sort_period == 0;
+    return s->sort_period > 0 && s->step % s->sort_period == 0 && s->sorted_at != s->step;
 }
 
 // Auto sort period. A period of K steps costs one sort and lets particles
@@ -420,8 +421,12 @@ template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
     if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
     if (s->n == 0) return cudaSuccess;
-    k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
-        particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->lone, s->status);
+    if (s->fused_sacc)
+        k_g2p2g<D, S, G2P, true><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, true>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
+    else
+        k_g2p2g<D, S, G2P, false><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, false>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
     return cudaGetLastError();
 }
 
@@ -576,28 +581,44 @@ mpm_status setup_tiled(mpm_solver* s) {
     s->q.capacity = n > 0 ? n : 1;
     if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 1) ||
         dalloc(&s->q.fh, (size_t)s->q.capacity * D * D) || dalloc(&s->q.slot, (size_t)s->q.capacity) ||
-        dalloc(&ti.tile_len, (size_t)ti.n_tiles) || dalloc(&ti.fused_next, 1) || dalloc(&s->lone, (size_t)n)) {
+        dalloc(&ti.tile_len, (size_t)ti.n_tiles) || dalloc(&ti.fused_next, 1)) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
     }
-    if (cudaMemset(s->lone, 0, (size_t)(n > 0 ? n : 1)) != cudaSuccess) return MPM_ERR_CUDA;
     {
         // MPM_TRANSFER=split selects the separate P2G / G2P kernels (for comparison)
         const char* tr = std::getenv("MPM_TRANSFER");
         s->fused = !(tr && std::strcmp(tr, "split") == 0);
     }
     if (s->fused) {
+        {
+            const char* sa = std::getenv("MPM_FUSED_SACC");
+            if (sa) s->fused_sacc = std::strcmp(sa, "0") != 0;
+        }
         const void* kfn;
         size_t fsm;
         const void* kpro;
+        const bool sacc = s->fused_sacc;
         if (D == 3) {
-            kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
-            kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false> : (const void*)k_g2p2g<3, 4, false>;
-            fsm = sizeof(FusedSmem<3>);
+            if (sacc) {
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, true> : (const void*)k_g2p2g<3, 4, true, true>;
+                kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false, true> : (const void*)k_g2p2g<3, 4, false, true>;
+            } else {
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, false> : (const void*)k_g2p2g<3, 4, true, false>;
+                kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false, false>
+                                       : (const void*)k_g2p2g<3, 4, false, false>;
+            }
+            fsm = sacc ? sizeof(FusedSmem<3, true>) : sizeof(FusedSmem<3, false>);
         } else {
-            kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
-            kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false> : (const void*)k_g2p2g<2, 4, false>;
-            fsm = sizeof(FusedSmem<2>);
+            if (sacc) {
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, true> : (const void*)k_g2p2g<2, 4, true, true>;
+                kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false, true> : (const void*)k_g2p2g<2, 4, false, true>;
+            } else {
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, false> : (const void*)k_g2p2g<2, 4, true, false>;
+                kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false, false>
+                                       : (const void*)k_g2p2g<2, 4, false, false>;
+            }
+            fsm = sacc ? sizeof(FusedSmem<2, true>) : sizeof(FusedSmem<2, false>);
         }
         int per = 0;
         cudaError_t ef = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
@@ -756,7 +777,7 @@ int run_period_graph(mpm_solver* s) {
             return 0;
         }
         cudaStream_t saved = s->stream;
-        const long long step0 = s->step, next0 = s->next_sort, sorts0 = s->sorts_done;
+        const long long step0 = s->step, next0 = s->next_sort, sorts0 = s->sorts_done, sorted0 = s->sorted_at;
         const bool ns = s->needs_sort;
         s->stream = cap;
         cudaGraph_t g = nullptr;
@@ -775,6 +796,7 @@ int run_period_graph(mpm_solver* s) {
         s->step = step0;
         s->next_sort = next0;
         s->sorts_done = sorts0;
+        s->sorted_at = sorted0;
         s->needs_sort = ns;
         if (s->parity != par) swap_buffers(s);
         if (e == cudaSuccess) e = cudaGraphInstantiate(&slot, g, 0);
@@ -792,6 +814,7 @@ int run_period_graph(mpm_solver* s) {
     swap_buffers(s);
     s->needs_sort = false;
     s->next_sort = s->step + K;  // the period's sort ran at its first step
+    s->sorted_at = s->step;
     ++s->sorts_done;
     s->step += K;
     return 1;
@@ -1050,9 +1073,9 @@ mpm_status mpm_set_state(mpm_solver* s, const mpm_state_host* st) {
     if (st->plastic_det && (r = import_field(s, s->Jp, 1, st->plastic_det)) != MPM_OK) return r;
     if (s->fused) {
         // the pending grid sums belong to the old state; the next step starts
-        // with the P2G-only prologue, every particle grouped
+        // with the P2G-only prologue
         if (s->acc_pending) MPM_CUDA(s, clear_after_p2g(s));
-        MPM_CUDA(s, cudaMemsetAsync(s->lone, 0, (size_t)(s->n > 0 ? s->n : 1), s->stream));
+        MPM_CUDA(s, cudaStreamSynchronize(s->stream));
     }
     s->needs_sort = true;
     s->needs_affine = true;
@@ -1135,20 +1158,23 @@ mpm_status mpm_get_fixed_point(const mpm_solver* s, int32_t* lm, int32_t* lp) {
 
 constexpr int kSchedTag = 0x4B504552;  // extra record: auto sort schedule
 constexpr int kTileTag = 0x454C4954;   // extra record: {tag, tile, first slot, particles} of the last sort
-constexpr int kLoneTag = 0x454E4F4C;   // extra record: {tag, 64-slot word, bits 0-31, bits 32-63} of lone flags
 
-// Checkpoint: "MPMS" | u32 version=2 | i32 dim | i64 count | i32 W, H, D |
+// Checkpoint: "MPMS" | u32 version=3 | i32 dim | i64 count | i32 W, H, D |
 // u64 params hash | i64 step | f32 x[n*d] v[n*d] B[n*d*d] Fe[n*d*d] Jp[n]
 // (creation order) | u32 has_order | [i32 slot_id[n] | i32 n_extra |
-// i32x4 extra[n_extra]]. The slot order of the tiled path is saved so that a
-// resumed run groups particles exactly as the original did and continues
-// bit-identically. `extra` holds tagged records: with the auto sort period,
-// one {kSchedTag, period, steps to the next sort, next two periods (8 bits
-// each; 0: measure)}; on the fused path one {kTileTag, tile, first slot,
-// count} per non-empty tile of the last sort (the particles' tiles at that
-// sort cannot be recomputed from their current positions) and {kLoneTag,
-// word, low bits, high bits} for each 64 slots holding particles the last step
-// scattered one by one; unknown records are skipped on load.
+// i32x4 extra[n_extra]] | u32 has_sums | [i32 channels | i32 nodes per block
+// | i32 nblocks | i32 block[nblocks] | i64 sums[nblocks][channels][nodes]].
+// The slot order of the tiled path is saved so that a resumed run groups
+// particles exactly as the original did and continues bit-identically.
+// `extra` holds tagged records: with the auto sort period, one {kSchedTag,
+// period, steps to the next sort, next two periods (8 bits each; 0:
+// measure)}; on the fused path one {kTileTag, tile, first slot, count} per
+// non-empty tile of the last sort (the particles' tiles at that sort cannot
+// be recomputed from their current positions); unknown records are skipped on
+// load. On the fused path the grid already holds the next step's P2G sums;
+// `sums` keeps them (the node blocks marked for the grid update), so a resumed
+// run continues from the very same integers. Version 2 files (no sums
+// section) load as well.
 mpm_status mpm_save_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
     const int D = s->dim;
@@ -1180,21 +1206,37 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
         }
         MPM_CUDA(s, cudaMemcpy(tstart.data(), s->ti.tile_start, sizeof(int) * s->ti.n_tiles, cudaMemcpyDeviceToHost));
         for (int e = 0; e < ntl; ++e) extra.push_back(make_int4(kTileTag, tl[e], tstart[tl[e]], tlen[e]));
-        if (s->acc_pending) {
-            std::vector<unsigned char> lone(n);
-            MPM_CUDA(s, cudaMemcpy(lone.data(), s->lone, n, cudaMemcpyDeviceToHost));
-            for (size_t w = 0; w * 64 < n; ++w) {
-                unsigned lo = 0, hi = 0;
-                for (size_t b = 0; b < 64 && w * 64 + b < n; ++b)
-                    if (lone[w * 64 + b]) (b < 32 ? lo : hi) |= 1u << (b & 31);
-                if (lo | hi) extra.push_back(make_int4(kLoneTag, (int)w, (int)lo, (int)hi));
-            }
+    }
+    // the pending grid sums of the fused path, block by block
+    uint32_t has_sums = 0;
+    int32_t sum_hdr[3] = {nacc(D, s->form), D == 3 ? TileGeom<3>::BN : TileGeom<2>::BN, 0};
+    std::vector<int> sum_blocks;
+    std::vector<unsigned long long> sums;
+    if (has_order && s->fused && s->acc_pending) {
+        has_sums = 1;
+        MPM_CUDA(s, cudaMemcpy(&sum_hdr[2], s->ti.n_marked, sizeof(int), cudaMemcpyDeviceToHost));
+        const int nb = sum_hdr[2];
+        sum_blocks.resize(nb);
+        sums.resize((size_t)nb * sum_hdr[0] * sum_hdr[1]);
+        if (nb > 0) {
+            MPM_CUDA(s, cudaMemcpy(sum_blocks.data(), s->ti.mark_list, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+            mpm_status es = ensure_staging(s, sums.size() * 2);
+            if (es != MPM_OK) return es;
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(s->staging);
+            if (D == 3)
+                k_pack_marked<3><<<s->sms * 4, 256, 0, s->stream>>>(s->C, s->ti, sum_hdr[0], nb, s->acc, dst);
+            else
+                k_pack_marked<2><<<s->sms * 4, 256, 0, s->stream>>>(s->C, s->ti, sum_hdr[0], nb, s->acc, dst);
+            MPM_CUDA(s, cudaGetLastError());
+            MPM_CUDA(s, cudaMemcpyAsync(sums.data(), dst, sizeof(unsigned long long) * sums.size(),
+                                        cudaMemcpyDeviceToHost, s->stream));
+            MPM_CUDA(s, cudaStreamSynchronize(s->stream));
         }
     }
     const int32_t n_extra = (int32_t)extra.size();
     FILE* f = std::fopen(path, "wb");
     if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
-    const uint32_t ver = 2;
+    const uint32_t ver = 3;
     const int32_t dim = D, ext[3] = {s->params.width, s->params.height, D == 3 ? s->params.depth : 0};
     const int64_t count = (int64_t)n, step = s->step;
     const uint64_t h = params_hash(s->params);
@@ -1208,12 +1250,20 @@ mpm_status mpm_save_state(mpm_solver* s, const char* path) {
         ok = ok && std::fwrite(ids.data(), sizeof(int), n, f) == n && std::fwrite(&n_extra, 4, 1, f) == 1;
         if (n_extra) ok = ok && std::fwrite(extra.data(), sizeof(int4), extra.size(), f) == extra.size();
     }
+    ok = ok && std::fwrite(&has_sums, 4, 1, f) == 1;
+    if (has_sums) {
+        ok = ok && std::fwrite(sum_hdr, 4, 3, f) == 3 &&
+             std::fwrite(sum_blocks.data(), sizeof(int), sum_blocks.size(), f) == sum_blocks.size() &&
+             std::fwrite(sums.data(), sizeof(unsigned long long), sums.size(), f) == sums.size();
+    }
     ok = (std::fclose(f) == 0) && ok;
     return ok ? MPM_OK : fail(s, MPM_ERR_IO, "short write");
 }
 
 mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     if (!s || !path) return MPM_ERR_INVALID_ARGUMENT;
+    // the uploads below replace buffers that work already queued may still read
+    MPM_CUDA(s, cudaStreamSynchronize(s->stream));
     FILE* f = std::fopen(path, "rb");
     if (!f) return fail(s, MPM_ERR_IO, std::string("cannot open ") + path);
     char magic[4];
@@ -1224,7 +1274,7 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     bool ok = std::fread(magic, 1, 4, f) == 4 && std::fread(&ver, 4, 1, f) == 1 && std::fread(&dim, 4, 1, f) == 1 &&
               std::fread(&count, 8, 1, f) == 1 && std::fread(ext, 4, 3, f) == 3 && std::fread(&h, 8, 1, f) == 1 &&
               std::fread(&step, 8, 1, f) == 1;
-    if (!ok || std::memcmp(magic, "MPMS", 4) != 0 || (ver != 1 && ver != 2)) { std::fclose(f); return fail(s, MPM_ERR_IO, "not a checkpoint"); }
+    if (!ok || std::memcmp(magic, "MPMS", 4) != 0 || ver < 1 || ver > 3) { std::fclose(f); return fail(s, MPM_ERR_IO, "not a checkpoint"); }
     if (dim != s->dim || count != s->n || ext[0] != s->params.width || ext[1] != s->params.height ||
         (dim == 3 && ext[2] != s->params.depth) || h != params_hash(s->params)) {
         std::fclose(f);
@@ -1239,8 +1289,11 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
     int n_extra = 0;
     int sched_K = 0, sched_next = 0, sched_pending = 0;
     std::vector<int4> tiles;                 // {tile, first slot, count} of the last sort (fused path)
-    std::vector<unsigned char> lone_flags;   // per slot (fused path)
-    if (ok && ver == 2) {
+    uint32_t has_sums = 0;                   // the pending grid sums (fused path)
+    int32_t sum_hdr[3] = {0, 0, 0};
+    std::vector<int> sum_blocks;
+    std::vector<unsigned long long> sums;
+    if (ok && ver >= 2) {
         ok = std::fread(&has_order, 4, 1, f) == 1;
         if (ok && has_order) {
             ids.resize(n);
@@ -1258,11 +1311,6 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
                         sched_pending = extra[q].w;
                     } else if (extra[q].x == kTileTag) {
                         tiles.push_back(make_int4(extra[q].y, extra[q].z, extra[q].w, 0));
-                    } else if (extra[q].x == kLoneTag && extra[q].y >= 0 && (size_t)extra[q].y * 64 < n) {
-                        if (lone_flags.empty()) lone_flags.assign(n, 0);
-                        for (int b = 0; b < 64 && (size_t)extra[q].y * 64 + b < n; ++b)
-                            if (((unsigned)(b < 32 ? extra[q].z : extra[q].w) >> (b & 31)) & 1u)
-                                lone_flags[(size_t)extra[q].y * 64 + b] = kLoneScatter;
                     }
             }
             // every slot must name a distinct particle
@@ -1270,6 +1318,27 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
             for (size_t i = 0; ok && i < n; ++i) {
                 ok = ids[i] >= 0 && (size_t)ids[i] < n && !seen[ids[i]];
                 if (ok) seen[ids[i]] = 1;
+            }
+        }
+    }
+    if (ok && ver >= 3) {
+        ok = std::fread(&has_sums, 4, 1, f) == 1;
+        if (ok && has_sums) {
+            const int nb_max = s->ti.n_blocks;
+            ok = std::fread(sum_hdr, 4, 3, f) == 3 && sum_hdr[0] == nacc(s->dim, s->form) &&
+                 sum_hdr[1] == (s->dim == 3 ? TileGeom<3>::BN : TileGeom<2>::BN) && sum_hdr[2] >= 0 &&
+                 sum_hdr[2] <= nb_max;
+            if (ok) {
+                sum_blocks.resize(sum_hdr[2]);
+                sums.resize((size_t)sum_hdr[2] * sum_hdr[0] * sum_hdr[1]);
+                ok = std::fread(sum_blocks.data(), sizeof(int), sum_blocks.size(), f) == sum_blocks.size() &&
+                     std::fread(sums.data(), sizeof(unsigned long long), sums.size(), f) == sums.size();
+                // every block in range and listed once
+                std::vector<char> seenb(ok ? (size_t)nb_max : 0, 0);
+                for (size_t b = 0; ok && b < sum_blocks.size(); ++b) {
+                    ok = sum_blocks[b] >= 0 && sum_blocks[b] < nb_max && !seenb[sum_blocks[b]];
+                    if (ok) seenb[sum_blocks[b]] = 1;
+                }
             }
         }
     }
@@ -1302,12 +1371,37 @@ mpm_status mpm_load_state(mpm_solver* s, const char* path) {
             const int ntl = (int)tiles.size();
             std::vector<int> tl(ntl), tlen(ntl), tstart(s->ti.n_tiles, 0);
             for (int e = 0; e < ntl; ++e) { tl[e] = tiles[e].x; tlen[e] = tiles[e].z; tstart[tiles[e].x] = tiles[e].y; }
-            MPM_CUDA(s, cudaMemcpy(s->ti.tile_list, tl.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice));
-            MPM_CUDA(s, cudaMemcpy(s->ti.tile_len, tlen.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice));
-            MPM_CUDA(s, cudaMemcpy(s->ti.tile_start, tstart.data(), sizeof(int) * s->ti.n_tiles, cudaMemcpyHostToDevice));
-            MPM_CUDA(s, cudaMemcpy(s->ti.n_tile_list, &ntl, sizeof(int), cudaMemcpyHostToDevice));
-            if (!lone_flags.empty())
-                MPM_CUDA(s, cudaMemcpy(s->lone, lone_flags.data(), n, cudaMemcpyHostToDevice));
+            // on the solver's stream, after the clear of the flags that mpm_set_state queued there
+            cudaStream_t st = s->stream;
+            MPM_CUDA(s, cudaMemcpyAsync(s->ti.tile_list, tl.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice, st));
+            MPM_CUDA(s, cudaMemcpyAsync(s->ti.tile_len, tlen.data(), sizeof(int) * ntl, cudaMemcpyHostToDevice, st));
+            MPM_CUDA(s, cudaMemcpyAsync(s->ti.tile_start, tstart.data(), sizeof(int) * s->ti.n_tiles,
+                                        cudaMemcpyHostToDevice, st));
+            MPM_CUDA(s, cudaMemcpyAsync(s->ti.n_tile_list, &ntl, sizeof(int), cudaMemcpyHostToDevice, st));
+            if (has_sums) {
+                // the next step's grid sums as the saved run held them: into the
+                // (cleared) accumulators, their blocks marked for the grid update
+                const int nb = sum_hdr[2];
+                if (nb > 0) {
+                    const size_t words = sums.size() + ((size_t)nb + 1) / 2;
+                    mpm_status es = ensure_staging(s, words * 2);
+                    if (es != MPM_OK) return es;
+                    unsigned long long* din = reinterpret_cast<unsigned long long*>(s->staging);
+                    int* dblk = reinterpret_cast<int*>(din + sums.size());
+                    MPM_CUDA(s, cudaMemcpyAsync(din, sums.data(), sizeof(unsigned long long) * sums.size(),
+                                                cudaMemcpyHostToDevice, st));
+                    MPM_CUDA(s, cudaMemcpyAsync(dblk, sum_blocks.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+                    if (s->dim == 3)
+                        k_unpack_marked<3><<<s->sms * 4, 256, 0, st>>>(s->C, s->ti, sum_hdr[0], nb, dblk, din, s->acc);
+                    else
+                        k_unpack_marked<2><<<s->sms * 4, 256, 0, st>>>(s->C, s->ti, sum_hdr[0], nb, dblk, din, s->acc);
+                    MPM_CUDA(s, cudaGetLastError());
+                }
+                MPM_CUDA(s, cudaMemcpyAsync(s->ti.n_marked, &sum_hdr[2], sizeof(int), cudaMemcpyHostToDevice, st));
+                s->acc_pending = true;
+                s->needs_affine = false;
+            }
+            MPM_CUDA(s, cudaStreamSynchronize(st));
         } else {
             s->needs_sort = true;
         }

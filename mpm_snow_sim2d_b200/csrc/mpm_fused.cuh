@@ -27,10 +27,10 @@
 //
 // Determinism: every cross-run sum is an integer add, and the runs are a
 // function of the slot order, the chunk boundaries (fixed offsets inside a
-// tile) and which particles were queued -- all functions of the state. A
-// prologue pass of the same kernel (P2G only, reading the stored state)
-// reproduces the sums of a step boundary bit for bit when it is told which
-// particles were scattered one by one (the per-slot `lone` flags).
+// tile) and which particles were queued -- all functions of the state. After
+// creation or a state upload a P2G-only pass of the same kernel (reading the
+// stored state) forms the first sums. A checkpoint stores the pending sums
+// themselves, so a resumed run never recomputes them.
 #pragma once
 
 #include "mpm_tiled.cuh"
@@ -48,12 +48,16 @@ template <int D> struct FusedGeom {
     static constexpr int KEYF = PS - 2;                 // payload floats holding the 64-bit stencil key
 };
 
-template <int D> struct FusedSmem {
+// SACC: the run sums go to an int64 accumulator over the node box in shared
+// memory, added to the global grid once per node at the end of the tile;
+// otherwise each run adds its sums to the global grid directly (red.global).
+template <int D, bool SACC> struct FusedSmem {
     using G = FusedGeom<D>;
     float4 box[G::BN];                                  // 3D: (vf, wall flag); 2D: (vf, vc)
-    unsigned long long acc[G::NCH][G::BN];              // int64 fixed-point sums of the next step's P2G
+    unsigned long long acc[SACC ? G::NCH : 1][SACC ? G::BN : 1];  // int64 fixed-point sums of the next P2G
     float4 pay[G::CHUNK * G::PS / 4];
     int run[G::CHUNK + 1];                              // start slot of each run, then the chunk end
+    int order[G::CHUNK];                                // runs, longest first
     unsigned starts[G::CHUNK / 32];                     // run-start ballot per warp
     int tile;
     unsigned bmask;                                     // node blocks (3^D around the tile) that received sums
@@ -62,11 +66,6 @@ template <int D> struct FusedSmem {
 #ifndef MPM_FUSED_MIN_BLOCKS
 #define MPM_FUSED_MIN_BLOCKS 3
 #endif
-
-// Per-slot flag of the last fused step: the particle was scattered one by one
-// (queued for the full return map); the P2G-only prologue scatters it the same
-// way so that resumed runs continue bit-identically.
-constexpr unsigned char kLoneScatter = 1;
 
 // ---------------------------------------------------------------------------
 // Interior gather from a node array with strides (sy, sz): the box in shared
@@ -227,14 +226,17 @@ __device__ __forceinline__ void add_fixed_shared(unsigned long long* p, float v,
 
 // ---------------------------------------------------------------------------
 // One work item of the run accumulation: split `a` of the run [j0, j1) with
-// stencil key kk. Sums in registers in slot order, then adds to the shared
-// box when the whole stencil lies in the box and in the grid, else to the
-// global grid (bounds-checked, marking node blocks). Same arithmetic as
-// k_p2g_warp.
-template <int D, int S>
-__device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& TI, FusedSmem<D>& SM, const int* bo,
-                                          int j0, int j1, unsigned long long kk, int a,
-                                          unsigned long long* __restrict__ acc, unsigned* __restrict__ status) {
+// stencil key kk. Sums in registers in slot order, then, when the whole
+// stencil lies in the node box and in the grid, adds them to the shared box
+// (SACC) or to the global grid and returns the node blocks it touched as bits
+// of the 3^D blocks around the tile (tile coordinates tc); otherwise adds them
+// to the global grid bounds-checked, marking node blocks itself, and returns 0.
+// Same arithmetic as k_p2g_warp.
+template <int D, int S, bool SACC>
+__device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInfo& TI, FusedSmem<D, SACC>& SM,
+                                              const int* bo, const int* tc, int j0, int j1, unsigned long long kk,
+                                              int a, unsigned long long* __restrict__ acc,
+                                              unsigned* __restrict__ status) {
     using G = FusedGeom<D>;
     using W = WarpGeom<D, S>;
     constexpr int T = TileGeom<D>::T;
@@ -302,18 +304,43 @@ __device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& T
             raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
         const int gx = cell[0] - 1 + ax;
         if (in_box && in_grid) {
-            const int l0 = ((cell[2] - 1 - bo[2]) * G::BE + (cell[1] - 1 + by0 - bo[1])) * G::BE + (gx - bo[0]);
+            if constexpr (SACC) {
+                const int l0 = ((cell[2] - 1 - bo[2]) * G::BE + (cell[1] - 1 + by0 - bo[1])) * G::BE + (gx - bo[0]);
 #pragma unroll
-            for (int bb = 0; bb < NB; ++bb)
+                for (int bb = 0; bb < NB; ++bb)
 #pragma unroll
-                for (int cc = 0; cc < S; ++cc) {
-                    const int idx = bb * S + cc, l = l0 + bb * G::BE + cc * G::BE * G::BE;
-                    add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
-                    add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
-                    add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
-                    add_fixed_shared(&SM.acc[3][l], a2[idx], C.sp);
-                }
-            return;
+                    for (int cc = 0; cc < S; ++cc) {
+                        const int idx = bb * S + cc, l = l0 + bb * G::BE + cc * G::BE * G::BE;
+                        add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
+                        add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
+                        add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
+                        add_fixed_shared(&SM.acc[3][l], a2[idx], C.sp);
+                    }
+                return 0u;
+            } else {
+                const long long sy = C.nx, sz = (long long)C.nx * C.ny;
+                const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1 + by0)) * C.nx + gx;
+#pragma unroll
+                for (int bb = 0; bb < NB; ++bb)
+#pragma unroll
+                    for (int cc = 0; cc < S; ++cc) {
+                        const int idx = bb * S + cc;
+                        unsigned long long* p0 = acc + (g0 + bb * sy + cc * sz);
+                        red_fixed(p0, am[idx], C.sm);
+                        red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                        red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                        red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
+                    }
+                // blocks of the thread's nodes: one x block, a y range, a z range
+                // (all within one block of the tile's, since the stencil is in the box)
+                unsigned bits = 0u;
+                const int rx = gx / T - tc[0] + 1;
+                const int y0 = (cell[1] - 1 + by0) / T - tc[1] + 1, y1 = (cell[1] - 2 + by0 + NB) / T - tc[1] + 1;
+                const int z0 = (cell[2] - 1) / T - tc[2] + 1, z1 = (cell[2] + S - 2) / T - tc[2] + 1;
+                for (int rz = z0; rz <= z1; ++rz)
+                    for (int ry = y0; ry <= y1; ++ry) bits |= 1u << ((rz * 3 + ry) * 3 + rx);
+                return bits;
+            }
         }
         bool outside = false;
         for (int bb = 0; bb < NB; ++bb)
@@ -336,6 +363,7 @@ __device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& T
                     for (int by = y0 / T; by <= y1 / T; ++by)
                         mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + gx / T);
         }
+        return 0u;
     } else {
         constexpr int NA = S / W::SPLIT;
         const int gx0 = cell[0] - 1 + a * NA;
@@ -377,17 +405,37 @@ __device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& T
         if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
             raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
         if (in_box && in_grid) {
-            const int l0 = (cell[1] - 1 - bo[1]) * G::BE + (gx0 - bo[0]);
+            if constexpr (SACC) {
+                const int l0 = (cell[1] - 1 - bo[1]) * G::BE + (gx0 - bo[0]);
 #pragma unroll
-            for (int i = 0; i < NA; ++i)
+                for (int i = 0; i < NA; ++i)
 #pragma unroll
-                for (int b = 0; b < S; ++b) {
-                    const int idx = i * S + b, l = l0 + i + b * G::BE;
-                    add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
-                    add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
-                    add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
-                }
-            return;
+                    for (int b = 0; b < S; ++b) {
+                        const int idx = i * S + b, l = l0 + i + b * G::BE;
+                        add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
+                        add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
+                        add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
+                    }
+                return 0u;
+            } else {
+                const long long g0 = (long long)(cell[1] - 1) * C.nx + gx0;
+#pragma unroll
+                for (int i = 0; i < NA; ++i)
+#pragma unroll
+                    for (int b = 0; b < S; ++b) {
+                        const int idx = i * S + b;
+                        unsigned long long* p0 = acc + (g0 + i + (long long)b * C.nx);
+                        red_fixed(p0, am[idx], C.sm);
+                        red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                        red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                    }
+                unsigned bits = 0u;
+                const int x0 = gx0 / T - tc[0] + 1, x1 = (gx0 + NA - 1) / T - tc[0] + 1;
+                const int y0 = (cell[1] - 1) / T - tc[1] + 1, y1 = (cell[1] + S - 2) / T - tc[1] + 1;
+                for (int ry = y0; ry <= y1; ++ry)
+                    for (int rx = x0; rx <= x1; ++rx) bits |= 1u << (ry * 3 + rx);
+                return bits;
+            }
         }
         bool outside = false;
         for (int i = 0; i < NA; ++i)
@@ -406,13 +454,13 @@ __device__ __forceinline__ void fused_run(const StepConsts& C, const TileInfo& T
         if (x0 <= x1 && y0 <= y1)
             for (int by = y0 / T; by <= y1 / T; ++by)
                 for (int bx = x0 / T; bx <= x1 / T; ++bx) mark_block_once(TI, by * TI.nblk[0] + bx);
+        return 0u;
     }
 }
 
 // ---------------------------------------------------------------------------
 // One particle's P2G contribution to one stencil node, added on its own (no
-// grouping): the path of queued particles, shared by k_p2g_lone and the
-// prologue so both give the same int64 values.
+// grouping): the path of queued particles.
 template <int D, int S>
 __device__ __forceinline__ void lone_node(const StepConsts& C, const TileInfo& TI, const float* x, const float* mv,
                                           const float* A, float mass, int node, unsigned long long* __restrict__ acc,
@@ -481,16 +529,16 @@ __global__ void __launch_bounds__(256) k_p2g_lone(Particles P, StepConsts C, Til
 // step's P2G into `acc`). G2P = false: the P2G of the stored state only (the
 // prologue after creation, a state upload or a checkpoint load), reading B,
 // F_E, J_p and forming A as every other path does (mls_affine).
-template <int D, int S, bool G2P>
+template <int D, int S, bool G2P, bool SACC>
 __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     k_g2p2g(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
-            SlowQueue Q, unsigned char* __restrict__ lone, unsigned* __restrict__ status) {
+            SlowQueue Q, unsigned* __restrict__ status) {
     using G = FusedGeom<D>;
     using W = WarpGeom<D, S>;
     using St = Stencil<S>;
     constexpr int T = G::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FusedSmem<D>& SM = *reinterpret_cast<FusedSmem<D>*>(smem_raw);
+    FusedSmem<D, SACC>& SM = *reinterpret_cast<FusedSmem<D, SACC>*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = P.n;
     const int ntl = *TI.n_tile_list;
@@ -518,10 +566,13 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                     v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
                 SM.box[l] = v;
             }
+            if constexpr (SACC) {
 #pragma unroll
-            for (int c = 0; c < G::NCH; ++c) SM.acc[c][l] = 0ull;
+                for (int c = 0; c < G::NCH; ++c) SM.acc[c][l] = 0ull;
+            }
         }
         if (tid == 0) SM.bmask = 0u;
+        unsigned bits = 0u;  // node blocks this thread's runs added to (global adds)
         __syncthreads();
         for (int c0 = 0; c0 < m; c0 += G::CHUNK) {
             const int cnt = min(G::CHUNK, m - c0);
@@ -610,7 +661,6 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                             scatter = false;
                         }
                     }
-                    lone[i] = scatter || vol == 0.f ? 0 : kLoneScatter;
                 } else {
                     float B[D * D], Fe[D * D];
 #pragma unroll
@@ -618,15 +668,6 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
 #pragma unroll
                     for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
                     mls_affine<D, S>(C, B, Fe, P.Jp[i], mass, vol, A);
-                    if (scatter && lone && lone[i] == kLoneScatter) {
-                        // scattered one by one at the step that produced this state
-                        float mv[D];
-#pragma unroll
-                        for (int k = 0; k < D; ++k) mv[k] = mass * v[k];
-                        constexpr int NN = D == 3 ? S * S * S : S * S;
-                        for (int nd = 0; nd < NN; ++nd) lone_node<D, S>(C, TI, x, mv, A, mass, nd, acc, status);
-                        scatter = false;
-                    }
                 }
                 if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
             }
@@ -650,17 +691,29 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             if (is_start) SM.run[before + __popc(ballot & ((1u << lane) - 1))] = tid;
             if (tid == 0) SM.run[nruns] = cnt;
             __syncthreads();
+            // runs longest first, so that the SPLIT-thread groups sharing a warp
+            // have similar lengths; which threads sum a run changes no result
+            if (tid < nruns) {
+                const int len = SM.run[tid + 1] - SM.run[tid];
+                int rank = 0;
+                for (int q = 0; q < nruns; ++q) {
+                    const int lq = SM.run[q + 1] - SM.run[q];
+                    rank += lq > len || (lq == len && q < tid);
+                }
+                SM.order[rank] = tid;
+            }
+            __syncthreads();
             for (int u = tid; u < nruns * W::SPLIT; u += G::THREADS) {
-                const int r = u / W::SPLIT, a = u % W::SPLIT;
+                const int r = SM.order[u / W::SPLIT], a = u % W::SPLIT;
                 const int j0 = SM.run[r], j1 = SM.run[r + 1];
                 const unsigned long long kk = key_at(j0);
                 if (kk == kNoStencil) continue;
-                fused_run<D, S>(C, TI, SM, bo, j0, j1, kk, a, acc, status);
+                bits |= fused_run<D, S, SACC>(C, TI, SM, bo, tc, j0, j1, kk, a, acc, status);
             }
             __syncthreads();
         }
         // the box's sums into the global grid, once per node; mark node blocks
-        unsigned bits = 0u;
+        if constexpr (SACC) {
         for (int l = tid; l < G::BN; l += G::THREADS) {
             unsigned long long v[G::NCH];
             bool any = false;
@@ -676,6 +729,7 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                 if (v[c] != 0ull) atomicAdd(&acc[c * C.nodes + gid], v[c]);
             const int rx = gx / T - tc[0] + 1, ry = gy / T - tc[1] + 1, rz = D == 3 ? gz / T - tc[2] + 1 : 0;
             bits |= 1u << ((rz * 3 + ry) * 3 + rx);
+        }
         }
         bits = __reduce_or_sync(0xffffffffu, bits);
         if (lane == 0 && bits) atomicOr(&SM.bmask, bits);

@@ -336,6 +336,50 @@ __global__ void __launch_bounds__(256) k_grid_marked(StepConsts C, TileInfo TI, 
     }
 }
 
+// The int64 sums of the marked node blocks to / from a packed array
+// [block][channel][node of block] (checkpoints of the fused transfer, which
+// keep the next step's grid sums). Unpacking also marks the blocks.
+template <int D>
+__global__ void __launch_bounds__(256) k_pack_marked(StepConsts C, TileInfo TI, int nch, int nb,
+                                                     const unsigned long long* __restrict__ acc,
+                                                     unsigned long long* __restrict__ out) {
+    using G = TileGeom<D>;
+    const long long total = (long long)nb * G::BN;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+        const int blk = TI.mark_list[w / G::BN], loc = int(w % G::BN);
+        int b[3] = {0, 0, 0}, l[3] = {0, 0, 0}, rb = blk, rl = loc;
+#pragma unroll
+        for (int k = 0; k < D; ++k) { b[k] = rb % TI.nblk[k]; rb /= TI.nblk[k]; l[k] = rl % G::T; rl /= G::T; }
+        const int gx = b[0] * G::T + l[0], gy = b[1] * G::T + l[1], gz = D == 3 ? b[2] * G::T + l[2] : 0;
+        const bool in = gx < C.nx && gy < C.ny && gz < C.nz;
+        const long long id = ((long long)gz * C.ny + gy) * C.nx + gx;
+        for (int c = 0; c < nch; ++c) out[((w / G::BN) * nch + c) * G::BN + loc] = in ? acc[c * C.nodes + id] : 0ull;
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_unpack_marked(StepConsts C, TileInfo TI, int nch, int nb,
+                                                       const int* __restrict__ blocks,
+                                                       const unsigned long long* __restrict__ in,
+                                                       unsigned long long* __restrict__ acc) {
+    using G = TileGeom<D>;
+    const long long total = (long long)nb * G::BN;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+        const int blk = blocks[w / G::BN], loc = int(w % G::BN);
+        if (loc == 0) {
+            TI.mark[blk] = 1;
+            TI.mark_list[w / G::BN] = blk;
+        }
+        int b[3] = {0, 0, 0}, l[3] = {0, 0, 0}, rb = blk, rl = loc;
+#pragma unroll
+        for (int k = 0; k < D; ++k) { b[k] = rb % TI.nblk[k]; rb /= TI.nblk[k]; l[k] = rl % G::T; rl /= G::T; }
+        const int gx = b[0] * G::T + l[0], gy = b[1] * G::T + l[1], gz = D == 3 ? b[2] * G::T + l[2] : 0;
+        if (gx >= C.nx || gy >= C.ny || gz >= C.nz) continue;
+        const long long id = ((long long)gz * C.ny + gy) * C.nx + gx;
+        for (int c = 0; c < nch; ++c) acc[c * C.nodes + id] = in[((w / G::BN) * nch + c) * G::BN + loc];
+    }
+}
+
 }  // namespace mpm
 
 namespace mpm {

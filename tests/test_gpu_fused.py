@@ -61,13 +61,14 @@ def test_fused_matches_split(gpu_lib, case):
     assert errs["velocity"] < 5e-4  # relative to near-zero velocities after contact
 
 
-def test_fused_resume_is_bitwise_with_lone_scatter(gpu_lib, tmp_path):
-    """Checkpoints at steps where out-of-band particles took the one-by-one
-    scatter: the resumed run rebuilds the tiles of the last sort and the
-    pending grid sums exactly."""
+def test_fused_resume_is_bitwise(gpu_lib, tmp_path):
+    """Checkpoints taken right after the first step, after a sort and while
+    out-of-band particles take the one-by-one scatter: the resumed run restores
+    the tiles of the last sort and the pending grid sums and continues bit for
+    bit."""
     from mpm_snow_sim2d_b200 import Solver, scenes
     sc = scenes.impact_3d(steps=200)
-    for save_at in (45, 90, 130):
+    for save_at in (1, 8, 45, 90, 130):
         with Solver.from_scene(sc) as a:
             a.Step(save_at)
             a.save(tmp_path / "ck.bin")

@@ -85,6 +85,7 @@ def test_solver_with_learned_return_map(mlp_mod):
     assert flags & 1 == 0
     assert acc + rej > 1000
     rel_F = np.linalg.norm(got.elastic_f - ref.elastic_f) / np.linalg.norm(ref.elastic_f)
+    g2p = lambda t: t.get("g2p", t.get("g2p2g", 0.0))  # the fused transfer reports its kernel as g2p2g
     rel_x = np.linalg.norm(got.position - ref.position) / np.linalg.norm(ref.position)
     print(f"learned return map: accepted {acc}, fell back {rej}, rel F {rel_F:.2e}, rel x {rel_x:.2e}")
     assert rel_F <= 1e-3
@@ -111,9 +112,10 @@ def test_pretrained_weights_take_particles_off_the_svd(mlp_mod):
         got = s.get_state()
         acc, rej = s.mlp_stats()
     rel_F = np.linalg.norm(got.elastic_f - ref.elastic_f) / np.linalg.norm(ref.elastic_f)
+    g2p = lambda t: t.get("g2p", t.get("g2p2g", 0.0))  # the fused transfer reports its kernel as g2p2g
     print(f"pretrained: accepted {acc}, fell back {rej}, rel F {rel_F:.2e}, "
           f"return map {t_plain['return_map']:.2f} ms -> {t_mlp['return_map']:.2f} ms, "
-          f"G2P {t_plain['g2p'] + t_plain['return_map']:.2f} ms -> {t_mlp['g2p'] + t_mlp['return_map']:.2f} ms "
+          f"G2P {g2p(t_plain) + t_plain['return_map']:.2f} ms -> {g2p(t_mlp) + t_mlp['return_map']:.2f} ms "
           f"over 300 steps")
     assert acc > 4 * rej
     assert rel_F <= 1e-3

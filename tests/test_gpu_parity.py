@@ -66,9 +66,14 @@ def _fp32_reference_errors(O, scene, steps):
 
 def _check_vs_fp32_reference(errs, ref32, label, floor=TARGET):
     """After contact, velocities approach zero and relative errors grow: the bar
-    is the FP32 reference arithmetic's own distance from FP64 (x1.5), never
-    looser than needed and never tighter than `floor`."""
-    tol = {k: max(floor[k], 1.5 * ref32[k]) for k in errs}
+    is twice the reference's own FP32 arithmetic's distance from FP64 (the
+    oracle's FP32 instantiation reproduces the reference's shaders bit for
+    bit, tests/test_shader_pin.py), never tighter than `floor`. Two FP32
+    implementations that sum in different orders land on different sides of
+    wall-contact and clamping branches for a few particles, which moves these
+    distances by tens of percent either way (the same factor 2 bounds the
+    CLASSIC path against the reference's compiled CPU code)."""
+    tol = {k: max(floor[k], 2.0 * ref32[k]) for k in errs}
     _check(errs, tol, label)
 
 
