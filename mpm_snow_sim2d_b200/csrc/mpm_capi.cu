@@ -113,7 +113,6 @@ struct mpm_solver {
     bool fused = false;
     bool acc_pending = false;
     int fused_grid = 0;
-    bool fused_sacc = true;         // run sums through a shared-memory node box (else straight to the grid)
 };
 
 namespace {
@@ -421,12 +420,8 @@ template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
     if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
     if (s->n == 0) return cudaSuccess;
-    if (s->fused_sacc)
-        k_g2p2g<D, S, G2P, true><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, true>), s->stream>>>(
-            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
-    else
-        k_g2p2g<D, S, G2P, false><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, false>), s->stream>>>(
-            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
+    k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
+        particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
     return cudaGetLastError();
 }
 
@@ -591,34 +586,17 @@ mpm_status setup_tiled(mpm_solver* s) {
         s->fused = !(tr && std::strcmp(tr, "split") == 0);
     }
     if (s->fused) {
-        {
-            const char* sa = std::getenv("MPM_FUSED_SACC");
-            if (sa) s->fused_sacc = std::strcmp(sa, "0") != 0;
-        }
         const void* kfn;
         size_t fsm;
         const void* kpro;
-        const bool sacc = s->fused_sacc;
         if (D == 3) {
-            if (sacc) {
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, true> : (const void*)k_g2p2g<3, 4, true, true>;
-                kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false, true> : (const void*)k_g2p2g<3, 4, false, true>;
-            } else {
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, false> : (const void*)k_g2p2g<3, 4, true, false>;
-                kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false, false>
-                                       : (const void*)k_g2p2g<3, 4, false, false>;
-            }
-            fsm = sacc ? sizeof(FusedSmem<3, true>) : sizeof(FusedSmem<3, false>);
+            kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
+            kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false> : (const void*)k_g2p2g<3, 4, false>;
+            fsm = sizeof(FusedSmem<3>);
         } else {
-            if (sacc) {
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, true> : (const void*)k_g2p2g<2, 4, true, true>;
-                kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false, true> : (const void*)k_g2p2g<2, 4, false, true>;
-            } else {
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, false> : (const void*)k_g2p2g<2, 4, true, false>;
-                kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false, false>
-                                       : (const void*)k_g2p2g<2, 4, false, false>;
-            }
-            fsm = sacc ? sizeof(FusedSmem<2, true>) : sizeof(FusedSmem<2, false>);
+            kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
+            kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false> : (const void*)k_g2p2g<2, 4, false>;
+            fsm = sizeof(FusedSmem<2>);
         }
         int per = 0;
         cudaError_t ef = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);

@@ -3,30 +3,32 @@
 // and Scalable Multi-GPU Material Point Method", ACM TOG 39(4), 2020).
 //
 // One CTA per non-empty cell tile of the last sort (tiles handed out from a
-// counter). For its tile it
-//   1. stages the node velocities of a fixed box of BE^D nodes around the
-//      tile in shared memory (the stencils of every particle sorted into the
-//      tile that has since moved less than a cell);
-//   2. per particle (one thread each, in chunks of CHUNK slots): gathers the
-//      grid from that box (src/gpu/shaders/3d/g2p.glsl:28-71), updates x, v, B
-//      and the trial F_E, and when the return map is provably the identity
-//      (elastic band) computes the next step's P2G affine matrix
-//      A = 3 m B - 3 dt V sigma in registers (3d/p2g.glsl:44-90); the rest are
-//      queued for the exact (or learned) return map with their trial F;
-//   3. writes each in-band particle's P2G payload (stencil weights at the new
-//      position, m v, A) to shared memory, groups consecutive slots that share
-//      a stencil into runs, and SPLIT threads per run sum the run's node
-//      contributions in FP32 registers in slot order, then add them as int64
-//      fixed point to a shared-memory accumulator over the same node box;
-//   4. adds the box's non-zero sums to the global grid once per node and marks
-//      the touched node blocks for the grid update.
-// Particles whose stencil leaves the box (drifted more than a cell since the
-// sort) gather from and scatter to global memory directly. Queued particles
-// (out of the elastic band, or a stencil clipped by the grid edge) are
-// scattered one by one after their return map (k_p2g_lone).
+// counter). The CTA stages the node velocities of a fixed box of BE^D nodes
+// around its tile in shared memory (the stencils of every particle sorted into
+// the tile that has since moved less than a cell). Then each warp, on its own,
+// takes windows of 32 consecutive slots of the tile (handed out from a shared
+// counter) and for its window
+//   1. per particle (one lane each): gathers the grid from the box
+//      (src/gpu/shaders/3d/g2p.glsl:28-71), updates x, v, B and the trial F_E,
+//      and when the return map is provably the identity (elastic band)
+//      computes the next step's P2G affine matrix A = 3 m B - 3 dt V sigma in
+//      registers (3d/p2g.glsl:44-90); the rest are queued for the exact (or
+//      learned) return map with their trial F;
+//   2. writes each in-band particle's P2G payload (stencil weights at the new
+//      position, m v, A) to the warp's shared-memory window, groups
+//      consecutive slots that share a stencil into runs, and SPLIT lanes per
+//      run (longest runs first) sum the run's node contributions in FP32
+//      registers in slot order and add them to the global grid as int64 fixed
+//      point (red.global, no return value).
+// Warps synchronise only per tile (staging the box), so a warp with slow
+// particles or a long run holds up no other. Particles whose stencil leaves
+// the box (drifted more than a cell since the sort) gather from global memory
+// and their runs add bounds-checked. Queued particles (out of the elastic
+// band, or a stencil clipped by the grid edge) are scattered one by one after
+// their return map (k_p2g_lone).
 //
 // Determinism: every cross-run sum is an integer add, and the runs are a
-// function of the slot order, the chunk boundaries (fixed offsets inside a
+// function of the slot order, the window boundaries (fixed offsets inside a
 // tile) and which particles were queued -- all functions of the state. After
 // creation or a state upload a P2G-only pass of the same kernel (reading the
 // stored state) forms the first sums. A checkpoint stores the pending sums
@@ -37,34 +39,35 @@
 
 namespace mpm {
 
+#ifndef MPM_FUSED_THREADS
+#define MPM_FUSED_THREADS 128
+#endif
 template <int D> struct FusedGeom {
     static constexpr int T = TileGeom<D>::T;            // cells per tile edge: 4 (3D), 8 (2D)
     static constexpr int BE = T + 5;                    // box edge in nodes: tile nodes - 2 .. tile + T + 2
     static constexpr int BN = D == 3 ? BE * BE * BE : BE * BE;  // 729 (3D), 169 (2D)
-    static constexpr int NCH = 1 + D;                   // mass + momentum channels
-    static constexpr int THREADS = 256;
-    static constexpr int CHUNK = 256;                   // slots per pass (one per thread)
+    static constexpr int THREADS = MPM_FUSED_THREADS;
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int WIN = 32;                      // slots per warp window (one per lane)
     static constexpr int PS = WarpGeom<D, 4>::PS;       // payload floats per particle (3D 36, 2D 20)
     static constexpr int KEYF = PS - 2;                 // payload floats holding the 64-bit stencil key
+    static_assert(THREADS % 32 == 0, "whole warps");
 };
 
-// SACC: the run sums go to an int64 accumulator over the node box in shared
-// memory, added to the global grid once per node at the end of the tile;
-// otherwise each run adds its sums to the global grid directly (red.global).
-template <int D, bool SACC> struct FusedSmem {
+template <int D> struct FusedSmem {
     using G = FusedGeom<D>;
     float4 box[G::BN];                                  // 3D: (vf, wall flag); 2D: (vf, vc)
-    unsigned long long acc[SACC ? G::NCH : 1][SACC ? G::BN : 1];  // int64 fixed-point sums of the next P2G
-    float4 pay[G::CHUNK * G::PS / 4];
-    int run[G::CHUNK + 1];                              // start slot of each run, then the chunk end
-    int order[G::CHUNK];                                // runs, longest first
-    unsigned starts[G::CHUNK / 32];                     // run-start ballot per warp
+    float4 pay[G::WARPS][G::WIN * G::PS / 4];           // per warp: the window's P2G payloads
+    int run[G::WARPS][G::WIN + 1];                      // per warp: start slot of each run, then the window end
+    int order[G::WARPS][G::WIN];                        // per warp: runs, longest first
     int tile;
+    int next_win;                                       // next window of the tile to hand out
     unsigned bmask;                                     // node blocks (3^D around the tile) that received sums
 };
 
+// CTAs per SM the register budget is sized for: 24 warps per SM (80 registers)
 #ifndef MPM_FUSED_MIN_BLOCKS
-#define MPM_FUSED_MIN_BLOCKS 3
+#define MPM_FUSED_MIN_BLOCKS (768 / MPM_FUSED_THREADS)
 #endif
 
 // ---------------------------------------------------------------------------
@@ -220,28 +223,24 @@ __device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, c
 }
 
 // Adds one int64 value: to the shared box (local index) or the global grid.
-__device__ __forceinline__ void add_fixed_shared(unsigned long long* p, float v, float scale) {
-    atomicAdd(p, (unsigned long long)__float2ll_rn(v * scale));
-}
-
 // ---------------------------------------------------------------------------
-// One work item of the run accumulation: split `a` of the run [j0, j1) with
-// stencil key kk. Sums in registers in slot order, then, when the whole
-// stencil lies in the node box and in the grid, adds them to the shared box
-// (SACC) or to the global grid and returns the node blocks it touched as bits
-// of the 3^D blocks around the tile (tile coordinates tc); otherwise adds them
-// to the global grid bounds-checked, marking node blocks itself, and returns 0.
-// Same arithmetic as k_p2g_warp.
-template <int D, int S, bool SACC>
-__device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInfo& TI, FusedSmem<D, SACC>& SM,
+// One work item of the run accumulation: split `a` of the run [j0, j1) of a
+// warp's payload window `pay`, stencil key kk. Sums in registers in slot
+// order and adds them to the global grid as int64 fixed point. When the whole
+// stencil lies in the tile's node box and in the grid the adds need no bounds
+// checks and the function returns the node blocks they touched, as bits of
+// the 3^D blocks around the tile (tile coordinates tc); otherwise the adds
+// are bounds-checked, the node blocks marked here, and it returns 0. Same
+// arithmetic as k_p2g_warp.
+template <int D, int S>
+__device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInfo& TI, const float4* pay,
                                               const int* bo, const int* tc, int j0, int j1, unsigned long long kk,
                                               int a, unsigned long long* __restrict__ acc,
                                               unsigned* __restrict__ status) {
     using G = FusedGeom<D>;
     using W = WarpGeom<D, S>;
     constexpr int T = TileGeom<D>::T;
-    const float4* pay = SM.pay;
-    const float* payf = reinterpret_cast<const float*>(SM.pay);
+    const float* payf = reinterpret_cast<const float*>(pay);
     int cell[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < D; ++k) cell[k] = int((kk >> (StencilKey<D>::BITS * k)) & StencilKey<D>::MASK) - 8;
@@ -304,43 +303,28 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
             raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
         const int gx = cell[0] - 1 + ax;
         if (in_box && in_grid) {
-            if constexpr (SACC) {
-                const int l0 = ((cell[2] - 1 - bo[2]) * G::BE + (cell[1] - 1 + by0 - bo[1])) * G::BE + (gx - bo[0]);
+            const long long sy = C.nx, sz = (long long)C.nx * C.ny;
+            const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1 + by0)) * C.nx + gx;
 #pragma unroll
-                for (int bb = 0; bb < NB; ++bb)
+            for (int bb = 0; bb < NB; ++bb)
 #pragma unroll
-                    for (int cc = 0; cc < S; ++cc) {
-                        const int idx = bb * S + cc, l = l0 + bb * G::BE + cc * G::BE * G::BE;
-                        add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
-                        add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
-                        add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
-                        add_fixed_shared(&SM.acc[3][l], a2[idx], C.sp);
-                    }
-                return 0u;
-            } else {
-                const long long sy = C.nx, sz = (long long)C.nx * C.ny;
-                const long long g0 = ((long long)(cell[2] - 1) * C.ny + (cell[1] - 1 + by0)) * C.nx + gx;
-#pragma unroll
-                for (int bb = 0; bb < NB; ++bb)
-#pragma unroll
-                    for (int cc = 0; cc < S; ++cc) {
-                        const int idx = bb * S + cc;
-                        unsigned long long* p0 = acc + (g0 + bb * sy + cc * sz);
-                        red_fixed(p0, am[idx], C.sm);
-                        red_fixed(p0 + C.nodes, a0[idx], C.sp);
-                        red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
-                        red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
-                    }
-                // blocks of the thread's nodes: one x block, a y range, a z range
-                // (all within one block of the tile's, since the stencil is in the box)
-                unsigned bits = 0u;
-                const int rx = gx / T - tc[0] + 1;
-                const int y0 = (cell[1] - 1 + by0) / T - tc[1] + 1, y1 = (cell[1] - 2 + by0 + NB) / T - tc[1] + 1;
-                const int z0 = (cell[2] - 1) / T - tc[2] + 1, z1 = (cell[2] + S - 2) / T - tc[2] + 1;
-                for (int rz = z0; rz <= z1; ++rz)
-                    for (int ry = y0; ry <= y1; ++ry) bits |= 1u << ((rz * 3 + ry) * 3 + rx);
-                return bits;
-            }
+                for (int cc = 0; cc < S; ++cc) {
+                    const int idx = bb * S + cc;
+                    unsigned long long* p0 = acc + (g0 + bb * sy + cc * sz);
+                    red_fixed(p0, am[idx], C.sm);
+                    red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                    red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                    red_fixed(p0 + 3 * C.nodes, a2[idx], C.sp);
+                }
+            // blocks of the thread's nodes: one x block, a y range, a z range
+            // (all within one block of the tile's, since the stencil is in the box)
+            unsigned bits = 0u;
+            const int rx = gx / T - tc[0] + 1;
+            const int y0 = (cell[1] - 1 + by0) / T - tc[1] + 1, y1 = (cell[1] - 2 + by0 + NB) / T - tc[1] + 1;
+            const int z0 = (cell[2] - 1) / T - tc[2] + 1, z1 = (cell[2] + S - 2) / T - tc[2] + 1;
+            for (int rz = z0; rz <= z1; ++rz)
+                for (int ry = y0; ry <= y1; ++ry) bits |= 1u << ((rz * 3 + ry) * 3 + rx);
+            return bits;
         }
         bool outside = false;
         for (int bb = 0; bb < NB; ++bb)
@@ -405,37 +389,23 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
         if (!(mx_m * C.sm < kFixedLimit && mx_p * C.sp < kFixedLimit))
             raise_flag(status, (mx_m != mx_m || mx_p != mx_p) ? 1u : 2u);
         if (in_box && in_grid) {
-            if constexpr (SACC) {
-                const int l0 = (cell[1] - 1 - bo[1]) * G::BE + (gx0 - bo[0]);
+            const long long g0 = (long long)(cell[1] - 1) * C.nx + gx0;
 #pragma unroll
-                for (int i = 0; i < NA; ++i)
+            for (int i = 0; i < NA; ++i)
 #pragma unroll
-                    for (int b = 0; b < S; ++b) {
-                        const int idx = i * S + b, l = l0 + i + b * G::BE;
-                        add_fixed_shared(&SM.acc[0][l], am[idx], C.sm);
-                        add_fixed_shared(&SM.acc[1][l], a0[idx], C.sp);
-                        add_fixed_shared(&SM.acc[2][l], a1[idx], C.sp);
-                    }
-                return 0u;
-            } else {
-                const long long g0 = (long long)(cell[1] - 1) * C.nx + gx0;
-#pragma unroll
-                for (int i = 0; i < NA; ++i)
-#pragma unroll
-                    for (int b = 0; b < S; ++b) {
-                        const int idx = i * S + b;
-                        unsigned long long* p0 = acc + (g0 + i + (long long)b * C.nx);
-                        red_fixed(p0, am[idx], C.sm);
-                        red_fixed(p0 + C.nodes, a0[idx], C.sp);
-                        red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
-                    }
-                unsigned bits = 0u;
-                const int x0 = gx0 / T - tc[0] + 1, x1 = (gx0 + NA - 1) / T - tc[0] + 1;
-                const int y0 = (cell[1] - 1) / T - tc[1] + 1, y1 = (cell[1] + S - 2) / T - tc[1] + 1;
-                for (int ry = y0; ry <= y1; ++ry)
-                    for (int rx = x0; rx <= x1; ++rx) bits |= 1u << (ry * 3 + rx);
-                return bits;
-            }
+                for (int b = 0; b < S; ++b) {
+                    const int idx = i * S + b;
+                    unsigned long long* p0 = acc + (g0 + i + (long long)b * C.nx);
+                    red_fixed(p0, am[idx], C.sm);
+                    red_fixed(p0 + C.nodes, a0[idx], C.sp);
+                    red_fixed(p0 + 2 * C.nodes, a1[idx], C.sp);
+                }
+            unsigned bits = 0u;
+            const int x0 = gx0 / T - tc[0] + 1, x1 = (gx0 + NA - 1) / T - tc[0] + 1;
+            const int y0 = (cell[1] - 1) / T - tc[1] + 1, y1 = (cell[1] + S - 2) / T - tc[1] + 1;
+            for (int ry = y0; ry <= y1; ++ry)
+                for (int rx = x0; rx <= x1; ++rx) bits |= 1u << (ry * 3 + rx);
+            return bits;
         }
         bool outside = false;
         for (int i = 0; i < NA; ++i)
@@ -526,10 +496,10 @@ __global__ void __launch_bounds__(256) k_p2g_lone(Particles P, StepConsts C, Til
 
 // ---------------------------------------------------------------------------
 // The fused kernel. G2P = true: one step (G2P of the state, then the next
-// step's P2G into `acc`). G2P = false: the P2G of the stored state only (the
-// prologue after creation, a state upload or a checkpoint load), reading B,
-// F_E, J_p and forming A as every other path does (mls_affine).
-template <int D, int S, bool G2P, bool SACC>
+// step's P2G into `acc`). G2P = false: the P2G of the stored state only (after
+// creation or a state upload), reading B, F_E, J_p and forming A as every
+// other path does (mls_affine).
+template <int D, int S, bool G2P>
 __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     k_g2p2g(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
             SlowQueue Q, unsigned* __restrict__ status) {
@@ -538,14 +508,21 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     using St = Stencil<S>;
     constexpr int T = G::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FusedSmem<D, SACC>& SM = *reinterpret_cast<FusedSmem<D, SACC>*>(smem_raw);
+    FusedSmem<D>& SM = *reinterpret_cast<FusedSmem<D>*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = P.n;
     const int ntl = *TI.n_tile_list;
     const long long gsy = C.nx, gsz = (long long)C.nx * C.ny;
+    float4* pay = SM.pay[wid];
+    int* run = SM.run[wid];
+    int* order = SM.order[wid];
     for (;;) {
-        if (tid == 0) SM.tile = atomicAdd(TI.fused_next, 1);
-        __syncthreads();
+        if (tid == 0) {
+            SM.tile = atomicAdd(TI.fused_next, 1);
+            SM.next_win = 0;
+            SM.bmask = 0u;
+        }
+        __syncthreads();  // also: every warp is done with the previous tile's box
         const int e = SM.tile;
         if (e >= ntl) break;
         const int t = TI.tile_list[e];
@@ -556,9 +533,8 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
 #pragma unroll
             for (int k = 0; k < D; ++k) { tc[k] = r % TI.tiles[k]; r /= TI.tiles[k]; bo[k] = tc[k] * T - 2; }
         }
-        // stage the box: node velocities (G2P), zero sums
-        for (int l = tid; l < G::BN; l += G::THREADS) {
-            if constexpr (G2P) {
+        if constexpr (G2P) {  // stage the node velocities of the box
+            for (int l = tid; l < G::BN; l += G::THREADS) {
                 const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
                 const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -566,20 +542,20 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                     v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
                 SM.box[l] = v;
             }
-            if constexpr (SACC) {
-#pragma unroll
-                for (int c = 0; c < G::NCH; ++c) SM.acc[c][l] = 0ull;
-            }
+            __syncthreads();
         }
-        if (tid == 0) SM.bmask = 0u;
-        unsigned bits = 0u;  // node blocks this thread's runs added to (global adds)
-        __syncthreads();
-        for (int c0 = 0; c0 < m; c0 += G::CHUNK) {
-            const int cnt = min(G::CHUNK, m - c0);
-            const bool valid = tid < cnt;
-            const int i = start + c0 + tid;
+        unsigned bits = 0u;  // node blocks this lane's in-box runs added to
+        const int nwin = (m + G::WIN - 1) / G::WIN;
+        for (;;) {
+            int w = 0;
+            if (lane == 0) w = atomicAdd(&SM.next_win, 1);
+            w = __shfl_sync(0xffffffffu, w, 0);
+            if (w >= nwin) break;
+            const int cnt = min(G::WIN, m - w * G::WIN);
+            const bool valid = lane < cnt;
+            const int i = start + w * G::WIN + lane;
             unsigned long long key = kNoStencil;
-            float* q = reinterpret_cast<float*>(SM.pay) + tid * G::PS;
+            float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
             if (valid) {
                 const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
                 float x[D], v[D], A[D * D];
@@ -672,65 +648,40 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                 if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
             }
             reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
-            __syncthreads();
+            __syncwarp();
             // runs: maximal stretches of consecutive slots with one stencil key
             const unsigned long long* keyp = reinterpret_cast<const unsigned long long*>(
-                reinterpret_cast<const float*>(SM.pay) + G::KEYF);
+                reinterpret_cast<const float*>(pay) + G::KEYF);
             auto key_at = [&](int j) { return keyp[j * (G::PS / 2)]; };
-            const bool is_start = valid && (tid == 0 || key_at(tid) != key_at(tid - 1));
-            const unsigned ballot = __ballot_sync(0xffffffffu, is_start);
-            if (lane == 0) SM.starts[wid] = ballot;
-            __syncthreads();
-            int nruns = 0, before = 0;
-#pragma unroll
-            for (int w = 0; w < G::CHUNK / 32; ++w) {
-                const int c = __popc(SM.starts[w]);
-                before += w < wid ? c : 0;
-                nruns += c;
-            }
-            if (is_start) SM.run[before + __popc(ballot & ((1u << lane) - 1))] = tid;
-            if (tid == 0) SM.run[nruns] = cnt;
-            __syncthreads();
-            // runs longest first, so that the SPLIT-thread groups sharing a warp
-            // have similar lengths; which threads sum a run changes no result
-            if (tid < nruns) {
-                const int len = SM.run[tid + 1] - SM.run[tid];
+            const bool is_start = valid && (lane == 0 || key_at(lane) != key_at(lane - 1));
+            const unsigned starts = __ballot_sync(0xffffffffu, is_start);
+            const int nruns = __popc(starts);
+            const int r_me = __popc(starts & ((1u << lane) - 1));
+            if (is_start) run[r_me] = lane;
+            if (lane == 0) run[nruns] = cnt;
+            __syncwarp();
+            // runs longest first, so that the SPLIT-lane groups sharing a pass
+            // have similar lengths; which lanes sum a run changes no result
+            {
+                const int len = lane < nruns ? run[lane + 1] - run[lane] : 0;
                 int rank = 0;
-                for (int q = 0; q < nruns; ++q) {
-                    const int lq = SM.run[q + 1] - SM.run[q];
-                    rank += lq > len || (lq == len && q < tid);
+                for (int qr = 0; qr < nruns; ++qr) {
+                    const int lq = __shfl_sync(0xffffffffu, len, qr);
+                    rank += lq > len || (lq == len && qr < lane);
                 }
-                SM.order[rank] = tid;
+                if (lane < nruns) order[rank] = lane;
             }
-            __syncthreads();
-            for (int u = tid; u < nruns * W::SPLIT; u += G::THREADS) {
-                const int r = SM.order[u / W::SPLIT], a = u % W::SPLIT;
-                const int j0 = SM.run[r], j1 = SM.run[r + 1];
+            __syncwarp();
+            for (int u = lane; u < nruns * W::SPLIT; u += 32) {
+                const int r = order[u / W::SPLIT], a = u % W::SPLIT;
+                const int j0 = run[r], j1 = run[r + 1];
                 const unsigned long long kk = key_at(j0);
                 if (kk == kNoStencil) continue;
-                bits |= fused_run<D, S, SACC>(C, TI, SM, bo, tc, j0, j1, kk, a, acc, status);
+                bits |= fused_run<D, S>(C, TI, pay, bo, tc, j0, j1, kk, a, acc, status);
             }
-            __syncthreads();
+            __syncwarp();  // the window's payload and runs are reused by the next window
         }
-        // the box's sums into the global grid, once per node; mark node blocks
-        if constexpr (SACC) {
-        for (int l = tid; l < G::BN; l += G::THREADS) {
-            unsigned long long v[G::NCH];
-            bool any = false;
-#pragma unroll
-            for (int c = 0; c < G::NCH; ++c) { v[c] = SM.acc[c][l]; any = any || v[c] != 0ull; }
-            if (!any) continue;
-            const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
-            const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
-            // only runs wholly inside the grid add to the box: gx, gy, gz are in range
-            const long long gid = gz * gsz + gy * gsy + gx;
-#pragma unroll
-            for (int c = 0; c < G::NCH; ++c)
-                if (v[c] != 0ull) atomicAdd(&acc[c * C.nodes + gid], v[c]);
-            const int rx = gx / T - tc[0] + 1, ry = gy / T - tc[1] + 1, rz = D == 3 ? gz / T - tc[2] + 1 : 0;
-            bits |= 1u << ((rz * 3 + ry) * 3 + rx);
-        }
-        }
+        // mark the node blocks the tile's in-box runs added to
         bits = __reduce_or_sync(0xffffffffu, bits);
         if (lane == 0 && bits) atomicOr(&SM.bmask, bits);
         __syncthreads();
@@ -740,6 +691,7 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             const int bx = tc[0] - 1 + rx, by = tc[1] - 1 + ry, bz = D == 3 ? tc[2] - 1 + rz : 0;
             mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
         }
+        __syncthreads();  // SM.bmask is reset for the next tile
     }
 }
 
