@@ -49,7 +49,7 @@ template <int D> struct FusedGeom {
     static constexpr int THREADS = MPM_FUSED_THREADS;
     static constexpr int WARPS = THREADS / 32;
     static constexpr int WIN = 32;                      // slots per warp window (one per lane)
-    static constexpr int PS = WarpGeom<D, 4>::PS;       // payload floats per particle (3D 36, 2D 20)
+    static constexpr int PS = D == 3 ? 40 : 20;         // payload floats per particle (layout: p2g_payload)
     static constexpr int KEYF = PS - 2;                 // payload floats holding the 64-bit stencil key
     static_assert(THREADS % 32 == 0, "whole warps");
 };
@@ -65,9 +65,11 @@ template <int D> struct FusedSmem {
     unsigned bmask;                                     // node blocks (3^D around the tile) that received sums
 };
 
-// CTAs per SM the register budget is sized for: 24 warps per SM (80 registers)
+// CTAs per SM the register budget is sized for: 20 warps per SM, 96
+// registers (measured on the 128^3 snowball scene: 6 % faster than 24 warps at
+// 80 registers, which spill)
 #ifndef MPM_FUSED_MIN_BLOCKS
-#define MPM_FUSED_MIN_BLOCKS (768 / MPM_FUSED_THREADS)
+#define MPM_FUSED_MIN_BLOCKS (640 / MPM_FUSED_THREADS)
 #endif
 
 // ---------------------------------------------------------------------------
@@ -182,8 +184,14 @@ __device__ __forceinline__ void gather_nodes(const StepConsts& C, const float4* 
 }
 
 // ---------------------------------------------------------------------------
-// P2G payload of one particle at position x (layout of k_p2g_warp's payload;
-// the 64-bit stencil key goes in the last two floats).
+// P2G payload of one particle at position x; the 64-bit stencil key goes in
+// the last two floats. f = x - (base + 1) is the offset in the particle's cell.
+//   3D (40): wx[4] | wy[4] | wz[4] | yd[4] | zd[4] | s0 s1 m s2 |
+//            A00 A10 0 A20 | A01 A11 0 A21 | A02 A12 0 A22 | pad pad key
+//            with yd[b] = wy[b] (b - 1 - fy), zd[c] = wz[c] (c - 1 - fz),
+//            s_r = m v_r - fx A_r0: the momentum channels in pairs (0, 1) and
+//            (mass, 2) for the packed FP32 accumulation of fused_run.
+//   2D (20): wx[4] | wy[4] | fx fy m mv0 | mv1 A00 A01 A10 | A11 pad key
 template <int D, int S>
 __device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, const float* x, const float* v,
                                                           const float* A, float mass, float* q) {
@@ -208,11 +216,10 @@ __device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, c
             q[12 + o] = q[4 + o] * (float(o - 1) - f[1]);
             q[16 + o] = q[8 + o] * (float(o - 1) - f[2]);
         }
-        reinterpret_cast<float4*>(q)[5] = make_float4(mass, mv[0] - f[0] * A[0], mv[1] - f[0] * A[3], mv[2] - f[0] * A[6]);
-        reinterpret_cast<float4*>(q)[6] = make_float4(A[0], A[3], A[6], A[1]);
-        reinterpret_cast<float4*>(q)[7] = make_float4(A[4], A[7], A[2], A[5]);
-        q[32] = A[8];
-        q[33] = 0.f;
+        reinterpret_cast<float4*>(q)[5] = make_float4(mv[0] - f[0] * A[0], mv[1] - f[0] * A[3], mass, mv[2] - f[0] * A[6]);
+        reinterpret_cast<float4*>(q)[6] = make_float4(A[0], A[3], 0.f, A[6]);
+        reinterpret_cast<float4*>(q)[7] = make_float4(A[1], A[4], 0.f, A[7]);
+        reinterpret_cast<float4*>(q)[8] = make_float4(A[2], A[5], 0.f, A[8]);
     } else {
         reinterpret_cast<float4*>(q)[2] = make_float4(f[0], f[1], mass, mv[0]);
         reinterpret_cast<float4*>(q)[3] = make_float4(mv[1], A[0], A[1], A[2]);
@@ -222,7 +229,6 @@ __device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, c
     return k3;
 }
 
-// Adds one int64 value: to the shared box (local index) or the global grid.
 // ---------------------------------------------------------------------------
 // One work item of the run accumulation: split `a` of the run [j0, j1) of a
 // warp's payload window `pay`, stencil key kk. Sums in registers in slot
@@ -256,43 +262,51 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
         constexpr int NB = S * S / W::SPLIT;
         constexpr int NN = NB * S;
         const int ax = a % S, by0 = (a / S) * NB;
-        float am[NN], a0[NN], a1[NN], a2[NN];
+        // channel pairs (a0, a1) and (am, a2) per node, in packed FP32
+        // (fma.rn.f32x2: two FP32 FMAs per instruction)
+        float2 p01[NN], pm2[NN];
 #pragma unroll
-        for (int k = 0; k < NN; ++k) { am[k] = 0.f; a0[k] = 0.f; a1[k] = 0.f; a2[k] = 0.f; }
-        const float da = float(ax - 1);
+        for (int k = 0; k < NN; ++k) { p01[k] = make_float2(0.f, 0.f); pm2[k] = make_float2(0.f, 0.f); }
+        const float2 da2 = make_float2(float(ax - 1), float(ax - 1));
         for (int j = j0; j < j1; ++j) {
             const float4* pp = pay + j * (G::PS / 4);
             const float alpha = payf[j * G::PS + ax];
-            const float4 wy = pp[1], wz = pp[2], yd = pp[3], zd = pp[4], ms = pp[5], q6 = pp[6], q7 = pp[7];
-            const float a22 = payf[j * G::PS + 32];
-            const float ad = alpha * da;
-            const float e0 = alpha * ms.y + ad * q6.x;
-            const float e1 = alpha * ms.z + ad * q6.y;
-            const float e2 = alpha * ms.w + ad * q6.z;
-            const float f0 = alpha * q6.w, f1 = alpha * q7.x, f2 = alpha * q7.y;
-            const float g0 = alpha * q7.z, g1 = alpha * q7.w, g2 = alpha * a22;
-            const float ma = ms.x * alpha;
+            const float2 al2 = make_float2(alpha, alpha);
+            const float4 wy = pp[1], wz = pp[2], yd = pp[3], zd = pp[4], p5 = pp[5], p6 = pp[6], p7 = pp[7],
+                         p8 = pp[8];
+            // (e0, e1) = alpha (s0 + da A00, s1 + da A10); (ma, e2) = alpha (m, s2 + da A20)
+            const float2 e01 = __fmul2_rn(al2, __ffma2_rn(da2, make_float2(p6.x, p6.y), make_float2(p5.x, p5.y)));
+            const float2 me2 = __fmul2_rn(al2, __ffma2_rn(da2, make_float2(p6.z, p6.w), make_float2(p5.z, p5.w)));
+            const float2 f01 = __fmul2_rn(al2, make_float2(p7.x, p7.y)), f_2 = __fmul2_rn(al2, make_float2(p7.z, p7.w));
+            const float2 g01 = __fmul2_rn(al2, make_float2(p8.x, p8.y)), g_2 = __fmul2_rn(al2, make_float2(p8.z, p8.w));
             const float Z[4] = {wz.x, wz.y, wz.z, wz.w};
             const float Zd[4] = {zd.x, zd.y, zd.z, zd.w};
             const float Yv[4] = {wy.x, wy.y, wy.z, wy.w};
             const float Ydv[4] = {yd.x, yd.y, yd.z, yd.w};
+            float2 Z2[S], Zd2[S];
+#pragma unroll
+            for (int cc = 0; cc < S; ++cc) { Z2[cc] = make_float2(Z[cc], Z[cc]); Zd2[cc] = make_float2(Zd[cc], Zd[cc]); }
 #pragma unroll
             for (int bb = 0; bb < NB; ++bb) {
                 const int b = by0 + bb;
                 const float Y = NB == S ? Yv[bb] : (b == 0 ? wy.x : b == 1 ? wy.y : b == 2 ? wy.z : wy.w);
                 const float Yd = NB == S ? Ydv[bb] : (b == 0 ? yd.x : b == 1 ? yd.y : b == 2 ? yd.z : yd.w);
-                const float h0 = e0 * Y + f0 * Yd, h1 = e1 * Y + f1 * Yd, h2 = e2 * Y + f2 * Yd;
-                const float k0 = g0 * Y, k1 = g1 * Y, k2 = g2 * Y, mY = ma * Y;
+                const float2 Y2 = make_float2(Y, Y), Yd2 = make_float2(Yd, Yd);
+                // (h0, h1), (mY, h2): h_r = e_r Y + f_r Yd, mY = ma Y; (k0, k1), (0, k2): k_r = g_r Y
+                const float2 h01 = __ffma2_rn(e01, Y2, __fmul2_rn(f01, Yd2));
+                const float2 hm2 = __ffma2_rn(me2, Y2, __fmul2_rn(f_2, Yd2));
+                const float2 k01 = __fmul2_rn(g01, Y2), k_2 = __fmul2_rn(g_2, Y2);
 #pragma unroll
                 for (int cc = 0; cc < S; ++cc) {
                     const int idx = bb * S + cc;
-                    am[idx] += mY * Z[cc];
-                    a0[idx] += h0 * Z[cc] + k0 * Zd[cc];
-                    a1[idx] += h1 * Z[cc] + k1 * Zd[cc];
-                    a2[idx] += h2 * Z[cc] + k2 * Zd[cc];
+                    p01[idx] = __ffma2_rn(h01, Z2[cc], __ffma2_rn(k01, Zd2[cc], p01[idx]));
+                    pm2[idx] = __ffma2_rn(hm2, Z2[cc], __ffma2_rn(k_2, Zd2[cc], pm2[idx]));
                 }
             }
         }
+        float am[NN], a0[NN], a1[NN], a2[NN];
+#pragma unroll
+        for (int k = 0; k < NN; ++k) { am[k] = pm2[k].x; a2[k] = pm2[k].y; a0[k] = p01[k].x; a1[k] = p01[k].y; }
         float mx_m = 0.f, mx_p = 0.f;
 #pragma unroll
         for (int k = 0; k < NN; ++k) {
