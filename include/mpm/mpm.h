@@ -65,8 +65,9 @@ enum {
     MPM_FLAG_FIXED_POINT_OVERFLOW = 1u << 1,
     MPM_FLAG_PARTICLE_OUT_OF_DOMAIN = 1u << 2, /* a stencil reached outside the grid */
     MPM_FLAG_SVD_FP64_FALLBACK = 1u << 3,      /* informational: the FP64 SVD branch ran */
-    MPM_FLAG_TIMEOUT = 1u << 4                  /* reserved: no kernel of this library waits on the
-                                                   device (no spin on a flag or barrier), so none sets it */
+    MPM_FLAG_TIMEOUT = 1u << 4                  /* a bounded device-side wait gave up: the TMA node-box
+                                                   load of the fused transfer (MPM_BOX_LOAD=tma) did not
+                                                   arrive; that step's results are invalid */
 };
 
 typedef enum mpm_formulation {
@@ -190,8 +191,8 @@ MPM_API mpm_status mpm_rasterize(mpm_solver* solver, double* node_mass, double* 
 MPM_API mpm_status mpm_get_status(mpm_solver* solver, uint32_t* flags);
 
 /* The status word as an error code (synchronises): MPM_ERR_NAN_STATE,
- * MPM_ERR_FIXED_POINT_OVERFLOW or MPM_ERR_PARTICLE_OUT_OF_DOMAIN for the
- * first of those flags that is set, else MPM_OK (the informational FP64-SVD
+ * MPM_ERR_FIXED_POINT_OVERFLOW, MPM_ERR_PARTICLE_OUT_OF_DOMAIN or
+ * MPM_ERR_TIMEOUT for the first of those flags that is set, else MPM_OK (the informational FP64-SVD
  * flag is not an error); mpm_last_error names every flag set. This replaces
  * the reference's response to a non-finite stress, which prints and spins
  * forever (src/cpu/Particles.cpp:50-61): here the step completes, the flag

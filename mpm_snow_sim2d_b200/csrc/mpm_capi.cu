@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "mpm/mpm.h"
@@ -113,6 +114,8 @@ struct mpm_solver {
     bool fused = false;
     bool acc_pending = false;
     int fused_grid = 0;
+    bool box_tma = false;  // node boxes by TMA loads one tile ahead (MPM_BOX_LOAD=tma) instead of staged by the CTA
+    CUtensorMap gv_map{};  // the node velocities (vf, wall flag) as a [nz][ny][nx][4] float tensor for TMA
 };
 
 namespace {
@@ -420,8 +423,12 @@ template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
     if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
     if (e != cudaSuccess) return e;
     if (s->n == 0) return cudaSuccess;
-    k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
-        particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
+    if (G2P && s->box_tma)
+        k_g2p2g<D, S, G2P, true><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, 2>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status, s->gv_map);
+    else
+        k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
+            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status, s->gv_map);
     return cudaGetLastError();
 }
 
@@ -519,6 +526,36 @@ cudaError_t clear_after_p2g(mpm_solver* s) {
 }
 
 
+// The tensor map of the fused kernel's box loads: gv's first half (one float4
+// (vf, wall flag) per node) as a rank D+1 FP32 tensor [nz][ny][nx][4], boxes of
+// 4 x BE^D. The encoder comes from the driver through the runtime, so the
+// library needs no link to libcuda.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+mpm_status make_box_map(mpm_solver* s) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return fail(s, MPM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    }
+    const int D = s->dim;
+    const cuuint32_t rank = (cuuint32_t)(D + 1);
+    cuuint64_t dims[4] = {4, (cuuint64_t)s->C.nx, (cuuint64_t)s->C.ny, (cuuint64_t)s->C.nz};
+    cuuint64_t strides[3] = {16, 16ull * (cuuint64_t)s->C.nx, 16ull * (cuuint64_t)s->C.nx * (cuuint64_t)s->C.ny};
+    const cuuint32_t be = (cuuint32_t)(D == 3 ? FusedGeom<3>::BE : FusedGeom<2>::BE);
+    cuuint32_t box[4] = {4, be, be, be};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = reinterpret_cast<EncodeTiledFn>(fn)(
+        &s->gv_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, s->gv, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(s, MPM_ERR_CUDA, "cuTensorMapEncodeTiled failed for the node-velocity box");
+    return MPM_OK;
+}
+
 // Tiles, node-block marks and the sort's alternate buffers.
 mpm_status setup_tiled(mpm_solver* s) {
     const int D = s->dim, n = s->n;
@@ -586,25 +623,40 @@ mpm_status setup_tiled(mpm_solver* s) {
         s->fused = !(tr && std::strcmp(tr, "split") == 0);
     }
     if (s->fused) {
+        // MPM_BOX_LOAD=tma: node boxes by TMA tensor loads (same results)
+        const char* bl = std::getenv("MPM_BOX_LOAD");
+        s->box_tma = bl && std::strcmp(bl, "tma") == 0;
         const void* kfn;
-        size_t fsm;
+        size_t fsm, psm;
         const void* kpro;
         if (D == 3) {
-            kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
+            if (s->box_tma)
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, true> : (const void*)k_g2p2g<3, 4, true, true>;
+            else
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
             kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false> : (const void*)k_g2p2g<3, 4, false>;
-            fsm = sizeof(FusedSmem<3>);
+            fsm = s->box_tma ? sizeof(FusedSmem<3, 2>) : sizeof(FusedSmem<3>);
+            psm = sizeof(FusedSmem<3>);
         } else {
-            kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
+            if (s->box_tma)
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, true> : (const void*)k_g2p2g<2, 4, true, true>;
+            else
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
             kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false> : (const void*)k_g2p2g<2, 4, false>;
-            fsm = sizeof(FusedSmem<2>);
+            fsm = s->box_tma ? sizeof(FusedSmem<2, 2>) : sizeof(FusedSmem<2>);
+            psm = sizeof(FusedSmem<2>);
         }
         int per = 0;
         cudaError_t ef = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
-        if (ef == cudaSuccess) ef = cudaFuncSetAttribute(kpro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm);
+        if (ef == cudaSuccess) ef = cudaFuncSetAttribute(kpro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
         if (ef == cudaSuccess)
             ef = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, FusedGeom<3>::THREADS, fsm);
         if (ef != cudaSuccess || per < 1) return MPM_ERR_CUDA;
         s->fused_grid = s->sms * per;
+        if (s->box_tma) {
+            mpm_status em = make_box_map(s);
+            if (em != MPM_OK) return em;
+        }
     }
     s->sort_period = s->params.sort_period > 0 ? s->params.sort_period : 16;
     s->auto_sort = s->params.sort_period <= 0;

@@ -5,7 +5,11 @@
 // One CTA per non-empty cell tile of the last sort (tiles handed out from a
 // counter). The CTA stages the node velocities of a fixed box of BE^D nodes
 // around its tile in shared memory (the stencils of every particle sorted into
-// the tile that has since moved less than a cell). Then each warp, on its own,
+// the tile that has since moved less than a cell): by default all threads load
+// it; with TMA = true one thread issues a TMA tensor load
+// (cp.async.bulk.tensor, out-of-grid nodes zero-filled) of the CTA's next
+// tile's box while the current one is processed (two buffers, one mbarrier
+// each, waits bounded). Then each warp, on its own,
 // takes windows of 32 consecutive slots of the tile (handed out from a shared
 // counter) and for its window
 //   1. per particle (one lane each): gathers the grid from the box
@@ -35,6 +39,8 @@
 // themselves, so a resumed run never recomputes them.
 #pragma once
 
+#include <cuda.h>
+
 #include "mpm_tiled.cuh"
 
 namespace mpm {
@@ -46,6 +52,7 @@ template <int D> struct FusedGeom {
     static constexpr int T = TileGeom<D>::T;            // cells per tile edge: 4 (3D), 8 (2D)
     static constexpr int BE = T + 5;                    // box edge in nodes: tile nodes - 2 .. tile + T + 2
     static constexpr int BN = D == 3 ? BE * BE * BE : BE * BE;  // 729 (3D), 169 (2D)
+    static constexpr int BNP = (BN + 7) / 8 * 8;        // box rows padded to 128 bytes (TMA destinations)
     static constexpr int THREADS = MPM_FUSED_THREADS;
     static constexpr int WARPS = THREADS / 32;
     static constexpr int WIN = 32;                      // slots per warp window (one per lane)
@@ -54,13 +61,16 @@ template <int D> struct FusedGeom {
     static_assert(THREADS % 32 == 0, "whole warps");
 };
 
-template <int D> struct FusedSmem {
+// NB box buffers: 1 (staged by all threads) or 2 (TMA loads, one tile ahead).
+template <int D, int NB = 1> struct FusedSmem {
     using G = FusedGeom<D>;
-    float4 box[G::BN];                                  // 3D: (vf, wall flag); 2D: (vf, vc)
+    alignas(128) float4 box[NB][G::BNP];                // 3D: (vf, wall flag); 2D: (vf, vc)
+    unsigned long long bar[NB];                         // mbarrier of each box buffer's TMA load
+    int tile_next;                                      // the tile whose box is loading into the other buffer
+    int box_ok;                                         // the current box arrived
     float4 pay[G::WARPS][G::WIN * G::PS / 4];           // per warp: the window's P2G payloads
     int run[G::WARPS][G::WIN + 1];                      // per warp: start slot of each run, then the window end
     int order[G::WARPS][G::WIN];                        // per warp: runs, longest first
-    int tile;
     int next_win;                                       // next window of the tile to hand out
     unsigned bmask;                                     // node blocks (3^D around the tile) that received sums
 };
@@ -509,20 +519,87 @@ __global__ void __launch_bounds__(256) k_p2g_lone(Particles P, StepConsts C, Til
 }
 
 // ---------------------------------------------------------------------------
+// TMA load of a tile's node box and its mbarrier (sm_90+ PTX; one CTA, no
+// cluster multicast).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before
+// later async-proxy (TMA) writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Waits for the phase `parity` of the mbarrier to complete; false after
+// `limit` polls (each poll may suspend the thread for a short while).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit) {
+    const uint32_t a = smem_u32(bar);
+    for (int it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr int kBoxWaitPolls = 1 << 20;
+
+// The node box of tile t (origin node bo) into `dst`: one tensor load of the
+// node-velocity array viewed as [nz][ny][nx][4] floats (gv's first half);
+// nodes outside the grid read as zero. The mbarrier expects the box's bytes.
+template <int D>
+__device__ __forceinline__ void box_load(const CUtensorMap& map, const int* bo, float4* dst, unsigned long long* bar) {
+    constexpr uint32_t bytes = FusedGeom<D>::BN * sizeof(float4);
+    const uint32_t b = smem_u32(bar), d = smem_u32(dst);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    if constexpr (D == 3) {
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+            ::"r"(d), "l"(reinterpret_cast<uint64_t>(&map)), "r"(0), "r"(bo[0]), "r"(bo[1]), "r"(bo[2]), "r"(b)
+            : "memory");
+    } else {
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+            ::"r"(d), "l"(reinterpret_cast<uint64_t>(&map)), "r"(0), "r"(bo[0]), "r"(bo[1]), "r"(b)
+            : "memory");
+    }
+}
+
+// Tile coordinates and box origin node of tile t.
+template <int D>
+__device__ __forceinline__ void tile_origin(const TileInfo& TI, int t, int* tc, int* bo) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) { tc[k] = t % TI.tiles[k]; t /= TI.tiles[k]; bo[k] = tc[k] * FusedGeom<D>::T - 2; }
+}
+
+// ---------------------------------------------------------------------------
 // The fused kernel. G2P = true: one step (G2P of the state, then the next
 // step's P2G into `acc`). G2P = false: the P2G of the stored state only (after
 // creation or a state upload), reading B, F_E, J_p and forming A as every
-// other path does (mls_affine).
-template <int D, int S, bool G2P>
+// other path does (mls_affine). TMA (with G2P): the box arrives by TMA tensor
+// loads one tile ahead instead of being staged by the CTA's threads; same
+// box contents, same results.
+template <int D, int S, bool G2P, bool TMA = false>
 __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     k_g2p2g(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
-            SlowQueue Q, unsigned* __restrict__ status) {
+            SlowQueue Q, unsigned* __restrict__ status, const __grid_constant__ CUtensorMap gv_map) {
     using G = FusedGeom<D>;
     using W = WarpGeom<D, S>;
     using St = Stencil<S>;
     constexpr int T = G::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FusedSmem<D>& SM = *reinterpret_cast<FusedSmem<D>*>(smem_raw);
+    constexpr bool kTma = G2P && TMA;
+    extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destinations: 128-byte aligned
+    FusedSmem<D, kTma ? 2 : 1>& SM = *reinterpret_cast<FusedSmem<D, kTma ? 2 : 1>*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = P.n;
     const int ntl = *TI.n_tile_list;
@@ -530,31 +607,74 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     float4* pay = SM.pay[wid];
     int* run = SM.run[wid];
     int* order = SM.order[wid];
-    for (;;) {
+    int kbuf = 0;             // box buffer of the current tile
+    unsigned parity = 0u;     // bit k: phase of buffer k's next completion
+    if constexpr (kTma) {
         if (tid == 0) {
-            SM.tile = atomicAdd(TI.fused_next, 1);
-            SM.next_win = 0;
-            SM.bmask = 0u;
+            mbar_init(&SM.bar[0], 1);
+            mbar_init(&SM.bar[1], 1);
+            mbar_init_fence();
+            const int e0 = atomicAdd(TI.fused_next, 1);
+            SM.tile_next = e0;
+            if (e0 < ntl) {
+                int tc0[3], bo0[3];
+                tile_origin<D>(TI, TI.tile_list[e0], tc0, bo0);
+                box_load<D>(gv_map, bo0, SM.box[0], &SM.bar[0]);
+            }
         }
-        __syncthreads();  // also: every warp is done with the previous tile's box
-        const int e = SM.tile;
-        if (e >= ntl) break;
+        __syncthreads();
+    }
+    for (;;) {
+        int e;
+        if constexpr (kTma) {
+            e = SM.tile_next;
+            __syncthreads();  // every thread has read it, and every warp is done with the other buffer
+            if (e >= ntl) break;
+            if (tid == 0) {
+                SM.next_win = 0;
+                SM.bmask = 0u;
+                // the next tile's box into the other buffer, then wait for this one's
+                const int e1 = atomicAdd(TI.fused_next, 1);
+                SM.tile_next = e1;
+                if (e1 < ntl) {
+                    int tc1[3], bo1[3];
+                    tile_origin<D>(TI, TI.tile_list[e1], tc1, bo1);
+                    fence_proxy_async_smem();
+                    box_load<D>(gv_map, bo1, SM.box[kbuf ^ 1], &SM.bar[kbuf ^ 1]);
+                }
+                SM.box_ok = mbar_wait(&SM.bar[kbuf], (parity >> kbuf) & 1u, kBoxWaitPolls);
+                if (!SM.box_ok) {
+                    // give up (flagged); let the other load land before the CTA leaves
+                    raise_flag(status, 16u);
+                    if (e1 < ntl) mbar_wait(&SM.bar[kbuf ^ 1], (parity >> (kbuf ^ 1)) & 1u, kBoxWaitPolls);
+                }
+            }
+            __syncthreads();
+            if (!SM.box_ok) return;
+            parity ^= 1u << kbuf;
+        } else {
+            if (tid == 0) {
+                SM.tile_next = atomicAdd(TI.fused_next, 1);
+                SM.next_win = 0;
+                SM.bmask = 0u;
+            }
+            __syncthreads();
+            e = SM.tile_next;
+            if (e >= ntl) break;
+        }
+        const float4* box = SM.box[kTma ? kbuf : 0];
         const int t = TI.tile_list[e];
         const int start = TI.tile_start[t], m = TI.tile_len[e];
         int tc[3] = {0, 0, 0}, bo[3] = {0, 0, 0};  // tile coordinates, box origin node
-        {
-            int r = t;
-#pragma unroll
-            for (int k = 0; k < D; ++k) { tc[k] = r % TI.tiles[k]; r /= TI.tiles[k]; bo[k] = tc[k] * T - 2; }
-        }
-        if constexpr (G2P) {  // stage the node velocities of the box
+        tile_origin<D>(TI, t, tc, bo);
+        if constexpr (G2P && !TMA) {  // stage the node velocities of the box
             for (int l = tid; l < G::BN; l += G::THREADS) {
                 const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
                 const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (gx >= 0 && gx <= C.W && gy >= 0 && gy <= C.H && (D == 2 || (gz >= 0 && gz <= C.Dp)))
                     v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
-                SM.box[l] = v;
+                SM.box[0][l] = v;
             }
             __syncthreads();
         }
@@ -603,7 +723,7 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                         if (boxed) {
                             const int l0 = (D == 3 ? (base[2] - bo[2]) * G::BE * G::BE : 0) + (base[1] - bo[1]) * G::BE +
                                            (base[0] - bo[0]);
-                            gather_nodes<D, S, true, int>(C, SM.box, l0, G::BE, G::BE * G::BE, gv, gc0, gsy, gsz, wk, off,
+                            gather_nodes<D, S, true, int>(C, box, l0, G::BE, G::BE * G::BE, gv, gc0, gsy, gsz, wk, off,
                                                           nv, nB, nx);
                         } else {
                             gather_nodes<D, S, false, long long>(C, gv, gc0, gsy, gsz, gv, gc0, gsy, gsz, wk, off, nv, nB,
@@ -705,7 +825,8 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             const int bx = tc[0] - 1 + rx, by = tc[1] - 1 + ry, bz = D == 3 ? tc[2] - 1 + rz : 0;
             mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
         }
-        __syncthreads();  // SM.bmask is reset for the next tile
+        kbuf ^= 1;
+        if constexpr (!kTma) __syncthreads();  // SM.bmask, the tile and the box are reset for the next tile
     }
 }
 

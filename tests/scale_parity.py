@@ -71,14 +71,15 @@ def run_gpu(args):
 
 
 def contact_band(scene, position):
-    """Particles with a stencil node within two cells of a wall plane."""
+    """Particles with a cubic-stencil node (floor(x) - 1 .. floor(x) + 2)
+    within two cells of a wall plane (x = m and x = extent - m)."""
     d = scene.dim
     ext = np.array([scene.width, scene.height, scene.depth][:d], np.float64)
     m = float(scene.border_margin)
     p = np.asarray(position, np.float64)
     near = np.zeros(p.shape[0], bool)
     for k in range(d):
-        near |= (p[:, k] < m + 3.0) | (p[:, k] > ext[k] - m - 3.0)
+        near |= (p[:, k] < m + 4.0) | (p[:, k] >= ext[k] - m - 4.0)
     return near
 
 
