@@ -13,6 +13,10 @@ bit-deterministic, so its final state can also be written in pieces:
     python tests/scale_parity.py gpu     --workload c3 --steps 1000 --fields position,velocity --out DIR
     python tests/scale_parity.py compare --workload c3 --steps 1000 --oracle DIR --gpu DIR [DIR ...]
 
+or, with the oracle's files copied to the GPU machine, in one go:
+
+    python tests/scale_parity.py gpu --workload c3 --steps 1000 --compare-with DIR --json report.json
+
 Reported: relative L2 over all particles of x, v, B (normalised by |v|), F_E
 and J_p, overall and split into particles inside the wall-contact band (a
 stencil node within two cells of a wall plane: the nodes where the predictive
@@ -58,12 +62,25 @@ def run_oracle(args):
 def run_gpu(args):
     from mpm_snow_sim2d_b200 import Solver
     sc = _scene(args.workload)
-    out = Path(args.out)
-    out.mkdir(parents=True, exist_ok=True)
+    t0 = time.time()
     with Solver.from_scene(sc) as s:
         s.Step(args.steps)
         st = s.get_state()
         flags = s.status()
+    gpu_s = time.time() - t0
+    if args.compare_with:
+        # compare on this machine against the oracle's files; keep only the report
+        od = Path(args.compare_with)
+        ref = dict(np.load(od / f"{args.workload}_{args.steps}_fp64.npz"))
+        r32 = dict(np.load(od / f"{args.workload}_{args.steps}_fp32.npz"))
+        res = report(sc, args.steps, {f: getattr(st, f) for f in FIELDS}, flags, ref, r32)
+        res["gpu_wall_s"] = round(gpu_s, 2)
+        print(json.dumps(res, indent=1))
+        if args.json:
+            Path(args.json).write_text(json.dumps(res, indent=1))
+        return
+    out = Path(args.out)
+    out.mkdir(parents=True, exist_ok=True)
     fields = args.fields.split(",")
     np.savez(out / f"{args.workload}_{args.steps}_gpu_{'_'.join(fields)}.npz", flags=np.uint32(flags),
              **{f: getattr(st, f) for f in fields})
@@ -109,15 +126,20 @@ def compare(args):
     missing = [f for f in FIELDS if f not in gpu]
     if missing:
         raise SystemExit(f"GPU fields missing: {missing}")
+    res = report(sc, args.steps, gpu, flags, ref, r32)
+    print(json.dumps(res, indent=1))
+    if args.json:
+        Path(args.json).write_text(json.dumps(res, indent=1))
+
+
+def report(sc, steps, gpu, flags, ref, r32):
     band = contact_band(sc, ref["position"])
-    res = {"workload": args.workload, "particles": sc.count, "steps": args.steps, "gpu_status_flags": flags,
+    res = {"workload": sc.name, "particles": sc.count, "steps": steps, "gpu_status_flags": int(flags),
            "contact_particles": int(band.sum()), "free_particles": int((~band).sum())}
     for name, a, base in (("gpu_vs_fp64", gpu, ref), ("reference_fp32_vs_fp64", r32, ref),
                           ("gpu_vs_reference_fp32", gpu, r32)):
         res[name] = {"all": errors(a, base), "contact": errors(a, base, band), "free": errors(a, base, ~band)}
-    print(json.dumps(res, indent=1))
-    if args.json:
-        Path(args.json).write_text(json.dumps(res, indent=1))
+    return res
 
 
 def main():
@@ -132,7 +154,9 @@ def main():
             p.add_argument("--out", required=True)
         elif name == "gpu":
             p.add_argument("--fields", default=",".join(FIELDS))
-            p.add_argument("--out", required=True)
+            p.add_argument("--out", help="write the final state's fields here")
+            p.add_argument("--compare-with", help="oracle directory: compare on this machine, write only the report")
+            p.add_argument("--json")
         else:
             p.add_argument("--oracle", required=True)
             p.add_argument("--gpu", nargs="+", required=True)
