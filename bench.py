@@ -226,7 +226,7 @@ def mlp_vs_plain(args, torch, stream):
     from mpm_snow_sim2d_b200 import Solver, _lib
     from mpm_snow_sim2d_b200.mlp import DEFAULT_WEIGHTS, Mlp
     scene = make_scene(args.mlp_workload)
-    net = Mlp.load(DEFAULT_WEIGHTS)
+    net = Mlp.load(args.mlp_weights or DEFAULT_WEIGHTS)
     rng = np.random.Generator(np.random.PCG64(99))
     solvers = {}
     for mode in ("exact", "mlp", "control"):
@@ -469,6 +469,8 @@ def main():
     ap.add_argument("--mlp-workload", default="c5", choices=sorted(WORKLOADS))
     ap.add_argument("--mlp-steps", type=int, default=1000)
     ap.add_argument("--mlp-tolerance", type=float, default=1e-3)
+    ap.add_argument("--mlp-weights", default=None, help="network weights (.npz) for the learned return map "
+                    "(default: the shipped ones)")
     ap.add_argument("--no-mlp", action="store_true", help="skip the learned-plasticity comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes measurement")
     ap.add_argument("--batch-scenes", type=int, default=256)

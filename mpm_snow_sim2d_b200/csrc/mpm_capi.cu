@@ -190,7 +190,7 @@ void release(mpm_solver* s) {
     if (s->q.list) cudaFree(s->q.list);
     if (s->q.count) cudaFree(s->q.count);
     if (s->q.fh) cudaFree(s->q.fh);
-    if (s->q.slot) cudaFree(s->q.slot);
+    if (s->q.win) cudaFree(s->q.win);
     if (s->ti.tile_len) cudaFree(s->ti.tile_len);
     if (s->ti.fused_next) cudaFree(s->ti.fused_next);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -420,7 +420,7 @@ template <int D, int S> cudaError_t launch_p2g_tiled(mpm_solver* s) {
 // step), or with G2P = false the P2G of the stored state (prologue).
 template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
     cudaError_t e = cudaMemsetAsync(s->ti.fused_next, 0, sizeof(int), s->stream);
-    if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, sizeof(int), s->stream);
+    if (e == cudaSuccess && G2P) e = cudaMemsetAsync(s->q.count, 0, 2 * sizeof(int), s->stream);  // count, nwin
     if (e != cudaSuccess) return e;
     if (s->n == 0) return cudaSuccess;
     if (G2P && s->box_tma)
@@ -433,12 +433,14 @@ template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
 }
 
 // Queued particles after the G2P part: their return map (learned and/or
-// exact), then their P2G for the next step one by one.
+// exact), then their P2G for the next step by the windows the fused kernel
+// recorded.
 template <int D, int S> cudaError_t launch_queued_fused(mpm_solver* s) {
     if (s->n == 0) return cudaSuccess;
     cudaError_t e = launch_return_map<D, S>(s);
     if (e != cudaSuccess) return e;
-    k_p2g_lone<D, S><<<s->sms * 4, 256, 0, s->stream>>>(particle_view(s), s->C, s->ti, s->q, s->acc, s->status);
+    k_p2g_windows<D, S><<<s->fused_grid, FusedGeom<D>::THREADS, 0, s->stream>>>(particle_view(s), s->C, s->ti, s->q,
+                                                                                s->acc, s->status);
     return cudaGetLastError();
 }
 
@@ -611,12 +613,15 @@ mpm_status setup_tiled(mpm_solver* s) {
         s->p2g_warp_grid = s->sms * per;
     }
     s->q.capacity = n > 0 ? n : 1;
-    if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 1) ||
-        dalloc(&s->q.fh, (size_t)s->q.capacity * D * D) || dalloc(&s->q.slot, (size_t)s->q.capacity) ||
+    // windows of a sort: at most ceil(m / 32) per tile of m slots
+    s->q.win_capacity = s->q.capacity / 32 + ti.n_tiles + 1;
+    if (dalloc(&s->q.list, (size_t)s->q.capacity) || dalloc(&s->q.count, 2) ||
+        dalloc(&s->q.fh, (size_t)s->q.capacity * D * D) || dalloc(&s->q.win, (size_t)s->q.win_capacity) ||
         dalloc(&ti.tile_len, (size_t)ti.n_tiles) || dalloc(&ti.fused_next, 1)) {
         cudaGetLastError();
         return MPM_ERR_OUT_OF_MEMORY;
     }
+    s->q.nwin = s->q.count + 1;
     {
         // MPM_TRANSFER=split selects the separate P2G / G2P kernels (for comparison)
         const char* tr = std::getenv("MPM_TRANSFER");

@@ -28,8 +28,9 @@
 // particles or a long run holds up no other. Particles whose stencil leaves
 // the box (drifted more than a cell since the sort) gather from global memory
 // and their runs add bounds-checked. Queued particles (out of the elastic
-// band, or a stencil clipped by the grid edge) are scattered one by one after
-// their return map (k_p2g_lone).
+// band, or a stencil clipped by the grid edge) are scattered after their
+// return map: the warp records its window (first slot, mask of the queued
+// lanes), and k_p2g_windows repeats the window's run scatter over those lanes.
 //
 // Determinism: every cross-run sum is an integer add, and the runs are a
 // function of the slot order, the window boundaries (fixed offsets inside a
@@ -242,14 +243,14 @@ __device__ __forceinline__ unsigned long long p2g_payload(const StepConsts& C, c
 // ---------------------------------------------------------------------------
 // One work item of the run accumulation: split `a` of the run [j0, j1) of a
 // warp's payload window `pay`, stencil key kk. Sums in registers in slot
-// order and adds them to the global grid as int64 fixed point. When the whole
-// stencil lies in the tile's node box and in the grid the adds need no bounds
-// checks and the function returns the node blocks they touched, as bits of
-// the 3^D blocks around the tile (tile coordinates tc); otherwise the adds
-// are bounds-checked, the node blocks marked here, and it returns 0. Same
-// arithmetic as k_p2g_warp.
+// order and adds them to the global grid as int64 fixed point. When `boxed`
+// and the whole stencil lies in the tile's node box (origin bo) and in the
+// grid, the adds need no bounds checks and the function returns the node
+// blocks they touched, as bits of the 3^D blocks around the tile (tile
+// coordinates tc); otherwise the adds are bounds-checked, the node blocks
+// marked here, and it returns 0. Same arithmetic as k_p2g_warp.
 template <int D, int S>
-__device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInfo& TI, const float4* pay,
+__device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInfo& TI, const float4* pay, bool boxed,
                                               const int* bo, const int* tc, int j0, int j1, unsigned long long kk,
                                               int a, unsigned long long* __restrict__ acc,
                                               unsigned* __restrict__ status) {
@@ -261,7 +262,7 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
 #pragma unroll
     for (int k = 0; k < D; ++k) cell[k] = int((kk >> (StencilKey<D>::BITS * k)) & StencilKey<D>::MASK) - 8;
     // stencil nodes cell - 1 .. cell + S - 2 per axis
-    bool in_box = true, in_grid = true;
+    bool in_box = boxed, in_grid = true;
     const int ext[3] = {C.W, C.H, C.Dp};
 #pragma unroll
     for (int k = 0; k < D; ++k) {
@@ -453,68 +454,93 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
 }
 
 // ---------------------------------------------------------------------------
-// One particle's P2G contribution to one stencil node, added on its own (no
-// grouping): the path of queued particles.
+// The scatter of one warp's window of payloads (`pay`, stencil keys in the
+// last two floats of each; kNoStencil for slots that add nothing): runs of
+// consecutive slots with one key, longest first, SPLIT lanes per run summing
+// it (fused_run). `cnt` slots of the window are filled. Returns this lane's
+// node-block bits (boxed runs only).
 template <int D, int S>
-__device__ __forceinline__ void lone_node(const StepConsts& C, const TileInfo& TI, const float* x, const float* mv,
-                                          const float* A, float mass, int node, unsigned long long* __restrict__ acc,
-                                          unsigned* __restrict__ status) {
-    using St = Stencil<S>;
-    constexpr int T = TileGeom<D>::T;
-    const int ext[3] = {C.W, C.H, C.Dp};
-    int g[3] = {0, 0, 0};
-    float w = 1.f, d[3] = {0.f, 0.f, 0.f};
-    int rem = node;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-        const int o = rem % S;
-        rem /= S;
-        const int base = St::base(x[k], ext[k]);
-        float wt[S];
-        St::weights(x[k], base, wt);
-        w *= pick<S>(wt, o);
-        g[k] = base + o;
-        d[k] = float(g[k]) - x[k];
+__device__ __forceinline__ unsigned scatter_window(const StepConsts& C, const TileInfo& TI, const float4* pay,
+                                                   int* run, int* order, int cnt, bool boxed, const int* bo,
+                                                   const int* tc, unsigned long long* __restrict__ acc,
+                                                   unsigned* __restrict__ status) {
+    using G = FusedGeom<D>;
+    using W = WarpGeom<D, S>;
+    const int lane = threadIdx.x & 31;
+    const bool valid = lane < cnt;
+    // runs: maximal stretches of consecutive slots with one stencil key
+    const unsigned long long* keyp = reinterpret_cast<const unsigned long long*>(
+        reinterpret_cast<const float*>(pay) + G::KEYF);
+    auto key_at = [&](int j) { return keyp[j * (G::PS / 2)]; };
+    const bool is_start = valid && (lane == 0 || key_at(lane) != key_at(lane - 1));
+    const unsigned starts = __ballot_sync(0xffffffffu, is_start);
+    const int nruns = __popc(starts);
+    const int r_me = __popc(starts & ((1u << lane) - 1));
+    if (is_start) run[r_me] = lane;
+    if (lane == 0) run[nruns] = cnt;
+    __syncwarp();
+    // runs longest first, so that the SPLIT-lane groups sharing a pass have
+    // similar lengths; which lanes sum a run changes no result
+    {
+        const int len = lane < nruns ? run[lane + 1] - run[lane] : 0;
+        int rank = 0;
+        for (int qr = 0; qr < nruns; ++qr) {
+            const int lq = __shfl_sync(0xffffffffu, len, qr);
+            rank += lq > len || (lq == len && qr < lane);
+        }
+        if (lane < nruns) order[rank] = lane;
     }
-    if (g[0] < 0 || g[0] > C.W || g[1] < 0 || g[1] > C.H || (D == 3 && (g[2] < 0 || g[2] > C.Dp))) {
-        raise_flag(status, 4u);
-        return;
+    __syncwarp();
+    unsigned bits = 0u;
+    for (int u = lane; u < nruns * W::SPLIT; u += 32) {
+        const int r = order[u / W::SPLIT], a = u % W::SPLIT;
+        const int j0 = run[r], j1 = run[r + 1];
+        const unsigned long long kk = key_at(j0);
+        if (kk == kNoStencil) continue;
+        bits |= fused_run<D, S>(C, TI, pay, boxed, bo, tc, j0, j1, kk, a, acc, status);
     }
-    const long long id = ((long long)g[2] * C.ny + g[1]) * C.nx + g[0];
-    red_add(&acc[id], to_fixed(w * mass, C.sm, status));
-#pragma unroll
-    for (int r = 0; r < D; ++r) {
-        float s = mv[r];
-#pragma unroll
-        for (int k = 0; k < D; ++k) s += A[r * D + k] * d[k];
-        red_add(&acc[(1 + r) * C.nodes + id], to_fixed(w * s, C.sp, status));
-    }
-    const int b = D == 3 ? ((g[2] / T) * TI.nblk[1] + g[1] / T) * TI.nblk[0] + g[0] / T : (g[1] / T) * TI.nblk[0] + g[0] / T;
-    mark_block_once(TI, b);
+    __syncwarp();  // the window's payload and runs are reused by the next window
+    return bits;
 }
 
-// P2G of the queued particles after their return map: (particle, node) per
-// thread; x, v, A as the G2P and return-map kernels left them.
+// P2G of the queued particles after their return map, by the windows the
+// fused kernel recorded: one warp per window, the window's queued slots
+// (x, v, A as the G2P and return-map kernels left them) grouped into runs of
+// one stencil and summed as in the fused kernel. The grouping is a function
+// of the window and of which of its particles were queued, so the int64 sums
+// do not depend on the order in which windows were recorded.
 template <int D, int S>
-__global__ void __launch_bounds__(256) k_p2g_lone(Particles P, StepConsts C, TileInfo TI, SlowQueue Q,
-                                                  unsigned long long* __restrict__ acc, unsigned* __restrict__ status) {
-    constexpr int NN = D == 3 ? S * S * S : S * S;
-    constexpr int PER = 256 / NN;
-    const int m = *Q.count;
-    const int node = threadIdx.x % NN, sub = threadIdx.x / NN;
-    if (sub >= PER) return;
+__global__ void __launch_bounds__(FusedGeom<D>::THREADS) k_p2g_windows(Particles P, StepConsts C, TileInfo TI,
+                                                                      SlowQueue Q,
+                                                                      unsigned long long* __restrict__ acc,
+                                                                      unsigned* __restrict__ status) {
+    using G = FusedGeom<D>;
+    __shared__ float4 pay_s[G::WARPS][G::WIN * G::PS / 4];
+    __shared__ int run_s[G::WARPS][G::WIN + 1];
+    __shared__ int order_s[G::WARPS][G::WIN];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = min(*Q.nwin, Q.win_capacity);
     const int n = P.n;
-    for (int e = blockIdx.x * PER + sub; e < m; e += gridDim.x * PER) {
-        const int i = Q.slot[e];
-        const float mass = P.mass ? P.mass[i] : P.mass_u;
-        const float vol = P.vol ? P.vol[i] : P.vol_u;
-        if (vol == 0.f) continue;
-        float x[D], mv[D], A[D * D];
+    const int none[3] = {0, 0, 0};
+    float4* pay = pay_s[wid];
+    for (int r = blockIdx.x * G::WARPS + wid; r < nw; r += gridDim.x * G::WARPS) {
+        const int2 rec = Q.win[r];
+        const unsigned mask = (unsigned)rec.y;
+        float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
+        unsigned long long key = kNoStencil;
+        if ((mask >> lane) & 1u) {
+            const int i = rec.x + lane;
+            const float mass = P.mass ? P.mass[i] : P.mass_u;
+            float x[D], v[D], A[D * D];
 #pragma unroll
-        for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; mv[k] = mass * P.v[k * n + i]; }
+            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
 #pragma unroll
-        for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
-        lone_node<D, S>(C, TI, x, mv, A, mass, node, acc, status);
+            for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
+            key = p2g_payload<D, S>(C, x, v, A, mass, q);
+        }
+        reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
+        __syncwarp();
+        scatter_window<D, S>(C, TI, pay, run_s[wid], order_s[wid], 32 - __clz(mask), false, none, none, acc, status);
     }
 }
 
@@ -689,6 +715,7 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             const bool valid = lane < cnt;
             const int i = start + w * G::WIN + lane;
             unsigned long long key = kNoStencil;
+            bool deferred = false;  // queued: scattered after the return map (k_p2g_windows)
             float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
             if (valid) {
                 const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
@@ -713,9 +740,8 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                     }
                     if (!interior) {
                         // stencil partly outside the grid: the general kernel does the whole G2P
-                        const int slot = queue_slot(Q);
-                        Q.list[slot] = -1 - i;
-                        Q.slot[slot] = i;
+                        Q.list[queue_slot(Q)] = -1 - i;
+                        deferred = scatter;
                         scatter = false;
                     } else {
                         float nv[D], nx[D], nB[D * D];
@@ -765,9 +791,9 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                         } else {
                             const int slot = queue_slot(Q);
                             Q.list[slot] = i;
-                            Q.slot[slot] = i;
 #pragma unroll
                             for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
+                            deferred = scatter;
                             scatter = false;
                         }
                     }
@@ -781,39 +807,17 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                 }
                 if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
             }
+            if constexpr (G2P) {
+                // record the window if some of its particles wait for the return map
+                const unsigned dm = __ballot_sync(0xffffffffu, deferred);
+                if (dm && lane == 0) {
+                    const int r = atomicAdd(Q.nwin, 1);
+                    if (r < Q.win_capacity) Q.win[r] = make_int2(start + w * G::WIN, (int)dm);
+                }
+            }
             reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
             __syncwarp();
-            // runs: maximal stretches of consecutive slots with one stencil key
-            const unsigned long long* keyp = reinterpret_cast<const unsigned long long*>(
-                reinterpret_cast<const float*>(pay) + G::KEYF);
-            auto key_at = [&](int j) { return keyp[j * (G::PS / 2)]; };
-            const bool is_start = valid && (lane == 0 || key_at(lane) != key_at(lane - 1));
-            const unsigned starts = __ballot_sync(0xffffffffu, is_start);
-            const int nruns = __popc(starts);
-            const int r_me = __popc(starts & ((1u << lane) - 1));
-            if (is_start) run[r_me] = lane;
-            if (lane == 0) run[nruns] = cnt;
-            __syncwarp();
-            // runs longest first, so that the SPLIT-lane groups sharing a pass
-            // have similar lengths; which lanes sum a run changes no result
-            {
-                const int len = lane < nruns ? run[lane + 1] - run[lane] : 0;
-                int rank = 0;
-                for (int qr = 0; qr < nruns; ++qr) {
-                    const int lq = __shfl_sync(0xffffffffu, len, qr);
-                    rank += lq > len || (lq == len && qr < lane);
-                }
-                if (lane < nruns) order[rank] = lane;
-            }
-            __syncwarp();
-            for (int u = lane; u < nruns * W::SPLIT; u += 32) {
-                const int r = order[u / W::SPLIT], a = u % W::SPLIT;
-                const int j0 = run[r], j1 = run[r + 1];
-                const unsigned long long kk = key_at(j0);
-                if (kk == kNoStencil) continue;
-                bits |= fused_run<D, S>(C, TI, pay, bo, tc, j0, j1, kk, a, acc, status);
-            }
-            __syncwarp();  // the window's payload and runs are reused by the next window
+            bits |= scatter_window<D, S>(C, TI, pay, run, order, cnt, true, bo, tc, acc, status);
         }
         // mark the node blocks the tile's in-box runs added to
         bits = __reduce_or_sync(0xffffffffu, bits);

@@ -613,8 +613,12 @@ struct SlowQueue {
     int* list;    // slots needing the full return map
     int* count;   // device scalar
     float* fh;    // trial F per queue entry, [D*D][capacity]
-    int* slot;    // fused path: the particle slot of each entry (kept when the entry is marked done)
     int capacity;
+    // fused path: the 32-slot windows holding queued particles, as (first
+    // slot, lane mask of the queued slots); their P2G runs after the return map
+    int2* win;
+    int* nwin;    // device scalar (count[1])
+    int win_capacity;
 };
 
 // Element a of an S-vector held in registers, for a loop index the compiler

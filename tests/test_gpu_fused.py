@@ -1,7 +1,7 @@
 """The fused transfer (G2P of a step and the next step's P2G in one kernel per
 cell tile) against the split kernels and itself: same results to FP32
 rounding, bit-identical resume from a checkpoint taken while particles are on
-the one-by-one scatter path, and pending grid sums equal to a fresh P2G of the
+the queued-window scatter path, and pending grid sums equal to a fresh P2G of the
 same state. The oracle parity tests in test_gpu_parity.py run the fused path
 (the default) as well."""
 import os
@@ -45,10 +45,14 @@ def _scenes():
         "blocks2d": (scenes.snow_blocks_2d(), 300),
         "impact3d_quad": (scenes.impact_3d().with_(**quad), 150),
         "impact2d_quad": (scenes.impact_2d().with_(**quad), 150),
+        # two snowballs through their collision: most particles leave the
+        # elastic band and take the queued-window scatter
+        "collide3d": (scenes.two_snowballs_3d(W=64, ppc=2), 400),
     }
 
 
-@pytest.mark.parametrize("case", ["impact2d", "impact3d", "slab3d", "blocks2d", "impact3d_quad", "impact2d_quad"])
+@pytest.mark.parametrize("case", ["impact2d", "impact3d", "slab3d", "blocks2d", "impact3d_quad", "impact2d_quad",
+                                  "collide3d"])
 def test_fused_matches_split(gpu_lib, case):
     """The two transfers differ only in how P2G groups particles before its
     int64 adds (FP32 partial sums over different runs), so they agree to a
@@ -61,6 +65,18 @@ def test_fused_matches_split(gpu_lib, case):
     print(case, ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     assert errs["position"] < 2e-6 and errs["elastic_f"] < 2e-5 and errs["plastic_det"] < 2e-5
     assert errs["velocity"] < 5e-4  # relative to near-zero velocities after contact
+
+
+def test_queued_windows_bitwise(gpu_lib):
+    """The queued particles' scatter groups them by the window the fused
+    kernel recorded, in whatever order the windows were recorded: two runs
+    through the collision (most particles queued) are bit-identical."""
+    sc, steps = _scenes()["collide3d"]
+    a, fa = _run(sc, steps, "fused")
+    b, fb = _run(sc, steps, "fused")
+    assert fa & 1 == 0 and fa == fb
+    for f in FIELDS:
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
 
 
 @pytest.mark.parametrize("case", ["impact2d", "slab3d", "impact3d_quad", "impact2d_quad"])
@@ -82,7 +98,7 @@ def test_tma_box_load(gpu_lib, case):
 
 def test_fused_resume_is_bitwise(gpu_lib, tmp_path):
     """Checkpoints taken right after the first step, after a sort and while
-    out-of-band particles take the one-by-one scatter: the resumed run restores
+    out-of-band particles take the queued-window scatter: the resumed run restores
     the tiles of the last sort and the pending grid sums and continues bit for
     bit."""
     from mpm_snow_sim2d_b200 import Solver, scenes
