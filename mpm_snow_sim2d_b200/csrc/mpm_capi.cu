@@ -114,7 +114,7 @@ struct mpm_solver {
     bool fused = false;
     bool acc_pending = false;
     int fused_grid = 0;
-    bool box_tma = false;  // node boxes by TMA loads one tile ahead (MPM_BOX_LOAD=tma) instead of staged by the CTA
+    bool box_tma = false;  // fused step as the TMA box pipeline (MPM_BOX_LOAD=tma) instead of staged boxes
     CUtensorMap gv_map{};  // the node velocities (vf, wall flag) as a [nz][ny][nx][4] float tensor for TMA
 };
 
@@ -424,11 +424,11 @@ template <int D, int S, bool G2P> cudaError_t launch_fused(mpm_solver* s) {
     if (e != cudaSuccess) return e;
     if (s->n == 0) return cudaSuccess;
     if (G2P && s->box_tma)
-        k_g2p2g<D, S, G2P, true><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D, 2>), s->stream>>>(
+        k_g2p2g_pipe<D, S><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(PipeSmem<D>), s->stream>>>(
             particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status, s->gv_map);
     else
         k_g2p2g<D, S, G2P><<<s->fused_grid, FusedGeom<D>::THREADS, sizeof(FusedSmem<D>), s->stream>>>(
-            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status, s->gv_map);
+            particle_view(s), s->C, s->ti, s->gv, s->acc, s->q, s->status);
     return cudaGetLastError();
 }
 
@@ -636,19 +636,19 @@ mpm_status setup_tiled(mpm_solver* s) {
         const void* kpro;
         if (D == 3) {
             if (s->box_tma)
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true, true> : (const void*)k_g2p2g<3, 4, true, true>;
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g_pipe<3, 3> : (const void*)k_g2p2g_pipe<3, 4>;
             else
                 kfn = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, true> : (const void*)k_g2p2g<3, 4, true>;
             kpro = s->stencil == 3 ? (const void*)k_g2p2g<3, 3, false> : (const void*)k_g2p2g<3, 4, false>;
-            fsm = s->box_tma ? sizeof(FusedSmem<3, 2>) : sizeof(FusedSmem<3>);
+            fsm = s->box_tma ? sizeof(PipeSmem<3>) : sizeof(FusedSmem<3>);
             psm = sizeof(FusedSmem<3>);
         } else {
             if (s->box_tma)
-                kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true, true> : (const void*)k_g2p2g<2, 4, true, true>;
+                kfn = s->stencil == 3 ? (const void*)k_g2p2g_pipe<2, 3> : (const void*)k_g2p2g_pipe<2, 4>;
             else
                 kfn = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, true> : (const void*)k_g2p2g<2, 4, true>;
             kpro = s->stencil == 3 ? (const void*)k_g2p2g<2, 3, false> : (const void*)k_g2p2g<2, 4, false>;
-            fsm = s->box_tma ? sizeof(FusedSmem<2, 2>) : sizeof(FusedSmem<2>);
+            fsm = s->box_tma ? sizeof(PipeSmem<2>) : sizeof(FusedSmem<2>);
             psm = sizeof(FusedSmem<2>);
         }
         int per = 0;

@@ -5,11 +5,10 @@
 // One CTA per non-empty cell tile of the last sort (tiles handed out from a
 // counter). The CTA stages the node velocities of a fixed box of BE^D nodes
 // around its tile in shared memory (the stencils of every particle sorted into
-// the tile that has since moved less than a cell): by default all threads load
-// it; with TMA = true one thread issues a TMA tensor load
-// (cp.async.bulk.tensor, out-of-grid nodes zero-filled) of the CTA's next
-// tile's box while the current one is processed (two buffers, one mbarrier
-// each, waits bounded). Then each warp, on its own,
+// the tile that has since moved less than a cell): in k_g2p2g all threads load
+// it between two CTA barriers; k_g2p2g_pipe (MPM_BOX_LOAD=tma) instead runs a
+// two-stage pipeline of TMA tensor loads (cp.async.bulk.tensor, out-of-grid
+// nodes zero-filled) with mbarriers and no CTA barrier. Then each warp, on its own,
 // takes windows of 32 consecutive slots of the tile (handed out from a shared
 // counter) and for its window
 //   1. per particle (one lane each): gathers the grid from the box
@@ -62,13 +61,10 @@ template <int D> struct FusedGeom {
     static_assert(THREADS % 32 == 0, "whole warps");
 };
 
-// NB box buffers: 1 (staged by all threads) or 2 (TMA loads, one tile ahead).
-template <int D, int NB = 1> struct FusedSmem {
+template <int D> struct FusedSmem {
     using G = FusedGeom<D>;
-    alignas(128) float4 box[NB][G::BNP];                // 3D: (vf, wall flag); 2D: (vf, vc)
-    unsigned long long bar[NB];                         // mbarrier of each box buffer's TMA load
-    int tile_next;                                      // the tile whose box is loading into the other buffer
-    int box_ok;                                         // the current box arrived
+    float4 box[G::BN];                                  // 3D: (vf, wall flag); 2D: (vf, vc)
+    int tile_next;                                      // tile-list entry of the CTA's current tile
     float4 pay[G::WARPS][G::WIN * G::PS / 4];           // per warp: the window's P2G payloads
     int run[G::WARPS][G::WIN + 1];                      // per warp: start slot of each run, then the window end
     int order[G::WARPS][G::WIN];                        // per warp: runs, longest first
@@ -580,6 +576,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 }
 constexpr int kBoxWaitPolls = 1 << 20;
 
+// One arrival on the mbarrier (release at CTA scope).
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // The node box of tile t (origin node bo) into `dst`: one tensor load of the
 // node-velocity array viewed as [nz][ny][nx][4] floats (gv's first half);
 // nodes outside the grid read as zero. The mbarrier expects the box's bytes.
@@ -609,98 +610,171 @@ __device__ __forceinline__ void tile_origin(const TileInfo& TI, int t, int* tc, 
 }
 
 // ---------------------------------------------------------------------------
+// Window w (slots start + 32 w ...) of a tile of m slots, by one warp: G2P of
+// each slot's particle against the tile's node box (G2P = true) or the stored
+// state (G2P = false), then the scatter of the in-band particles' payloads.
+// Returns this lane's node-block bits of the tile (tile coordinates tc, box
+// origin bo).
+template <int D, int S, bool G2P>
+__device__ __forceinline__ unsigned fused_window(const Particles& P, const StepConsts& C, const TileInfo& TI,
+                                                 const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
+                                                 const SlowQueue& Q, unsigned* __restrict__ status, const float4* box,
+                                                 const int* bo, const int* tc, int start, int m, int w, float4* pay,
+                                                 int* run, int* order) {
+    using G = FusedGeom<D>;
+    using St = Stencil<S>;
+    const int lane = threadIdx.x & 31;
+    const int n = P.n;
+    const long long gsy = C.nx, gsz = (long long)C.nx * C.ny;
+    const int cnt = min(G::WIN, m - w * G::WIN);
+    const bool valid = lane < cnt;
+    const int i = start + w * G::WIN + lane;
+    unsigned long long key = kNoStencil;
+    bool deferred = false;  // queued: scattered after the return map (k_p2g_windows)
+    float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
+    if (valid) {
+        const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
+        float x[D], v[D], A[D * D];
+        bool scatter = vol != 0.f;  // p2g.glsl:42
+        if constexpr (G2P) {
+            float xo[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) xo[k] = P.x[k * n + i];
+            int base[3] = {0, 0, 0};
+            float wk[3][S], off[3][S];
+            bool interior = true, boxed = true;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
+                base[k] = St::base(xo[k], ext);
+                interior = interior && base[k] >= 0 && base[k] + (S - 1) <= ext;
+                boxed = boxed && base[k] - bo[k] >= 0 && base[k] + (S - 1) - bo[k] <= G::BE - 1;
+                St::weights(xo[k], base[k], wk[k]);
+#pragma unroll
+                for (int o = 0; o < S; ++o) off[k][o] = float(base[k] + o) - xo[k];
+            }
+            if (!interior) {
+                // stencil partly outside the grid: the general kernel does the whole G2P
+                Q.list[queue_slot(Q)] = -1 - i;
+                deferred = scatter;
+                scatter = false;
+            } else {
+                float nv[D], nx[D], nB[D * D];
+                const long long gc0 = (D == 3 ? base[2] * gsz : 0) + base[1] * gsy + base[0];
+                if (boxed) {
+                    const int l0 = (D == 3 ? (base[2] - bo[2]) * G::BE * G::BE : 0) + (base[1] - bo[1]) * G::BE +
+                                   (base[0] - bo[0]);
+                    gather_nodes<D, S, true, int>(C, box, l0, G::BE, G::BE * G::BE, gv, gc0, gsy, gsz, wk, off,
+                                                  nv, nB, nx);
+                } else {
+                    gather_nodes<D, S, false, long long>(C, gv, gc0, gsy, gsz, gv, gc0, gsy, gsz, wk, off, nv, nB,
+                                                         nx);
+                }
+                bool finite = true;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    x[k] = xo[k] + nx[k];
+                    v[k] = nv[k];
+                    P.v[k * n + i] = nv[k];
+                    P.x[k * n + i] = x[k];
+                    finite = finite && isfinite(x[k]);
+                }
+                if (!finite) raise_flag(status, 1u);
+#pragma unroll
+                for (int k = 0; k < D * D; ++k) P.B[k * n + i] = nB[k];
+                float Fe[D * D], Fh[D * D];
+#pragma unroll
+                for (int k = 0; k < D * D; ++k) Fe[k] = P.Fe[k * n + i];
+#pragma unroll
+                for (int r = 0; r < D; ++r)
+#pragma unroll
+                    for (int c = 0; c < D; ++c) {
+                        float s = Fe[r * D + c];
+#pragma unroll
+                        for (int k = 0; k < D; ++k) s += (C.dt * St::DINV * nB[r * D + k]) * Fe[k * D + c];
+                        Fh[r * D + c] = s;
+                    }
+                float sig[D * D];
+                const float Jp = P.Jp[i];
+                if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s) &&
+                    hardened_stress_series<D>(Fh, Jp, C.mu0, C.la0, C.xi, sig)) {
+#pragma unroll
+                    for (int k = 0; k < D * D; ++k) {
+                        P.Fe[k * n + i] = Fh[k];
+                        A[k] = St::DINV * mass * nB[k] - St::DINV * C.dt * vol * sig[k];
+                    }
+                } else {
+                    const int slot = queue_slot(Q);
+                    Q.list[slot] = i;
+#pragma unroll
+                    for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
+                    deferred = scatter;
+                    scatter = false;
+                }
+            }
+        } else {
+            float B[D * D], Fe[D * D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
+            mls_affine<D, S>(C, B, Fe, P.Jp[i], mass, vol, A);
+        }
+        if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
+    }
+    if constexpr (G2P) {
+        // record the window if some of its particles wait for the return map
+        const unsigned dm = __ballot_sync(0xffffffffu, deferred);
+        if (dm && lane == 0) {
+            const int r = atomicAdd(Q.nwin, 1);
+            if (r < Q.win_capacity) Q.win[r] = make_int2(start + w * G::WIN, (int)dm);
+        }
+    }
+    reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
+    __syncwarp();
+    return scatter_window<D, S>(C, TI, pay, run, order, cnt, true, bo, tc, acc, status);
+}
+
+// ---------------------------------------------------------------------------
 // The fused kernel. G2P = true: one step (G2P of the state, then the next
 // step's P2G into `acc`). G2P = false: the P2G of the stored state only (after
 // creation or a state upload), reading B, F_E, J_p and forming A as every
-// other path does (mls_affine). TMA (with G2P): the box arrives by TMA tensor
-// loads one tile ahead instead of being staged by the CTA's threads; same
-// box contents, same results.
-template <int D, int S, bool G2P, bool TMA = false>
+// other path does (mls_affine).
+template <int D, int S, bool G2P>
 __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
     k_g2p2g(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv, unsigned long long* __restrict__ acc,
-            SlowQueue Q, unsigned* __restrict__ status, const __grid_constant__ CUtensorMap gv_map) {
+            SlowQueue Q, unsigned* __restrict__ status) {
     using G = FusedGeom<D>;
-    using W = WarpGeom<D, S>;
-    using St = Stencil<S>;
-    constexpr int T = G::T;
-    constexpr bool kTma = G2P && TMA;
-    extern __shared__ __align__(128) unsigned char smem_raw[];  // TMA destinations: 128-byte aligned
-    FusedSmem<D, kTma ? 2 : 1>& SM = *reinterpret_cast<FusedSmem<D, kTma ? 2 : 1>*>(smem_raw);
+    extern __shared__ __align__(128) unsigned char fused_smem[];
+    FusedSmem<D>& SM = *reinterpret_cast<FusedSmem<D>*>(fused_smem);
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int n = P.n;
     const int ntl = *TI.n_tile_list;
     const long long gsy = C.nx, gsz = (long long)C.nx * C.ny;
     float4* pay = SM.pay[wid];
     int* run = SM.run[wid];
     int* order = SM.order[wid];
-    int kbuf = 0;             // box buffer of the current tile
-    unsigned parity = 0u;     // bit k: phase of buffer k's next completion
-    if constexpr (kTma) {
+    for (;;) {
         if (tid == 0) {
-            mbar_init(&SM.bar[0], 1);
-            mbar_init(&SM.bar[1], 1);
-            mbar_init_fence();
-            const int e0 = atomicAdd(TI.fused_next, 1);
-            SM.tile_next = e0;
-            if (e0 < ntl) {
-                int tc0[3], bo0[3];
-                tile_origin<D>(TI, TI.tile_list[e0], tc0, bo0);
-                box_load<D>(gv_map, bo0, SM.box[0], &SM.bar[0]);
-            }
+            SM.tile_next = atomicAdd(TI.fused_next, 1);
+            SM.next_win = 0;
+            SM.bmask = 0u;
         }
         __syncthreads();
-    }
-    for (;;) {
-        int e;
-        if constexpr (kTma) {
-            e = SM.tile_next;
-            __syncthreads();  // every thread has read it, and every warp is done with the other buffer
-            if (e >= ntl) break;
-            if (tid == 0) {
-                SM.next_win = 0;
-                SM.bmask = 0u;
-                // the next tile's box into the other buffer, then wait for this one's
-                const int e1 = atomicAdd(TI.fused_next, 1);
-                SM.tile_next = e1;
-                if (e1 < ntl) {
-                    int tc1[3], bo1[3];
-                    tile_origin<D>(TI, TI.tile_list[e1], tc1, bo1);
-                    fence_proxy_async_smem();
-                    box_load<D>(gv_map, bo1, SM.box[kbuf ^ 1], &SM.bar[kbuf ^ 1]);
-                }
-                SM.box_ok = mbar_wait(&SM.bar[kbuf], (parity >> kbuf) & 1u, kBoxWaitPolls);
-                if (!SM.box_ok) {
-                    // give up (flagged); let the other load land before the CTA leaves
-                    raise_flag(status, 16u);
-                    if (e1 < ntl) mbar_wait(&SM.bar[kbuf ^ 1], (parity >> (kbuf ^ 1)) & 1u, kBoxWaitPolls);
-                }
-            }
-            __syncthreads();
-            if (!SM.box_ok) return;
-            parity ^= 1u << kbuf;
-        } else {
-            if (tid == 0) {
-                SM.tile_next = atomicAdd(TI.fused_next, 1);
-                SM.next_win = 0;
-                SM.bmask = 0u;
-            }
-            __syncthreads();
-            e = SM.tile_next;
-            if (e >= ntl) break;
-        }
-        const float4* box = SM.box[kTma ? kbuf : 0];
+        const int e = SM.tile_next;
+        if (e >= ntl) break;
+        const float4* box = SM.box;
         const int t = TI.tile_list[e];
         const int start = TI.tile_start[t], m = TI.tile_len[e];
         int tc[3] = {0, 0, 0}, bo[3] = {0, 0, 0};  // tile coordinates, box origin node
         tile_origin<D>(TI, t, tc, bo);
-        if constexpr (G2P && !TMA) {  // stage the node velocities of the box
+        if constexpr (G2P) {  // stage the node velocities of the box
             for (int l = tid; l < G::BN; l += G::THREADS) {
                 const int lx = l % G::BE, ly = (l / G::BE) % G::BE, lz = D == 3 ? l / (G::BE * G::BE) : 0;
                 const int gx = bo[0] + lx, gy = bo[1] + ly, gz = D == 3 ? bo[2] + lz : 0;
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (gx >= 0 && gx <= C.W && gy >= 0 && gy <= C.H && (D == 2 || (gz >= 0 && gz <= C.Dp)))
                     v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
-                SM.box[0][l] = v;
+                SM.box[l] = v;
             }
             __syncthreads();
         }
@@ -711,113 +785,7 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             if (lane == 0) w = atomicAdd(&SM.next_win, 1);
             w = __shfl_sync(0xffffffffu, w, 0);
             if (w >= nwin) break;
-            const int cnt = min(G::WIN, m - w * G::WIN);
-            const bool valid = lane < cnt;
-            const int i = start + w * G::WIN + lane;
-            unsigned long long key = kNoStencil;
-            bool deferred = false;  // queued: scattered after the return map (k_p2g_windows)
-            float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
-            if (valid) {
-                const float mass = P.mass ? P.mass[i] : P.mass_u, vol = P.vol ? P.vol[i] : P.vol_u;
-                float x[D], v[D], A[D * D];
-                bool scatter = vol != 0.f;  // p2g.glsl:42
-                if constexpr (G2P) {
-                    float xo[D];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) xo[k] = P.x[k * n + i];
-                    int base[3] = {0, 0, 0};
-                    float wk[3][S], off[3][S];
-                    bool interior = true, boxed = true;
-#pragma unroll
-                    for (int k = 0; k < D; ++k) {
-                        const int ext = k == 0 ? C.W : (k == 1 ? C.H : C.Dp);
-                        base[k] = St::base(xo[k], ext);
-                        interior = interior && base[k] >= 0 && base[k] + (S - 1) <= ext;
-                        boxed = boxed && base[k] - bo[k] >= 0 && base[k] + (S - 1) - bo[k] <= G::BE - 1;
-                        St::weights(xo[k], base[k], wk[k]);
-#pragma unroll
-                        for (int o = 0; o < S; ++o) off[k][o] = float(base[k] + o) - xo[k];
-                    }
-                    if (!interior) {
-                        // stencil partly outside the grid: the general kernel does the whole G2P
-                        Q.list[queue_slot(Q)] = -1 - i;
-                        deferred = scatter;
-                        scatter = false;
-                    } else {
-                        float nv[D], nx[D], nB[D * D];
-                        const long long gc0 = (D == 3 ? base[2] * gsz : 0) + base[1] * gsy + base[0];
-                        if (boxed) {
-                            const int l0 = (D == 3 ? (base[2] - bo[2]) * G::BE * G::BE : 0) + (base[1] - bo[1]) * G::BE +
-                                           (base[0] - bo[0]);
-                            gather_nodes<D, S, true, int>(C, box, l0, G::BE, G::BE * G::BE, gv, gc0, gsy, gsz, wk, off,
-                                                          nv, nB, nx);
-                        } else {
-                            gather_nodes<D, S, false, long long>(C, gv, gc0, gsy, gsz, gv, gc0, gsy, gsz, wk, off, nv, nB,
-                                                                 nx);
-                        }
-                        bool finite = true;
-#pragma unroll
-                        for (int k = 0; k < D; ++k) {
-                            x[k] = xo[k] + nx[k];
-                            v[k] = nv[k];
-                            P.v[k * n + i] = nv[k];
-                            P.x[k * n + i] = x[k];
-                            finite = finite && isfinite(x[k]);
-                        }
-                        if (!finite) raise_flag(status, 1u);
-#pragma unroll
-                        for (int k = 0; k < D * D; ++k) P.B[k * n + i] = nB[k];
-                        float Fe[D * D], Fh[D * D];
-#pragma unroll
-                        for (int k = 0; k < D * D; ++k) Fe[k] = P.Fe[k * n + i];
-#pragma unroll
-                        for (int r = 0; r < D; ++r)
-#pragma unroll
-                            for (int c = 0; c < D; ++c) {
-                                float s = Fe[r * D + c];
-#pragma unroll
-                                for (int k = 0; k < D; ++k) s += (C.dt * St::DINV * nB[r * D + k]) * Fe[k * D + c];
-                                Fh[r * D + c] = s;
-                            }
-                        float sig[D * D];
-                        const float Jp = P.Jp[i];
-                        if (det<D>(Fh) > 0.f && band_gershgorin<D>(Fh, 1.f - C.theta_c, 1.f + C.theta_s) &&
-                            hardened_stress_series<D>(Fh, Jp, C.mu0, C.la0, C.xi, sig)) {
-#pragma unroll
-                            for (int k = 0; k < D * D; ++k) {
-                                P.Fe[k * n + i] = Fh[k];
-                                A[k] = St::DINV * mass * nB[k] - St::DINV * C.dt * vol * sig[k];
-                            }
-                        } else {
-                            const int slot = queue_slot(Q);
-                            Q.list[slot] = i;
-#pragma unroll
-                            for (int k = 0; k < D * D; ++k) Q.fh[k * Q.capacity + slot] = Fh[k];
-                            deferred = scatter;
-                            scatter = false;
-                        }
-                    }
-                } else {
-                    float B[D * D], Fe[D * D];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
-#pragma unroll
-                    for (int k = 0; k < D * D; ++k) { B[k] = P.B[k * n + i]; Fe[k] = P.Fe[k * n + i]; }
-                    mls_affine<D, S>(C, B, Fe, P.Jp[i], mass, vol, A);
-                }
-                if (scatter) key = p2g_payload<D, S>(C, x, v, A, mass, q);
-            }
-            if constexpr (G2P) {
-                // record the window if some of its particles wait for the return map
-                const unsigned dm = __ballot_sync(0xffffffffu, deferred);
-                if (dm && lane == 0) {
-                    const int r = atomicAdd(Q.nwin, 1);
-                    if (r < Q.win_capacity) Q.win[r] = make_int2(start + w * G::WIN, (int)dm);
-                }
-            }
-            reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
-            __syncwarp();
-            bits |= scatter_window<D, S>(C, TI, pay, run, order, cnt, true, bo, tc, acc, status);
+            bits |= fused_window<D, S, G2P>(P, C, TI, gv, acc, Q, status, box, bo, tc, start, m, w, pay, run, order);
         }
         // mark the node blocks the tile's in-box runs added to
         bits = __reduce_or_sync(0xffffffffu, bits);
@@ -829,8 +797,131 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
             const int bx = tc[0] - 1 + rx, by = tc[1] - 1 + ry, bz = D == 3 ? tc[2] - 1 + rz : 0;
             mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
         }
-        kbuf ^= 1;
-        if constexpr (!kTma) __syncthreads();  // SM.bmask, the tile and the box are reset for the next tile
+        __syncthreads();  // SM.bmask, the tile and the box are reset for the next tile
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The fused step with the node boxes brought in by TMA and no CTA barrier
+// after the start: a two-stage pipeline per CTA. Stage k (tile k of the CTA)
+// lives in buffer k & 1: its tile, its box (one TMA tensor load, whose
+// mbarrier `full` completes when the bytes have landed), a window counter,
+// a count of the warps that have left it, and its node-block bits. Each warp
+// waits for the stage's box, takes windows of the tile until none are left,
+// and moves on to stage k + 1, which is already loaded; the last warp to leave
+// stage k marks the tile's node blocks and refills the buffer with stage
+// k + 2 (the next tile from the global counter, or an empty stage that ends
+// the CTA). A warp is thus held up only by a box that has not arrived, never
+// by the other warps' windows. Stages are refilled in order, so tile numbers
+// grow with the stage and the first empty stage ends the work for every warp.
+// Every wait is bounded: a box that does not arrive raises MPM_FLAG_TIMEOUT.
+template <int D> struct PipeSmem {
+    using G = FusedGeom<D>;
+    alignas(128) float4 box[2][G::BNP];                 // (vf, wall flag) per node
+    unsigned long long full[2];                         // the stage's box arrived (or the stage is empty)
+    int tile[2];                                        // tile-list entry of the stage (>= count: empty)
+    int next_win[2];
+    int left[2];                                        // warps done with the stage
+    unsigned bmask[2];
+    float4 pay[G::WARPS][G::WIN * G::PS / 4];
+    int run[G::WARPS][G::WIN + 1];
+    int order[G::WARPS][G::WIN];
+};
+
+// Stage for buffer b: the next tile of the global counter and its box load,
+// or an empty stage. One thread.
+template <int D>
+__device__ __forceinline__ void pipe_refill(PipeSmem<D>& SM, int b, const TileInfo& TI, int ntl,
+                                            const CUtensorMap& map) {
+    const int e = atomicAdd(TI.fused_next, 1);
+    SM.tile[b] = e;
+    if (e < ntl) {
+        int tc[3], bo[3];
+        tile_origin<D>(TI, TI.tile_list[e], tc, bo);
+        fence_proxy_async_smem();
+        box_load<D>(map, bo, SM.box[b], &SM.full[b]);
+    } else {
+        mbar_arrive(&SM.full[b]);
+    }
+}
+
+template <int D, int S>
+__global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
+    k_g2p2g_pipe(Particles P, StepConsts C, TileInfo TI, const float4* __restrict__ gv,
+                 unsigned long long* __restrict__ acc, SlowQueue Q, unsigned* __restrict__ status,
+                 const __grid_constant__ CUtensorMap gv_map) {
+    using G = FusedGeom<D>;
+    constexpr int NBLK = D == 3 ? 27 : 9;
+    extern __shared__ __align__(128) unsigned char fused_smem[];
+    PipeSmem<D>& SM = *reinterpret_cast<PipeSmem<D>*>(fused_smem);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int ntl = *TI.n_tile_list;
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&SM.full[b], 1);
+            SM.next_win[b] = 0;
+            SM.left[b] = 0;
+            SM.bmask[b] = 0u;
+        }
+        mbar_init_fence();
+        pipe_refill<D>(SM, 0, TI, ntl, gv_map);
+        pipe_refill<D>(SM, 1, TI, ntl, gv_map);
+    }
+    __syncthreads();
+    for (int k = 0;; ++k) {
+        const int b = k & 1;
+        const unsigned par = (unsigned)(k >> 1) & 1u;
+        if (!__all_sync(0xffffffffu, mbar_wait(&SM.full[b], par, kBoxWaitPolls))) {
+            // the box never arrived (flagged); let the other buffer's load land first
+            if (lane == 0) {
+                raise_flag(status, 16u);
+                mbar_wait(&SM.full[b ^ 1], (unsigned)((k + 1) >> 1) & 1u, kBoxWaitPolls);
+            }
+            return;
+        }
+        const int e = SM.tile[b];
+        if (e >= ntl) break;
+        const int t = TI.tile_list[e];
+        const int start = TI.tile_start[t], m = TI.tile_len[e];
+        int tc[3] = {0, 0, 0}, bo[3] = {0, 0, 0};
+        tile_origin<D>(TI, t, tc, bo);
+        const int nwin = (m + G::WIN - 1) / G::WIN;
+        unsigned bits = 0u;
+        for (;;) {
+            int w = 0;
+            if (lane == 0) w = atomicAdd(&SM.next_win[b], 1);
+            w = __shfl_sync(0xffffffffu, w, 0);
+            if (w >= nwin) break;
+            bits |= fused_window<D, S, true>(P, C, TI, gv, acc, Q, status, SM.box[b], bo, tc, start, m, w,
+                                             SM.pay[wid], SM.run[wid], SM.order[wid]);
+        }
+        bits = __reduce_or_sync(0xffffffffu, bits);
+        int last = 0;
+        if (lane == 0) {
+            if (bits) atomicOr(&SM.bmask[b], bits);
+            __threadfence_block();  // the bits and this warp's reads of the box before the count
+            last = atomicAdd(&SM.left[b], 1) == G::WARPS - 1;
+        }
+        if (__shfl_sync(0xffffffffu, last, 0)) {
+            // last warp out: mark the tile's node blocks, then stage k + 2 into this buffer
+            __threadfence_block();
+            unsigned bm = 0u;
+            if (lane == 0) bm = atomicOr(&SM.bmask[b], 0u);
+            bm = __shfl_sync(0xffffffffu, bm, 0);
+            if (lane < NBLK && (bm >> lane) & 1u) {
+                const int rx = lane % 3, ry = (lane / 3) % 3, rz = lane / 9;
+                const int bx = tc[0] - 1 + rx, by = tc[1] - 1 + ry, bz = D == 3 ? tc[2] - 1 + rz : 0;
+                mark_block_once(TI, (bz * TI.nblk[1] + by) * TI.nblk[0] + bx);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                SM.bmask[b] = 0u;
+                SM.next_win[b] = 0;
+                SM.left[b] = 0;
+                pipe_refill<D>(SM, b, TI, ntl, gv_map);
+            }
+            __syncwarp();
+        }
     }
 }
 

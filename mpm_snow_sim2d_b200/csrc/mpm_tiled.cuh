@@ -459,7 +459,11 @@ __device__ __forceinline__ void mark_block_once(const TileInfo& TI, int b) {
 
 // int64 fixed-point add of a unit's sums; the range is checked once per unit.
 __device__ __forceinline__ void red_fixed(unsigned long long* p, float v, float scale) {
-    atomicAdd(p, (unsigned long long)__float2ll_rn(v * scale));
+    // an explicit global reduction (no return value): p always points into the
+    // grid sums, and spelling it out keeps the compiler from falling back to a
+    // generic atomic with a return where it cannot prove the address space
+    const unsigned long long g = (unsigned long long)__cvta_generic_to_global(p);
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(g), "l"((unsigned long long)__float2ll_rn(v * scale)));
 }
 
 #ifndef MPM_P2G_MIN_BLOCKS

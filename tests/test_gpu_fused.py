@@ -79,12 +79,13 @@ def test_queued_windows_bitwise(gpu_lib):
         assert np.array_equal(getattr(a, f), getattr(b, f)), f
 
 
-@pytest.mark.parametrize("case", ["impact2d", "slab3d", "impact3d_quad", "impact2d_quad"])
+@pytest.mark.parametrize("case", ["impact2d", "slab3d", "impact3d_quad", "impact2d_quad", "collide3d"])
 def test_tma_box_load(gpu_lib, case):
-    """Node boxes by TMA tensor loads (one thread, one tile ahead, mbarrier
-    waits bounded) hold the same values as boxes staged by the CTA, with
-    zeros outside the grid: the runs agree to FP32 contraction differences
-    between the two kernel builds, and no wait gives up."""
+    """The TMA box pipeline (k_g2p2g_pipe: node boxes by TMA tensor loads two
+    stages deep, warps moving between tiles without CTA barriers, mbarrier
+    waits bounded) against the staged boxes: the same windows and runs, so the
+    runs agree to FP32 contraction differences between the two kernel builds,
+    and no wait gives up."""
     sc, steps = _scenes()[case]
     a, fa = _run(sc, steps, "fused", "gather")
     b, fb = _run(sc, steps, "fused", "tma")
