@@ -224,9 +224,11 @@ def mlp_vs_plain(args, torch, stream):
     of the exact solver from initial velocities perturbed by 1e-6 (relative)
     shows how much any per-step difference of that size grows in this scene."""
     from mpm_snow_sim2d_b200 import Solver, _lib
-    from mpm_snow_sim2d_b200.mlp import DEFAULT_WEIGHTS, Mlp
+    from mpm_snow_sim2d_b200.mlp import DEFAULT_WEIGHTS, MIXED_WEIGHTS, Mlp
     scene = make_scene(args.mlp_workload)
-    net = Mlp.load(args.mlp_weights or DEFAULT_WEIGHTS)
+    # colliding-snowball workloads take the weights trained with collisions
+    weights = args.mlp_weights or (MIXED_WEIGHTS if args.mlp_workload == "c5" else DEFAULT_WEIGHTS)
+    net = Mlp.load(weights)
     rng = np.random.Generator(np.random.PCG64(99))
     solvers = {}
     for mode in ("exact", "mlp", "control"):
@@ -268,7 +270,8 @@ def mlp_vs_plain(args, torch, stream):
     g2p = lambda r: r["stages_ms"].get("g2p", r["stages_ms"].get("g2p2g", 0.0)) + r["stages_ms"]["return_map"]
     return {
         "workload": f"{args.mlp_workload}: {WORKLOADS[args.mlp_workload]}", "particles": scene.count,
-        "steps": args.mlp_steps, "tolerance": args.mlp_tolerance, "plain": res["exact"], "mlp": res["mlp"],
+        "steps": args.mlp_steps, "tolerance": args.mlp_tolerance, "weights": Path(weights).name,
+        "plain": res["exact"], "mlp": res["mlp"],
         "g2p_speedup": g2p(res["exact"]) / g2p(res["mlp"]),
         "return_map_speedup": res["exact"]["stages_ms"]["return_map"] / res["mlp"]["stages_ms"]["return_map"],
         "step_speedup": res["exact"]["ms_per_step"] / res["mlp"]["ms_per_step"],
@@ -470,7 +473,7 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=1000)
     ap.add_argument("--mlp-tolerance", type=float, default=1e-3)
     ap.add_argument("--mlp-weights", default=None, help="network weights (.npz) for the learned return map "
-                    "(default: the shipped ones)")
+                    "(default: the shipped ones for the workload: collisions for c5, impacts otherwise)")
     ap.add_argument("--no-mlp", action="store_true", help="skip the learned-plasticity comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes measurement")
     ap.add_argument("--batch-scenes", type=int, default=256)
