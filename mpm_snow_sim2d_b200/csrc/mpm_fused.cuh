@@ -450,11 +450,11 @@ __device__ __forceinline__ unsigned fused_run(const StepConsts& C, const TileInf
 }
 
 // ---------------------------------------------------------------------------
-// The scatter of one warp's window of payloads (`pay`, stencil keys in the
+// The scatter of one warp's window of payloads (`pay`, the stencil key in the
 // last two floats of each; kNoStencil for slots that add nothing): runs of
 // consecutive slots with one key, longest first, SPLIT lanes per run summing
-// it (fused_run). `cnt` slots of the window are filled. Returns this lane's
-// node-block bits (boxed runs only).
+// it (fused_run). The first `cnt` slots of the window are filled. Returns this
+// lane's node-block bits (boxed runs only).
 template <int D, int S>
 __device__ __forceinline__ unsigned scatter_window(const StepConsts& C, const TileInfo& TI, const float4* pay,
                                                    int* run, int* order, int cnt, bool boxed, const int* bo,
@@ -522,9 +522,10 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS) k_p2g_windows(Particles
     for (int r = blockIdx.x * G::WARPS + wid; r < nw; r += gridDim.x * G::WARPS) {
         const int2 rec = Q.win[r];
         const unsigned mask = (unsigned)rec.y;
-        float* q = reinterpret_cast<float*>(pay) + lane * G::PS;
-        unsigned long long key = kNoStencil;
         if ((mask >> lane) & 1u) {
+            // the queued slots packed in slot order, so that particles of one
+            // cell form one run even when in-band ones sat between them
+            float* q = reinterpret_cast<float*>(pay) + __popc(mask & ((1u << lane) - 1)) * G::PS;
             const int i = rec.x + lane;
             const float mass = P.mass ? P.mass[i] : P.mass_u;
             float x[D], v[D], A[D * D];
@@ -532,11 +533,10 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS) k_p2g_windows(Particles
             for (int k = 0; k < D; ++k) { x[k] = P.x[k * n + i]; v[k] = P.v[k * n + i]; }
 #pragma unroll
             for (int k = 0; k < D * D; ++k) A[k] = P.A[k * n + i];
-            key = p2g_payload<D, S>(C, x, v, A, mass, q);
+            reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = p2g_payload<D, S>(C, x, v, A, mass, q);
         }
-        reinterpret_cast<unsigned long long*>(q + G::KEYF)[0] = key;
         __syncwarp();
-        scatter_window<D, S>(C, TI, pay, run_s[wid], order_s[wid], 32 - __clz(mask), false, none, none, acc, status);
+        scatter_window<D, S>(C, TI, pay, run_s[wid], order_s[wid], __popc(mask), false, none, none, acc, status);
     }
 }
 

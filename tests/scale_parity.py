@@ -101,14 +101,18 @@ def contact_band(scene, position):
 
 
 def errors(a, ref, mask=None):
+    """Relative L2 of each field both states hold (an oracle file may carry a
+    subset); B relative to |v| of `ref`."""
     from conftest import rel_l2
     sel = (lambda x: np.asarray(x)[mask]) if mask is not None else (lambda x: np.asarray(x))
-    vnorm = np.linalg.norm(sel(ref["velocity"]).astype(np.float64))
     out = {}
     for f, key in (("position", "x"), ("velocity", "v"), ("elastic_f", "F"), ("plastic_det", "Jp")):
-        out[key] = rel_l2(sel(a[f]), sel(ref[f]))
-    out["B"] = float(np.linalg.norm((sel(a["affine_b"]).astype(np.float64) - sel(ref["affine_b"])).ravel())
-                     / max(vnorm, 1e-30))
+        if f in a and f in ref:
+            out[key] = rel_l2(sel(a[f]), sel(ref[f]))
+    if "affine_b" in a and "affine_b" in ref and "velocity" in ref:
+        vnorm = np.linalg.norm(sel(ref["velocity"]).astype(np.float64))
+        out["B"] = float(np.linalg.norm((sel(a["affine_b"]).astype(np.float64) - sel(ref["affine_b"])).ravel())
+                         / max(vnorm, 1e-30))
     return out
 
 
