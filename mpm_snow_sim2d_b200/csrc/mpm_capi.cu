@@ -528,9 +528,9 @@ cudaError_t clear_after_p2g(mpm_solver* s) {
 }
 
 
-// The tensor map of the fused kernel's box loads: gv's first half (one float4
-// (vf, wall flag) per node) as a rank D+1 FP32 tensor [nz][ny][nx][4], boxes of
-// 4 x BE^D. The encoder comes from the driver through the runtime, so the
+// The tensor map of the TMA pipeline's box loads (k_g2p2g_pipe): gv's first
+// half (one float4 per node: (vf, wall flag) in 3D, (vf, vc) in 2D) as a rank
+// D+1 FP32 tensor [nz][ny][nx][4], boxes of 4 x BE^D. The encoder comes from the driver through the runtime, so the
 // library needs no link to libcuda.
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
