@@ -541,8 +541,8 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS) k_p2g_windows(Particles
 }
 
 // ---------------------------------------------------------------------------
-// TMA load of a tile's node box and its mbarrier (sm_90+ PTX; one CTA, no
-// cluster multicast).
+// TMA load of a tile's node box and its mbarrier (sm_90+ PTX): each CTA loads
+// its own boxes from this GPU's memory.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
