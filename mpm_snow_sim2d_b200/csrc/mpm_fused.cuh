@@ -776,6 +776,20 @@ __global__ void __launch_bounds__(FusedGeom<D>::THREADS, MPM_FUSED_MIN_BLOCKS)
                     v = __ldg(&gv[gz * gsz + gy * gsy + gx]);
                 SM.box[l] = v;
             }
+            // the tile's G2P inputs (x, F_E, J_p) towards L2 ahead of the windows
+            // that read them; one prefetch per 128-byte line, addresses kept
+            // inside the arrays
+            {
+                constexpr int NF = D + D * D + 1;
+                const int lines = (m + 31) / 32 + 1;
+                const int n = P.n;
+                for (int l = tid; l < NF * lines; l += G::THREADS) {
+                    const int f = l / lines, k = l % lines;
+                    const float* a = f < D ? P.x + (long long)f * n
+                                           : (f < D + D * D ? P.Fe + (long long)(f - D) * n : P.Jp);
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + min(start + 32 * k, n - 1)));
+                }
+            }
             __syncthreads();
         }
         unsigned bits = 0u;  // node blocks this lane's in-box runs added to
