@@ -259,10 +259,12 @@ __device__ __forceinline__ void collide(const StepConsts& C, const float* loc, c
     }
 #pragma unroll
     for (int k = 0; k < D; ++k) vc[k] = vel[k];
-    int hit[6];
-    int nh = 0;
+    // the planes that acted, as bits in plane order (a mask rather than a
+    // list, so that every index below is a compile-time constant)
+    unsigned hit = 0u;
 #pragma unroll
-    for (int b = 0; b < nb; ++b) {
+    for (int b = 0; b < 6; ++b) {
+        if (b >= nb) break;
         const int a = ax[b];
         // n . (loc - P): only the normal's axis contributes (the other terms are 0 * x)
         const float dist = ns[b] * (loc[a] - pp[b]);
@@ -271,13 +273,16 @@ __device__ __forceinline__ void collide(const StepConsts& C, const float* loc, c
         if (delta < 0.f) {
             if (FORM == kClassic) vc[a] -= (delta * ns[b]) / C.dt;
             else vc[a] -= (delta / C.dt) * ns[b];
-            hit[nh++] = b;
+            hit |= 1u << b;
         }
     }
 #pragma unroll
     for (int k = 0; k < D; ++k) vf[k] = vc[k];
-    for (int c = 0; c < nh; ++c) {
-        const int b = hit[c], a = ax[b];
+#pragma unroll
+    for (int b = 0; b < 6; ++b) {
+        if (b >= nb) break;
+        if (!((hit >> b) & 1u)) continue;
+        const int a = ax[b];
         // vt = vc - n (n . vf)
         float vt[3];
 #pragma unroll
@@ -339,8 +344,9 @@ __device__ __forceinline__ void grid_node_velocity(const StepConsts& C, const lo
 // fixed-point accumulators (the reference's separate reset pass,
 // reset.glsl:13-23, is fused here) and writes the velocities G2P gathers.
 template <int D, int FORM>
-__device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long long* __restrict__ acc,
-                                          float4* __restrict__ gv, unsigned* __restrict__ status, long long id) {
+__device__ __forceinline__ void grid_node_at(const StepConsts& C, unsigned long long* __restrict__ acc,
+                                             float4* __restrict__ gv, unsigned* __restrict__ status, long long id,
+                                             int ix, int iy, int iz) {
     constexpr int NACC = Layout<D, FORM>::NACC;
     long long q[NACC];
 #pragma unroll
@@ -349,7 +355,6 @@ __device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long lon
         if (q[c] != 0) acc[c * C.nodes + id] = 0ull;
     }
     float vc[3], vf[3];
-    const long long ix = id % C.nx, iy = (id / C.nx) % C.ny, iz = id / ((long long)C.nx * C.ny);
     grid_node_velocity<D, FORM>(C, q, ix, iy, iz, status, vc, vf);
     if (D == 2) {
         gv[id] = make_float4(vf[0], vf[1], vc[0], vc[1]);
@@ -361,6 +366,14 @@ __device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long lon
         gv[id] = make_float4(vf[0], vf[1], vf[2], hit ? 1.f : 0.f);
         if (hit) gv[C.nodes + id] = make_float4(vc[0], vc[1], vc[2], 0.f);
     }
+}
+
+// The same for a node given by its id alone.
+template <int D, int FORM>
+__device__ __forceinline__ void grid_node(const StepConsts& C, unsigned long long* __restrict__ acc,
+                                          float4* __restrict__ gv, unsigned* __restrict__ status, long long id) {
+    grid_node_at<D, FORM>(C, acc, gv, status, id, int(id % C.nx), int((id / C.nx) % C.ny),
+                          int(id / ((long long)C.nx * C.ny)));
 }
 
 // 3D node velocities as grid_node stores them: vf, and vc (= vf unless flagged).

@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(256) k_grid_marked(StepConsts C, TileInfo TI, 
         const int gx = b[0] * G::T + l[0], gy = b[1] * G::T + l[1], gz = D == 3 ? b[2] * G::T + l[2] : 0;
         if (loc == 0) TI.mark[blk] = 0;
         if (gx >= C.nx || gy >= C.ny || gz >= C.nz) continue;
-        grid_node<D, FORM>(C, acc, gv, status, ((long long)gz * C.ny + gy) * C.nx + gx);
+        grid_node_at<D, FORM>(C, acc, gv, status, ((long long)gz * C.ny + gy) * C.nx + gx, gx, gy, gz);
     }
 }
 
