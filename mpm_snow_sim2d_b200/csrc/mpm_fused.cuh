@@ -164,11 +164,11 @@ __device__ __forceinline__ void gather_nodes(const StepConsts& C, const float4* 
                         const float z = wk[2][c];
                         Pc[0] += z * g[0]; Pc[1] += z * g[1]; Pc[2] += z * g[2];
                     }
-                    const float y = wk[1][b];
+                    const float y = pick<S>(wk[1], b);  // loop index not unrolled: no local array
 #pragma unroll
                     for (int r = 0; r < 3; ++r) Qc[r] += y * Pc[r];
                 }
-                const float x = wk[0][a];
+                const float x = pick<S>(wk[0], a);
 #pragma unroll
                 for (int r = 0; r < 3; ++r) vc[r] += x * Qc[r];
             }
