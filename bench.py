@@ -399,23 +399,32 @@ def refcpu_time(scene, steps, replicas):
     return scene.count * steps * replicas / info["loop_seconds"], info
 
 
-def reference_cpu_leg(steps):
+def reference_cpu_leg(steps, c2_steps=0):
     """The reference's own CPU path (src/cpu compiled unmodified) on the 2D
     three-block workload (128^2, 4 ppc): `steps` steps on one core, then one
-    independent single-threaded solver per host core at once."""
+    independent single-threaded solver per host core at once; with c2_steps,
+    the same for a window of that many steps of the 512^2 eight-block
+    workload."""
     from mpm_snow_sim2d_b200 import scenes
     from oracle import oracle as O
     if not O.refcpu_available():
         return {"unavailable": "oracle/_ref/refcpu_driver is not built"}
-    scene = scenes.workload("c1")
     cores = os.cpu_count() or 1
-    one, info1 = refcpu_time(scene, steps, 1)
-    many, infon = refcpu_time(scene, steps, cores)
-    return {"workload": f"c1: {WORKLOADS['c1']}", "particles": scene.count, "steps": steps, "unit": UNIT,
-            "one_core": one, "all_cores": many, "cores": cores, "kind": "reference",
-            "sample": f"{steps} steps per solver; the reference's src/cpu (CLASSIC APIC, single-threaded) compiled "
-                      f"unmodified; all_cores = {cores} independent solvers at once",
-            "loop_seconds": {"one_core": info1.get("loop_seconds"), "all_cores": infon.get("loop_seconds")}}
+
+    def leg(name, n_steps):
+        scene = scenes.workload(name)
+        one, info1 = refcpu_time(scene, n_steps, 1)
+        many, infon = refcpu_time(scene, n_steps, cores)
+        return {"workload": f"{name}: {WORKLOADS[name]}", "particles": scene.count, "steps": n_steps, "unit": UNIT,
+                "one_core": one, "all_cores": many, "cores": cores, "kind": "reference",
+                "sample": f"{n_steps} steps per solver; the reference's src/cpu (CLASSIC APIC, single-threaded) "
+                          f"compiled unmodified; all_cores = {cores} independent solvers at once",
+                "loop_seconds": {"one_core": info1.get("loop_seconds"), "all_cores": infon.get("loop_seconds")}}
+
+    out = leg("c1", steps)
+    if c2_steps > 0:
+        out["c2_window"] = leg("c2", c2_steps)
+    return out
 
 
 def run_reference_arm(args):
@@ -482,6 +491,8 @@ def main():
     ap.add_argument("--quad-steps", type=int, default=500, help="timed steps of the quadratic-stencil line (0: skip)")
     ap.add_argument("--refcpu-steps", type=int, default=1000,
                     help="steps of the reference's compiled src/cpu on the 2D three-block workload (0: skip)")
+    ap.add_argument("--refcpu-c2-steps", type=int, default=20,
+                    help="a window of steps of the same on the 512^2 eight-block workload (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -633,7 +644,7 @@ def main():
     refcpu_leg = None
     if rank == 0 and world == 1 and args.refcpu_steps > 0:
         try:
-            refcpu_leg = reference_cpu_leg(args.refcpu_steps)
+            refcpu_leg = reference_cpu_leg(args.refcpu_steps, args.refcpu_c2_steps)
         except Exception as e:  # reported, never required
             refcpu_leg = {"error": str(e)}
 
